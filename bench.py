@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""PageRank throughput on one B200 (or N replicas): RMAT scale 24.
+
+Workload (the configuration the metric is quoted on): seeded RMAT graph,
+scale 24 (16,777,216 vertices), edge factor 16, (a,b,c,d) =
+(0.57, 0.19, 0.19, 0.05), self-loops and duplicate edges removed, int32 pull
+CSR + out-degree; plain pull PageRank in FP32 with an FP64 L1 residual,
+damping 0.85f, tolerance 1e-6, at most 100 sweeps, uniform 1/m start.
+
+One step = one complete solve (score initialisation, every sweep until the
+residual drops below the tolerance, scores scattered back to vertex order) on
+the device-resident graph.  value = GTEPS = edges x sweeps / time, summed
+over ranks (replicas, weak scaling).  The graph (1.07 GB of CSR) is larger
+than L2, so no flush is needed between steps.
+
+--impl reference times the reference's own OpenMP PRSolver
+(src/pr/omp_base.cc, compiled from the reference tree into oracle/_ref) on
+the same graph on the host cores: each step is a bounded sample of the same
+solve (SAMPLE_SWEEPS sweeps over the full graph).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+SCALE, EDGE_FACTOR, SEED = 24, 16, 1
+ABC = (0.57, 0.19, 0.19)
+TOL, MAX_ITER = 1e-6, 100
+DAMPING = np.float32(0.85)
+SAMPLE_SWEEPS = 2            # reference / CPU-baseline sample: sweeps per call
+CPU_BASELINE_BUDGET_S = 12.0  # CPU work for the cpu_baseline leg
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def pr_bytes_per_sweep(m, nnz):
+    """Algorithmic bytes of one plain FP32 sweep: 4 nnz (column indices) +
+    4 (m+1) (row offsets) + 12 m (contribution: read score, read degree,
+    write contribution) + 4 m (contributions gathered, counted once) + 8 m
+    (read old score, write new score)  =  4 nnz + 28 m + 4."""
+    return 4 * nnz + 28 * m + 4
+
+
+def spmv_bytes(m, nnz):
+    """Aj + Ax (8 nnz) + row offsets (4 (m+1)) + x once (4 m) + y read/write (8 m)."""
+    return 8 * nnz + 16 * m + 4
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled while the timed region runs."""
+
+    FIELDS = ("index,uuid,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid):
+        self.uuid = uuid
+        self.proc = None
+        self.f = tempfile.TemporaryFile(mode="w+")
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.seek(0)
+        rows = []
+        for line in self.f:
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 10 or (self.uuid and p[1] != self.uuid):
+                continue
+            rows.append(p)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = sorted(float(r[2]) for r in rows)
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[6:10]) if v.lower() == "active"})
+        return {"sm_mhz": sm[len(sm) // 2], "sm_max_mhz": float(rows[0][3]),
+                "samples": len(rows), "power_w_max": max(float(r[4]) for r in rows),
+                "reasons": reasons}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def cpu_reference_sample(rp, col, od, sweeps, budget_s, min_calls=1):
+    """Time the reference's OpenMP PRSolver (oracle/_ref) or, without it, the
+    oracle port, on the full graph, `sweeps` sweeps per call."""
+    import oracle as O
+    m = len(rp) - 1
+    kind = "reference" if O.ref_available() else "port"
+    total_t, total_sweeps, calls = 0.0, 0, 0
+    while calls < min_calls or total_t < budget_s:
+        s0 = np.full(m, np.float32(1.0) / np.float32(m), dtype=np.float32)
+        t0 = time.perf_counter()
+        if kind == "reference":
+            _, printed, _ = O.ref_pr_solver(rp, col, od, scores=s0, tol=0.0, max_iter=sweeps)
+            done = sweeps  # tol 0 never converges: exactly `sweeps` sweeps
+        else:
+            _, done, _ = O.pr_plain_f32(rp, col, od, scores=s0, tol=0.0, max_iter=sweeps)
+        total_t += time.perf_counter() - t0
+        total_sweeps += done
+        calls += 1
+        if calls >= 50:
+            break
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    return {"gteps": len(col) * total_sweeps / total_t / 1e9, "kind": kind, "cores": cores,
+            "calls": calls, "sweeps": total_sweeps, "seconds": total_t}
+
+
+def run_reference(args):
+    world, rank, local = dist_setup()
+    if rank != 0:
+        return 0
+    import oracle as O
+    t0 = time.time()
+    rp, col, od = O.rmat_graph(args.scale, EDGE_FACTOR, seed=SEED, abc=ABC)
+    log(f"[reference] graph s{args.scale}: m={len(rp) - 1} nnz={len(col)} built in {time.time() - t0:.1f}s")
+    kind = "reference" if O.ref_available() else "port"
+    m = len(rp) - 1
+    times = []
+    for i in range(args.warmup + args.steps):
+        s0 = np.full(m, np.float32(1.0) / np.float32(m), dtype=np.float32)
+        t1 = time.perf_counter()
+        if kind == "reference":
+            O.ref_pr_solver(rp, col, od, scores=s0, tol=0.0, max_iter=SAMPLE_SWEEPS)
+        else:
+            O.pr_plain_f32(rp, col, od, scores=s0, tol=0.0, max_iter=SAMPLE_SWEEPS)
+        dt = time.perf_counter() - t1
+        if i >= args.warmup:
+            times.append(dt)
+    total = sum(times)
+    gteps = len(col) * SAMPLE_SWEEPS * len(times) / total / 1e9
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    sample = (f"{SAMPLE_SWEEPS} sweeps of the full RMAT-{args.scale} graph per step "
+              f"(OpenMP, {cores} threads); GTEPS per sweep is what a full solve sustains")
+    line = {
+        "impl": "reference", "metric": "pagerank_gteps_rmat24", "value": gteps, "unit": "GTEPS",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * total / len(times), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded RMAT)",
+        "config": workload_config(args.scale, m, len(col)),
+        "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": cores, "kind": kind,
+                         "sample": sample},
+        "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def workload_config(scale, m, nnz):
+    return {"workload": f"pagerank_rmat{scale}_ef{EDGE_FACTOR}_tol1e-6",
+            "graph": f"RMAT scale {scale}, edge factor {EDGE_FACTOR}, abc={ABC}, seed {SEED}, "
+                     "scrambled ids, self-loops/duplicates removed",
+            "m": m, "nnz": nnz, "tol": TOL, "max_iter": MAX_ITER, "damping": float(DAMPING),
+            "precision": "plain fp32 (fp64 residual)",
+            "l2": "inputs larger than L2 (CSR > 1 GB vs 126 MB L2): no flush between steps",
+            "parallelism": "replicas (one independent solve per GPU)"}
+
+
+def run_ours(args):
+    import torch
+
+    import gardenia_ocl_b200 as G
+    world, rank, local = dist_setup()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    dev = torch.device("cuda", local)
+    stream = torch.cuda.current_stream()
+    t0 = time.time()
+    csr = G.gen_rmat(args.scale, EDGE_FACTOR, seed=SEED, abc=ABC)
+    m, nnz = csr.m, csr.nnz
+    g = G.Graph(csr.rowptr, csr.col, csr.third, m=m, nnz=nnz)
+    g.set_stream(stream.cuda_stream)
+    log(f"[ours] rank {rank}: graph s{args.scale} m={m} nnz={nnz} layout={g.layout()} "
+        f"ready in {time.time() - t0:.2f}s")
+    scores = torch.empty(m, dtype=torch.float32, device=dev)
+    init = float(np.float32(1.0) / np.float32(m))
+    opts = G.options(tol=TOL, max_iter=MAX_ITER, damping=DAMPING)
+
+    def step():
+        scores.fill_(init)
+        _, st = g.pagerank(scores, opts)
+        return st
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    props = torch.cuda.get_device_properties(dev)
+    uuid = getattr(props, "uuid", None)
+    uuid = f"GPU-{uuid}" if uuid is not None and not str(uuid).startswith("GPU-") else uuid
+    sampler = ClockSampler(str(uuid) if uuid else None)
+    sampler.start()
+    time.sleep(0.3)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    stats = []
+    ev0.record(stream)
+    for _ in range(args.steps):
+        stats.append(step())
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clocks = sampler.stop()
+    ms = ev0.elapsed_time(ev1)
+    if dist:
+        t = torch.tensor([ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    sweeps = sum(s.iterations for s in stats)
+    launches = sum(s.gpu_launches for s in stats)
+    gteps = world * nnz * sweeps / (ms / 1e3) / 1e9
+    loop_ms = sum(s.loop_ms for s in stats) / len(stats)
+    sweeps_per_solve = sweeps / len(stats)
+    per_sweep = pr_bytes_per_sweep(m, nnz)
+    alg_bytes = per_sweep * sweeps_per_solve
+    peak, peak_kind = load_peaks()
+    achieved = alg_bytes / (loop_ms / 1e3) / 1e9
+    traffic = load_traffic().get(f"k_pr_persistent_rmat{args.scale}")
+    roof = {"kernel": "k_pr_persistent (all sweeps of one solve)", "bound": "hbm",
+            "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+            "frac": achieved / peak,
+            "traffic": (traffic["bytes_per_sweep"] * sweeps_per_solve) if traffic else None,
+            "algorithmic_bytes_per_launch": alg_bytes,
+            "bytes_per_sweep_formula": "4*nnz + 28*m + 4",
+            "launch_ms": loop_ms}
+    resid = g.residual_f64(scores, DAMPING)
+    accuracy = {"fp64_residual_l1": resid,
+                "l1_error_bound_vs_fixed_point": resid / (1.0 - float(DAMPING)),
+                "sweeps_per_solve": sweeps_per_solve}
+
+    line = {"metric": "pagerank_gteps_rmat24", "value": gteps, "unit": "GTEPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded RMAT generated on the GPU)",
+            "config": workload_config(args.scale, m, nnz), "roofline": roof,
+            "gpu_launches": launches, "clocks": clocks, "accuracy": accuracy}
+
+    # End to end through the reference-shaped C-ABI call with host buffers:
+    # PageRank(m, nnz, row_offsets, column_indices, degree, scores) copies the
+    # CSR in, builds the layout, solves and copies the scores back.
+    if not args.no_e2e:
+        h_rp = torch.empty(m + 1, dtype=torch.int32, pin_memory=True)
+        h_col = torch.empty(nnz, dtype=torch.int32, pin_memory=True)
+        h_od = torch.empty(m, dtype=torch.int32, pin_memory=True)
+        h_sc = torch.empty(m, dtype=torch.float32, pin_memory=True)
+        for h, d in ((h_rp, csr.rowptr), (h_col, csr.col), (h_od, csr.third)):
+            G.lib().gpr_memcpy(G.C.c_void_p(h.data_ptr()), G.C.c_void_p(d.ptr), d.nbytes)
+        na = [x.numpy() for x in (h_rp, h_col, h_od, h_sc)]
+        e2e_steps = max(1, min(args.steps, 5))
+        e_sweeps, e_time = 0, 0.0
+        for i in range(1 + e2e_steps):
+            na[3].fill(np.float32(1.0) / np.float32(m))
+            torch.cuda.synchronize()
+            if dist:
+                dist.barrier()
+            t1 = time.perf_counter()
+            st = G.PageRank(m, nnz, na[0], na[1], na[2], na[3], tol=TOL, max_iter=MAX_ITER,
+                            damping=DAMPING)
+            dt = time.perf_counter() - t1
+            if i > 0:
+                e_sweeps += st.iterations
+                e_time += dt
+        if dist:
+            t = torch.tensor([e_time], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            e_time = float(t.item())
+        line["e2e"] = {"value": world * nnz * e_sweeps / e_time / 1e9, "unit": "GTEPS",
+                       "h2d_bytes_per_step": 4 * (m + 1) + 4 * nnz + 4 * m + 4 * m,
+                       "d2h_bytes_per_step": 4 * m, "ms_per_step": 1e3 * e_time / e2e_steps,
+                       "call": "PageRank(m, nnz, row_offsets, column_indices, degree, scores) "
+                               "via gpr_page_rank, pinned host buffers"}
+
+    if not args.no_spmv:
+        line["spmv"] = spmv_leg(G, torch, dev, stream, args)
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        import oracle as O  # checker / baseline only
+        rp = csr.rowptr.to_numpy()
+        col = csr.col.to_numpy()
+        od = csr.third.to_numpy()
+        cb = cpu_reference_sample(rp, col, od, SAMPLE_SWEEPS, CPU_BASELINE_BUDGET_S)
+        line["cpu_baseline"] = {"value": cb["gteps"], "unit": "GTEPS", "cores": cb["cores"],
+                                "kind": cb["kind"],
+                                "sample": f"{cb['calls']} calls x {SAMPLE_SWEEPS} sweeps of the "
+                                          f"full RMAT-{args.scale} graph ({cb['seconds']:.1f} s)"}
+        del O
+    g.close()
+    csr.close()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def spmv_leg(G, torch, dev, stream, args):
+    """27-point 3-D Laplacian, 128^3 grid: y = A x (x seeded uniform, y = 0)."""
+    A = G.gen_stencil27(128)
+    M = G.Matrix(A.rowptr, A.col, A.third, m=A.m, nnz=A.nnz)
+    x = torch.empty(A.m, dtype=torch.float32, device=dev)
+    G.gen_uniform(A.m, 11, x)
+    y = torch.zeros(A.m, dtype=torch.float32, device=dev)
+    for _ in range(3):
+        M.spmv(x, y, stream.cuda_stream)
+    torch.cuda.synchronize()
+    reps = 20
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(reps):
+        M.spmv(x, y, stream.cuda_stream)
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    ms = ev0.elapsed_time(ev1) / reps
+    peak, kind = load_peaks()
+    b = spmv_bytes(A.m, A.nnz)
+    M.close()
+    A.close()
+    return {"workload": "spmv_stencil27_128^3", "m": A.m, "nnz": A.nnz, "ms": ms,
+            "gflops": 2 * A.nnz / (ms / 1e3) / 1e9, "achieved_gbs": b / (ms / 1e3) / 1e9,
+            "frac": b / (ms / 1e3) / 1e9 / peak, "peak": peak, "peak_kind": kind,
+            "bytes_formula": "8*nnz + 16*m + 4"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--scale", type=int, default=SCALE)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-spmv", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        log("warm-up raised to 3 steps (minimum)")
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,399 @@
+"""gardenia_ocl_b200 -- B200-native pull PageRank and CSR SpMV.
+
+Python mirror of the reference's driver surface (Gardenia ``src/pr``,
+``src/spmv``): ``PRSolver``, ``PageRank``, ``SpmvSolver``, ``read_graph``, plus
+handle-based access (``Graph``, ``Matrix``) for device-resident, repeated
+solves.  Every call goes through the C ABI of ``libgpr.so`` (include/gpr.h),
+whose kernels are compiled for sm_100a; there is no CPU implementation of the
+solvers in this package, and importing it on a machine without the built
+library raises.
+
+Arrays may be numpy arrays (host) or objects exposing ``data_ptr()`` (e.g.
+torch CUDA tensors, device memory): the library copies host inputs itself.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libgpr.so")
+
+GPR_OK, GPR_EINVAL, GPR_ENOMEM, GPR_ECUDA, GPR_ETIMEOUT, GPR_ENODEV, GPR_EUNSUPPORTED = range(7)
+PREC_FP32, PREC_BF16, PREC_FP16 = 0, 1, 2
+LOOP_AUTO, LOOP_PERSISTENT, LOOP_GRAPH = 0, 1, 2
+KDAMP = np.float32(0.85)  # include/common.h:18
+EPSILON = 0.001           # src/pr/pr.h:4
+MAX_ITER = 30             # src/pr/pr.h:5
+
+
+class GprError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"gpr status {status}: {msg}")
+        self.status = status
+
+
+class PrOptions(C.Structure):
+    _fields_ = [("damping", C.c_float), ("tol", C.c_double), ("max_iter", C.c_int),
+                ("precision", C.c_int), ("loop", C.c_int), ("timeout_s", C.c_double),
+                ("refine_max", C.c_int), ("reserved", C.c_int * 8)]
+
+
+class PrStats(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("refine_iterations", C.c_int),
+                ("residual", C.c_double), ("solve_ms", C.c_double),
+                ("loop_ms", C.c_double), ("gpu_launches", C.c_int), ("reserved", C.c_int * 5)]
+
+    def as_dict(self):
+        return {"iterations": self.iterations, "refine_iterations": self.refine_iterations,
+                "residual": self.residual, "solve_ms": self.solve_ms, "loop_ms": self.loop_ms,
+                "gpu_launches": self.gpu_launches}
+
+
+_LIB = None
+_vp = C.c_void_p
+
+
+def lib():
+    """Load libgpr.so (built in-tree by ``build()``); raises if it is missing."""
+    global _LIB
+    if _LIB is not None:
+        return _LIB
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: run gardenia_ocl_b200.build() "
+                           "(the CUDA library is required; there is no CPU path)")
+    L = C.CDLL(LIB_PATH)
+    I, LL, D, F = C.c_int, C.c_longlong, C.c_double, C.c_float
+    sig = {
+        "gpr_last_error": (C.c_char_p, []),
+        "gpr_version": (C.c_char_p, []),
+        "gpr_pr_opts_default": (I, [C.POINTER(PrOptions)]),
+        "gpr_graph_create": (I, [I, LL, _vp, _vp, _vp, C.POINTER(_vp)]),
+        "gpr_graph_destroy": (I, [_vp]),
+        "gpr_graph_info": (I, [_vp, C.POINTER(I), C.POINTER(LL), C.POINTER(LL)]),
+        "gpr_graph_layout": (I, [_vp, C.POINTER(I), C.POINTER(I), C.POINTER(I), C.POINTER(I),
+                                 C.POINTER(LL), C.POINTER(LL)]),
+        "gpr_graph_set_stream": (I, [_vp, _vp]),
+        "gpr_graph_residuals": (I, [_vp, C.POINTER(D), I]),
+        "gpr_pagerank": (I, [_vp, _vp, C.POINTER(PrOptions), C.POINTER(PrStats)]),
+        "gpr_pr_residual_f64": (I, [_vp, _vp, F, C.POINTER(D)]),
+        "gpr_pr_solver": (I, [I, I, _vp, _vp, _vp, _vp, _vp, _vp, C.POINTER(PrOptions),
+                              C.POINTER(PrStats)]),
+        "gpr_page_rank": (I, [I, I, _vp, _vp, _vp, _vp, C.POINTER(PrOptions),
+                              C.POINTER(PrStats)]),
+        "gpr_matrix_create": (I, [I, LL, _vp, _vp, _vp, C.POINTER(_vp)]),
+        "gpr_matrix_destroy": (I, [_vp]),
+        "gpr_matrix_layout": (I, [_vp, C.POINTER(I), C.POINTER(I), C.POINTER(I), C.POINTER(LL)]),
+        "gpr_spmv": (I, [_vp, _vp, _vp, _vp]),
+        "gpr_spmv_solver": (I, [I, I, _vp, _vp, _vp, _vp, _vp]),
+        "gpr_gen_rmat": (I, [I, I, D, D, D, C.c_ulonglong, I, C.POINTER(_vp), C.POINTER(_vp),
+                             C.POINTER(_vp), C.POINTER(LL)]),
+        "gpr_gen_stencil27": (I, [I, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),
+                                  C.POINTER(LL)]),
+        "gpr_gen_uniform": (I, [LL, C.c_ulonglong, _vp]),
+        "gpr_free": (I, [_vp]),
+        "gpr_malloc": (I, [C.POINTER(_vp), C.c_size_t]),
+        "gpr_memcpy": (I, [_vp, _vp, C.c_size_t]),
+        "gpr_synchronize": (I, []),
+        "gpr_read_graph": (I, [C.c_char_p, I, I, I, I, I, C.POINTER(I), C.POINTER(I),
+                               C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
+        "gpr_read_graph_free": (None, [_vp]),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(L, name)
+        fn.restype = res
+        fn.argtypes = args
+    _LIB = L
+    return L
+
+
+def build(verbose: bool = False) -> None:
+    """Compile libgpr.so for sm_100a in-tree (make in csrc/)."""
+    import subprocess
+    subprocess.run(["make", "-s" if not verbose else "-j8", "-j8", "-C",
+                    os.path.join(_HERE, "csrc")], check=True)
+    global _LIB
+    _LIB = None
+
+
+def _check(status):
+    if status != GPR_OK:
+        msg = lib().gpr_last_error()
+        raise GprError(status, msg.decode() if msg else "")
+
+
+def _ptr(a, dtype=None):
+    """Pointer to host numpy / device (data_ptr) memory; keeps numpy alive via the caller."""
+    if a is None:
+        return None, None
+    if hasattr(a, "data_ptr"):
+        return C.c_void_p(a.data_ptr()), a
+    if isinstance(a, DeviceArray):
+        return C.c_void_p(a.ptr), a
+    arr = np.ascontiguousarray(a, dtype=dtype) if dtype is not None else np.ascontiguousarray(a)
+    return C.c_void_p(arr.ctypes.data), arr
+
+
+def options(tol=EPSILON, max_iter=MAX_ITER, damping=KDAMP, precision=PREC_FP32,
+            loop=LOOP_AUTO, timeout_s=5.0, refine_max=64) -> PrOptions:
+    o = PrOptions()
+    _check(lib().gpr_pr_opts_default(C.byref(o)))
+    o.tol, o.max_iter, o.damping = float(tol), int(max_iter), float(damping)
+    o.precision, o.loop, o.timeout_s, o.refine_max = int(precision), int(loop), float(timeout_s), int(refine_max)
+    return o
+
+
+class DeviceArray:
+    """Device memory owned by libgpr (from the generators); freed on close()."""
+
+    def __init__(self, ptr, n, dtype):
+        self.ptr, self.n, self.dtype = int(ptr or 0), int(n), np.dtype(dtype)
+
+    @property
+    def nbytes(self):
+        return self.n * self.dtype.itemsize
+
+    def __len__(self):
+        return self.n
+
+    def data_ptr(self):
+        return self.ptr
+
+    def to_numpy(self):
+        out = np.empty(self.n, dtype=self.dtype)
+        if self.n:
+            _check(lib().gpr_memcpy(C.c_void_p(out.ctypes.data), C.c_void_p(self.ptr), self.nbytes))
+        return out
+
+    def close(self):
+        if self.ptr:
+            lib().gpr_free(C.c_void_p(self.ptr))
+            self.ptr = 0
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+# ---------------------------------------------------------------------------
+# PageRank
+# ---------------------------------------------------------------------------
+class Graph:
+    """Device-resident pull graph: in-CSR (row v = sources of edges u->v) plus
+    the out-degree of every vertex (src/pr/omp_base.cc:9 arguments)."""
+
+    def __init__(self, rowptr, col, outdeg, m=None, nnz=None):
+        L = lib()
+        m = int(len(rowptr) - 1) if m is None else int(m)
+        nnz = int(len(col)) if nnz is None else int(nnz)
+        pr, k0 = _ptr(rowptr, np.int32)
+        pc, k1 = _ptr(col, np.int32)
+        pd, k2 = _ptr(outdeg, np.int32)
+        h = C.c_void_p()
+        _check(L.gpr_graph_create(m, nnz, pr, pc, pd, C.byref(h)))
+        self._h, self.m, self.nnz = h, m, nnz
+        self.last_stats = None
+
+    def pagerank(self, scores=None, opts: PrOptions | None = None, **kw):
+        """Solve in place.  ``scores``: host numpy float32 (returned as a new
+        array when None: uniform 1/m) or device memory (updated in place)."""
+        o = opts if opts is not None else options(**kw)
+        if scores is None:
+            scores = np.full(self.m, np.float32(1.0) / np.float32(self.m), dtype=np.float32)
+        if isinstance(scores, np.ndarray):
+            if scores.dtype != np.float32 or not scores.flags.c_contiguous:
+                raise TypeError("scores must be a contiguous float32 array")
+        ps, keep = _ptr(scores)
+        st = PrStats()
+        _check(lib().gpr_pagerank(self._h, ps, C.byref(o), C.byref(st)))
+        self.last_stats = st
+        return scores, st
+
+    def residuals(self):
+        n = self.last_stats.iterations if self.last_stats else 0
+        out = (C.c_double * max(n, 1))()
+        _check(lib().gpr_graph_residuals(self._h, out, n))
+        return np.array(out[:n])
+
+    def residual_f64(self, scores, damping=KDAMP) -> float:
+        ps, keep = _ptr(scores, np.float32)
+        r = C.c_double()
+        _check(lib().gpr_pr_residual_f64(self._h, ps, float(damping), C.byref(r)))
+        return float(r.value)
+
+    def layout(self):
+        v = [C.c_int() for _ in range(4)] + [C.c_longlong() for _ in range(2)]
+        _check(lib().gpr_graph_layout(self._h, *[C.byref(x) for x in v]))
+        keys = ["n_long", "n_nz", "n_chunks", "n_slices", "long_elems", "sell_elems"]
+        return {k: x.value for k, x in zip(keys, v)}
+
+    def info(self):
+        m, nnz, nb = C.c_int(), C.c_longlong(), C.c_longlong()
+        _check(lib().gpr_graph_info(self._h, C.byref(m), C.byref(nnz), C.byref(nb)))
+        return {"m": m.value, "nnz": nnz.value, "device_bytes": nb.value}
+
+    def set_stream(self, stream_handle: int):
+        _check(lib().gpr_graph_set_stream(self._h, C.c_void_p(stream_handle)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gpr_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def PRSolver(m, nnz, in_row_offsets, in_column_indices, out_row_offsets, out_column_indices,
+             degree, scores, tol=EPSILON, max_iter=MAX_ITER, **kw):
+    """src/pr/pr.h:23.  ``scores`` (float32, host or device) is updated in
+    place; returns the stats (iterations = sweeps executed)."""
+    o = options(tol=tol, max_iter=max_iter, **kw)
+    st = PrStats()
+    ptrs = [_ptr(a, np.int32) for a in (in_row_offsets, in_column_indices, out_row_offsets,
+                                        out_column_indices, degree)]
+    ps, keep = _ptr(scores)
+    if isinstance(scores, np.ndarray) and scores.dtype != np.float32:
+        raise TypeError("scores must be float32")
+    _check(lib().gpr_pr_solver(int(m), int(nnz), *[p for p, _ in ptrs], ps, C.byref(o), C.byref(st)))
+    return st
+
+
+def PageRank(m, nnz, row_offsets, column_indices, degree, scores, tol=EPSILON,
+             max_iter=MAX_ITER, **kw):
+    """Pull PageRank over the in-CSR and out-degree; ``scores`` updated in place."""
+    o = options(tol=tol, max_iter=max_iter, **kw)
+    st = PrStats()
+    ptrs = [_ptr(a, np.int32) for a in (row_offsets, column_indices, degree)]
+    ps, keep = _ptr(scores)
+    if isinstance(scores, np.ndarray) and scores.dtype != np.float32:
+        raise TypeError("scores must be float32")
+    _check(lib().gpr_page_rank(int(m), int(nnz), *[p for p, _ in ptrs], ps, C.byref(o), C.byref(st)))
+    return st
+
+
+# ---------------------------------------------------------------------------
+# SpMV
+# ---------------------------------------------------------------------------
+class Matrix:
+    """Device-resident CSR matrix for y <- y + A x."""
+
+    def __init__(self, Ap, Aj, Ax, m=None, nnz=None):
+        m = int(len(Ap) - 1) if m is None else int(m)
+        nnz = int(len(Aj)) if nnz is None else int(nnz)
+        pa, k0 = _ptr(Ap, np.int32)
+        pj, k1 = _ptr(Aj, np.int32)
+        px, k2 = _ptr(Ax, np.float32)
+        h = C.c_void_p()
+        _check(lib().gpr_matrix_create(m, nnz, pa, pj, px, C.byref(h)))
+        self._h, self.m, self.nnz = h, m, nnz
+
+    def spmv(self, d_x, d_y, stream_handle: int = 0):
+        """Device x, y (data_ptr objects); asynchronous on the stream."""
+        _check(lib().gpr_spmv(self._h, _ptr(d_x)[0], _ptr(d_y)[0], C.c_void_p(stream_handle)))
+
+    def layout(self):
+        v = [C.c_int() for _ in range(3)] + [C.c_longlong()]
+        _check(lib().gpr_matrix_layout(self._h, *[C.byref(x) for x in v]))
+        return dict(zip(["n_long", "n_chunks", "n_slices", "sell_elems"], [x.value for x in v]))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gpr_matrix_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def SpmvSolver(m, nnz, Ap, Aj, Ax, x, y):
+    """src/spmv/spmv.h:29: y <- y + A x, ``y`` (float32 numpy) updated in place."""
+    if not (isinstance(y, np.ndarray) and y.dtype == np.float32 and y.flags.c_contiguous):
+        raise TypeError("y must be a contiguous float32 numpy array")
+    args = [_ptr(Ap, np.int32), _ptr(Aj, np.int32), _ptr(Ax, np.float32), _ptr(x, np.float32)]
+    _check(lib().gpr_spmv_solver(int(m), int(nnz), *[p for p, _ in args],
+                                 C.c_void_p(y.ctypes.data)))
+
+
+# ---------------------------------------------------------------------------
+# Inputs: loaders and generators
+# ---------------------------------------------------------------------------
+def read_graph(path, symmetrize=False, transpose=False, sorted=True, remove_selfloops=True,
+               remove_redundents=True):
+    """include/graph_io.h:280 with the same flags.  Returns
+    (m, nnz, row_offsets, column_indices, degree, weight) as numpy arrays."""
+    L = lib()
+    m, nnz = C.c_int(), C.c_int()
+    p = [C.c_void_p() for _ in range(4)]
+    _check(L.gpr_read_graph(os.fsencode(path), int(symmetrize), int(transpose), int(sorted),
+                            int(remove_selfloops), int(remove_redundents), C.byref(m),
+                            C.byref(nnz), *[C.byref(q) for q in p]))
+    mm, nz = m.value, nnz.value
+
+    def take(ptr, n, ct, dt):
+        a = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(max(n, 1),))[:n].astype(dt, copy=True)
+        L.gpr_read_graph_free(ptr)
+        return a
+    rp = take(p[0], mm + 1, C.c_int, np.int32)
+    col = take(p[1], nz, C.c_int, np.int32)
+    deg = take(p[2], mm, C.c_int, np.int32)
+    wt = take(p[3], nz, C.c_float, np.float32)
+    return mm, nz, rp, col, deg, wt
+
+
+class DeviceCSR:
+    """CSR arrays in device memory produced by a generator."""
+
+    def __init__(self, m, nnz, rowptr, col, third, third_dtype):
+        self.m, self.nnz = m, nnz
+        self.rowptr = DeviceArray(rowptr, m + 1, np.int32)
+        self.col = DeviceArray(col, nnz, np.int32)
+        self.third = DeviceArray(third, m if third_dtype == np.int32 else nnz, third_dtype)
+
+    def close(self):
+        for a in (self.rowptr, self.col, self.third):
+            a.close()
+
+
+def gen_rmat(scale, edge_factor=16, seed=1, abc=(0.57, 0.19, 0.19), scramble=True) -> DeviceCSR:
+    """Seeded RMAT pull graph on the GPU: rowptr, col (in-CSR), third = out-degree."""
+    rp, cp, dp, nnz = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_longlong()
+    _check(lib().gpr_gen_rmat(int(scale), int(edge_factor), abc[0], abc[1], abc[2], int(seed),
+                              1 if scramble else 0, C.byref(rp), C.byref(cp), C.byref(dp),
+                              C.byref(nnz)))
+    return DeviceCSR(1 << scale, nnz.value, rp.value, cp.value, dp.value, np.int32)
+
+
+def gen_stencil27(n) -> DeviceCSR:
+    """27-point Laplacian on an n^3 grid on the GPU: rowptr, col, third = values."""
+    ap, aj, ax, nnz = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_longlong()
+    _check(lib().gpr_gen_stencil27(int(n), C.byref(ap), C.byref(aj), C.byref(ax), C.byref(nnz)))
+    return DeviceCSR(n ** 3, nnz.value, ap.value, aj.value, ax.value, np.float32)
+
+
+def gen_uniform(n, seed, d_out) -> None:
+    _check(lib().gpr_gen_uniform(int(n), int(seed), _ptr(d_out)[0]))
+
+
+def synchronize():
+    _check(lib().gpr_synchronize())
+
+
+def version() -> str:
+    return lib().gpr_version().decode()

@@ -1,0 +1,133 @@
+// Internal helpers and device layouts shared by the libgpr translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "gpr.h"
+
+namespace gpr {
+
+// Thread-local message of the last failure (gpr_last_error).
+void set_error(const char *fmt, ...);
+
+// Device allocation that records ENOMEM / ECUDA in the error slot.
+int dmalloc(void **p, size_t bytes, const char *what);
+template <typename T>
+int dalloc(T **p, size_t count, const char *what) {
+  return dmalloc(reinterpret_cast<void **>(p), (count ? count : 1) * sizeof(T), what);
+}
+void dfree(void *p);
+
+// True if `p` is device (or managed) memory of the current context.
+bool is_device_ptr(const void *p);
+
+// Copies `bytes` from a host-or-device pointer into a fresh device buffer,
+// or returns the pointer itself (owned = false) when it is already on the
+// device.
+int to_device(const void *any, size_t bytes, void **dev, bool *owned,
+              cudaStream_t st, const char *what);
+
+// ---------------------------------------------------------------------------
+// Pull-graph layout after relabelling vertices by descending in-degree.
+//
+//   new row i  <->  old vertex perm[i]
+//   rows [0, n_long)      in-degree > sell_max: CSR whose row starts are
+//                         16-byte aligned, each row cut into chunks of
+//                         `chunk` edges (one warp per chunk)
+//   rows [n_long, n_nz)   1 <= in-degree <= sell_max: SELL-32 slices, one
+//                         lane per row, column-major inside the slice, so a
+//                         lane sums its row in the original CSR order
+//   rows [n_nz, m)        in-degree 0
+//
+// Every padding entry of either edge array holds the sentinel index m, whose
+// contribution slot is kept at 0.
+// ---------------------------------------------------------------------------
+struct PrLayout {
+  int m = 0;
+  long long nnz = 0;
+  int n_long = 0, n_nz = 0;
+  int sell_max = 0, chunk = 0;
+  int n_chunks = 0, n_slices = 0, n_zblk = 0;
+  int max_row_chunks = 0;         // chunks of the longest row
+  int *perm = nullptr;            // [m] new -> old
+  int *outdeg = nullptr;          // [m] out-degree in new order
+  long long *long_ptr = nullptr;  // [n_long+1] padded offsets into long_col
+  int *long_col = nullptr;        // relabelled sources of the long rows
+  int *row_cbeg = nullptr;        // [n_long+1] first chunk of each long row
+  int *chunk_row = nullptr;       // [n_chunks] row of each chunk
+  long long *slice_ptr = nullptr; // [n_slices+1] offsets into sell_col
+  int *sell_col = nullptr;        // relabelled sources, SELL-32 column-major
+  long long long_elems = 0, sell_elems = 0;
+  long long device_bytes = 0;
+};
+
+int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
+                    const int *d_outdeg, int sell_max, int chunk, PrLayout *L,
+                    cudaStream_t st);
+void free_pr_layout(PrLayout *L);
+
+// Validates a device CSR (rowptr[0] = 0, monotone, rowptr[m] = nnz, every
+// column in [0, ncols)) and, when d_outdeg is given, out-degrees >= 0.
+int validate_csr(int m, long long nnz, int ncols, const int *d_rowptr,
+                 const int *d_col, const int *d_outdeg, cudaStream_t st);
+
+// ---------------------------------------------------------------------------
+// SpMV layout: natural row order.  Rows with more than sell_max entries are
+// long rows handled in chunks (listed in long_rows); every other row sits in
+// a SELL-32 slice with its own length (sell_len, 255 marks a long row whose
+// lane is idle in the slice).
+// ---------------------------------------------------------------------------
+struct SpmvLayout {
+  int m = 0;
+  long long nnz = 0;
+  int sell_max = 0, chunk = 0;
+  int n_long = 0, n_chunks = 0, n_slices = 0;
+  int *long_rows = nullptr;        // [n_long] row ids, ascending
+  long long *long_ptr = nullptr;   // [n_long+1] padded offsets
+  int *long_col = nullptr;
+  float *long_val = nullptr;
+  int *row_cbeg = nullptr;         // [n_long+1]
+  int *chunk_row = nullptr;        // [n_chunks] index into long_rows
+  long long *slice_ptr = nullptr;  // [n_slices+1]
+  int *sell_col = nullptr;
+  float *sell_val = nullptr;
+  unsigned char *sell_len = nullptr;  // [m]
+  long long long_elems = 0, sell_elems = 0;
+  long long device_bytes = 0;
+};
+
+int build_spmv_layout(int m, long long nnz, const int *d_Ap, const int *d_Aj,
+                      const float *d_Ax, int sell_max, int chunk, SpmvLayout *L,
+                      cudaStream_t st);
+void free_spmv_layout(SpmvLayout *L);
+
+}  // namespace gpr
+
+#define GPR_CUDA(call)                                                        \
+  do {                                                                        \
+    cudaError_t e_ = (call);                                                  \
+    if (e_ != cudaSuccess) {                                                  \
+      gpr::set_error("%s:%d: %s: %s", __FILE__, __LINE__, #call,             \
+                     cudaGetErrorString(e_));                                 \
+      return GPR_ECUDA;                                                       \
+    }                                                                         \
+  } while (0)
+
+#define GPR_TRY(call)                                                         \
+  do {                                                                        \
+    int s_ = (call);                                                          \
+    if (s_ != GPR_OK) return s_;                                              \
+  } while (0)
+
+namespace gpr {
+constexpr int kZeroRowsPerUnit = 128;  // rows per zero-in-degree work unit
+constexpr int kSellMaxDefault = 64;    // in-degree bound of the SELL bin
+constexpr int kChunkDefault = 2048;    // edges per long-row chunk (multiple of 128)
+constexpr int kBlock = 256;            // threads per CTA of the sweep kernels
+
+__host__ __device__ inline long long ceil_div(long long a, long long b) {
+  return (a + b - 1) / b;
+}
+}  // namespace gpr

@@ -1,0 +1,483 @@
+// Device-side construction of the PR and SpMV layouts from a CSR.
+//
+// PR: vertices are relabelled by descending in-degree (stable), which turns
+// the degree bins into contiguous row ranges (no row lists to read per sweep)
+// and packs the most-gathered contributions of a power-law graph into a
+// small, cache-friendly prefix.  Edge order inside each row is preserved.
+#include <cub/cub.cuh>
+
+#include "gpr_internal.cuh"
+
+namespace gpr {
+
+namespace {
+
+__global__ void k_validate_rows(int m, long long nnz, const int *__restrict__ rowptr,
+                                const int *__restrict__ outdeg, int *flag) {
+  long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i > m) return;
+  if (i == 0 && rowptr[0] != 0) atomicOr(flag, 1);
+  if (i == m && (long long)rowptr[m] != nnz) atomicOr(flag, 2);
+  if (i < m) {
+    if (rowptr[i] > rowptr[i + 1]) atomicOr(flag, 4);
+    if (outdeg && outdeg[i] < 0) atomicOr(flag, 16);
+  }
+}
+
+__global__ void k_validate_cols(long long nnz, int ncols, const int *__restrict__ col,
+                                int *flag) {
+  long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < nnz; e += stride) {
+    int c = col[e];
+    if (c < 0 || c >= ncols) atomicOr(flag, 8);
+  }
+}
+
+__global__ void k_indeg_iota(int m, const int *__restrict__ rowptr, int *indeg, int *iota) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) {
+    indeg[i] = rowptr[i + 1] - rowptr[i];
+    iota[i] = i;
+  }
+}
+
+// Sorted (descending) degrees -> n_long = #rows with deg > t, n_nz = #deg > 0.
+__global__ void k_bounds(int m, const int *__restrict__ sdeg, int t, int *out) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= m) return;
+  int d = sdeg[i];
+  int dn = (i + 1 < m) ? sdeg[i + 1] : -1;
+  if (d > t && dn <= t) out[0] = i + 1;
+  if (d > 0 && dn <= 0) out[1] = i + 1;
+}
+
+__global__ void k_relabel(int m, const int *__restrict__ perm, const int *__restrict__ outdeg,
+                          int *outdeg_new, int *inv) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) {
+    int o = perm[i];
+    outdeg_new[i] = outdeg[o];
+    inv[o] = i;
+  }
+}
+
+__global__ void k_long_lens(int n_long, const int *__restrict__ sdeg, int chunk,
+                            long long *plen, int *nch) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_long) {
+    long long p = ((long long)sdeg[i] + 3) & ~3LL;
+    plen[i] = p;
+    nch[i] = (int)((p + chunk - 1) / chunk);
+  } else if (i == n_long) {
+    plen[i] = 0;
+    nch[i] = 0;
+  }
+}
+
+__global__ void k_fill_chunk_row(int n_long, const int *__restrict__ cbeg, int *chunk_row) {
+  int lane = threadIdx.x & 31;
+  long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long r = w; r < n_long; r += nw)
+    for (int c = cbeg[r] + lane; c < cbeg[r + 1]; c += 32) chunk_row[c] = (int)r;
+}
+
+// One warp per long row: relabelled sources, padded with the sentinel m.
+__global__ void k_fill_long(int n_long, int m, const int *__restrict__ perm,
+                            const int *__restrict__ inv, const int *__restrict__ rowptr,
+                            const int *__restrict__ col, const long long *__restrict__ lptr,
+                            int *long_col) {
+  int lane = threadIdx.x & 31;
+  long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long r = w; r < n_long; r += nw) {
+    int o = perm[r];
+    long long sb = rowptr[o];
+    long long deg = rowptr[o + 1] - sb;
+    long long db = lptr[r], plen = lptr[r + 1] - db;
+    for (long long k = lane; k < plen; k += 32)
+      long_col[db + k] = (k < deg) ? inv[col[sb + k]] : m;
+  }
+}
+
+__global__ void k_slice_lens(int n_slices, int n_long, const int *__restrict__ sdeg,
+                             long long *slen) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n_slices) slen[s] = 32LL * sdeg[n_long + 32LL * s];
+  else if (s == n_slices) slen[s] = 0;
+}
+
+// One thread per (slice, lane).
+__global__ void k_fill_sell(int n_slices, int n_long, int n_nz, int m,
+                            const int *__restrict__ perm, const int *__restrict__ inv,
+                            const int *__restrict__ rowptr, const int *__restrict__ col,
+                            const int *__restrict__ sdeg, const long long *__restrict__ sptr,
+                            int *sell_col) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= 32LL * n_slices) return;
+  int s = (int)(t >> 5), lane = (int)(t & 31);
+  long long base = sptr[s];
+  int len = (int)((sptr[s + 1] - base) >> 5);
+  long long r = n_long + 32LL * s + lane;
+  int deg = 0;
+  long long sb = 0;
+  if (r < n_nz) {
+    deg = sdeg[r];
+    sb = rowptr[perm[r]];
+  }
+  for (int j = 0; j < len; ++j)
+    sell_col[base + 32LL * j + lane] = (j < deg) ? inv[col[sb + j]] : m;
+}
+
+template <typename T>
+int exclusive_scan(T *d, long long n, cudaStream_t st) {
+  size_t tmp_bytes = 0;
+  GPR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tmp_bytes, d, d, (int)n, st));
+  void *tmp = nullptr;
+  GPR_TRY(dmalloc(&tmp, tmp_bytes, "scan scratch"));
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, d, d, (int)n, st);
+  cudaFree(tmp);
+  if (e != cudaSuccess) {
+    set_error("DeviceScan::ExclusiveSum: %s", cudaGetErrorString(e));
+    return GPR_ECUDA;
+  }
+  return GPR_OK;
+}
+
+inline unsigned grid_for(long long n, int block = 256) {
+  long long g = (n + block - 1) / block;
+  if (g < 1) g = 1;
+  if (g > 0x7fffffffLL) g = 0x7fffffffLL;
+  return (unsigned)g;
+}
+
+struct Scratch {
+  void *p[8] = {nullptr};
+  ~Scratch() {
+    for (void *q : p) dfree(q);
+  }
+};
+
+}  // namespace
+
+int validate_csr(int m, long long nnz, int ncols, const int *d_rowptr, const int *d_col,
+                 const int *d_outdeg, cudaStream_t st) {
+  if (m < 0 || nnz < 0 || nnz > 0x7fffffffLL) {
+    set_error("invalid sizes m=%d nnz=%lld", m, nnz);
+    return GPR_EINVAL;
+  }
+  int *flag = nullptr;
+  GPR_TRY(dalloc(&flag, 1, "validation flag"));
+  cudaMemsetAsync(flag, 0, sizeof(int), st);
+  k_validate_rows<<<grid_for((long long)m + 1), 256, 0, st>>>(m, nnz, d_rowptr, d_outdeg, flag);
+  if (nnz > 0) {
+    long long g = grid_for(nnz);
+    if (g > 148 * 64) g = 148 * 64;
+    k_validate_cols<<<(unsigned)g, 256, 0, st>>>(nnz, ncols, d_col, flag);
+  }
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(flag);
+  if (e != cudaSuccess) {
+    set_error("CSR validation: %s", cudaGetErrorString(e));
+    return GPR_ECUDA;
+  }
+  if (h) {
+    set_error("malformed CSR (flags 0x%x: 1 rowptr[0]!=0, 2 rowptr[m]!=nnz, 4 rowptr not "
+              "monotone, 8 column out of range, 16 negative degree)", h);
+    return GPR_EINVAL;
+  }
+  return GPR_OK;
+}
+
+int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
+                    const int *d_outdeg, int sell_max, int chunk, PrLayout *L,
+                    cudaStream_t st) {
+  *L = PrLayout();
+  L->m = m;
+  L->nnz = nnz;
+  L->sell_max = sell_max;
+  L->chunk = chunk;
+  if (m <= 0) return GPR_OK;
+  Scratch S;
+  int *indeg = nullptr, *iota = nullptr, *sdeg = nullptr, *inv = nullptr, *bounds = nullptr;
+  GPR_TRY(dalloc(&indeg, m, "in-degree"));
+  S.p[0] = indeg;
+  GPR_TRY(dalloc(&iota, m, "iota"));
+  S.p[1] = iota;
+  GPR_TRY(dalloc(&sdeg, m, "sorted degree"));
+  S.p[2] = sdeg;
+  GPR_TRY(dalloc(&inv, m, "inverse permutation"));
+  S.p[3] = inv;
+  GPR_TRY(dalloc(&bounds, 2, "bounds"));
+  S.p[4] = bounds;
+  GPR_TRY(dalloc(&L->perm, m, "permutation"));
+  GPR_TRY(dalloc(&L->outdeg, m, "out-degree"));
+
+  k_indeg_iota<<<grid_for(m), 256, 0, st>>>(m, d_rowptr, indeg, iota);
+  {
+    size_t tb = 0;
+    GPR_CUDA(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb, indeg, sdeg, iota, L->perm,
+                                                       m, 0, 32, st));
+    void *tmp = nullptr;
+    GPR_TRY(dmalloc(&tmp, tb, "sort scratch"));
+    cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(tmp, tb, indeg, sdeg, iota,
+                                                              L->perm, m, 0, 32, st);
+    cudaFree(tmp);
+    if (e != cudaSuccess) {
+      set_error("degree sort: %s", cudaGetErrorString(e));
+      return GPR_ECUDA;
+    }
+  }
+  GPR_CUDA(cudaMemsetAsync(bounds, 0, 2 * sizeof(int), st));
+  k_bounds<<<grid_for(m), 256, 0, st>>>(m, sdeg, sell_max, bounds);
+  k_relabel<<<grid_for(m), 256, 0, st>>>(m, L->perm, d_outdeg, L->outdeg, inv);
+  int hb[2];
+  GPR_CUDA(cudaMemcpyAsync(hb, bounds, sizeof(hb), cudaMemcpyDeviceToHost, st));
+  GPR_CUDA(cudaStreamSynchronize(st));
+  L->n_long = hb[0];
+  L->n_nz = hb[1];
+
+  // Long rows: padded CSR + chunk table.
+  GPR_TRY(dalloc(&L->long_ptr, (size_t)L->n_long + 1, "long row offsets"));
+  GPR_TRY(dalloc(&L->row_cbeg, (size_t)L->n_long + 1, "long row chunk offsets"));
+  k_long_lens<<<grid_for((long long)L->n_long + 1), 256, 0, st>>>(L->n_long, sdeg, chunk,
+                                                                   L->long_ptr, L->row_cbeg);
+  GPR_TRY(exclusive_scan(L->long_ptr, (long long)L->n_long + 1, st));
+  GPR_TRY(exclusive_scan(L->row_cbeg, (long long)L->n_long + 1, st));
+  GPR_CUDA(cudaMemcpyAsync(&L->long_elems, L->long_ptr + L->n_long, sizeof(long long),
+                           cudaMemcpyDeviceToHost, st));
+  GPR_CUDA(cudaMemcpyAsync(&L->n_chunks, L->row_cbeg + L->n_long, sizeof(int),
+                           cudaMemcpyDeviceToHost, st));
+  GPR_CUDA(cudaStreamSynchronize(st));
+  if (L->n_long > 0) {
+    int top = 0;
+    GPR_CUDA(cudaMemcpy(&top, sdeg, sizeof(int), cudaMemcpyDeviceToHost));
+    L->max_row_chunks = (int)ceil_div(((long long)top + 3) & ~3LL, chunk);
+  }
+  GPR_TRY(dalloc(&L->long_col, (size_t)L->long_elems, "long rows"));
+  GPR_TRY(dalloc(&L->chunk_row, (size_t)L->n_chunks, "chunk rows"));
+  if (L->n_long > 0) {
+    unsigned g = grid_for(32LL * L->n_long);
+    if (g > 148u * 32u) g = 148u * 32u;
+    k_fill_chunk_row<<<g, 256, 0, st>>>(L->n_long, L->row_cbeg, L->chunk_row);
+    k_fill_long<<<g, 256, 0, st>>>(L->n_long, m, L->perm, inv, d_rowptr, d_col, L->long_ptr,
+                                   L->long_col);
+  }
+
+  // SELL-32 slices over rows [n_long, n_nz).
+  L->n_slices = (int)ceil_div((long long)L->n_nz - L->n_long, 32);
+  GPR_TRY(dalloc(&L->slice_ptr, (size_t)L->n_slices + 1, "slice offsets"));
+  k_slice_lens<<<grid_for((long long)L->n_slices + 1), 256, 0, st>>>(L->n_slices, L->n_long,
+                                                                      sdeg, L->slice_ptr);
+  GPR_TRY(exclusive_scan(L->slice_ptr, (long long)L->n_slices + 1, st));
+  GPR_CUDA(cudaMemcpyAsync(&L->sell_elems, L->slice_ptr + L->n_slices, sizeof(long long),
+                           cudaMemcpyDeviceToHost, st));
+  GPR_CUDA(cudaStreamSynchronize(st));
+  GPR_TRY(dalloc(&L->sell_col, (size_t)L->sell_elems, "sell slices"));
+  if (L->n_slices > 0)
+    k_fill_sell<<<grid_for(32LL * L->n_slices), 256, 0, st>>>(
+        L->n_slices, L->n_long, L->n_nz, m, L->perm, inv, d_rowptr, d_col, sdeg, L->slice_ptr,
+        L->sell_col);
+  L->n_zblk = (int)ceil_div((long long)m - L->n_nz, kZeroRowsPerUnit);
+  GPR_CUDA(cudaGetLastError());
+  GPR_CUDA(cudaStreamSynchronize(st));
+  L->device_bytes = 4LL * (2LL * m) + 8LL * (L->n_long + 1) + 4LL * L->long_elems +
+                    4LL * (L->n_long + 1) + 4LL * L->n_chunks + 8LL * (L->n_slices + 1) +
+                    4LL * L->sell_elems;
+  return GPR_OK;
+}
+
+void free_pr_layout(PrLayout *L) {
+  dfree(L->perm);
+  dfree(L->outdeg);
+  dfree(L->long_ptr);
+  dfree(L->long_col);
+  dfree(L->row_cbeg);
+  dfree(L->chunk_row);
+  dfree(L->slice_ptr);
+  dfree(L->sell_col);
+  *L = PrLayout();
+}
+
+// ---------------------------------------------------------------------------
+// SpMV layout (natural row order)
+// ---------------------------------------------------------------------------
+namespace {
+
+__global__ void k_spmv_flags(int m, const int *__restrict__ Ap, int sell_max, int *is_long,
+                             unsigned char *sell_len) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) {
+    int d = Ap[i + 1] - Ap[i];
+    int lg = d > sell_max;
+    is_long[i] = lg;
+    sell_len[i] = lg ? (unsigned char)255 : (unsigned char)d;
+  }
+}
+
+__global__ void k_spmv_long_lens(int n_long, const int *__restrict__ rows,
+                                 const int *__restrict__ Ap, int chunk, long long *plen,
+                                 int *nch) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n_long) {
+    int r = rows[i];
+    long long p = ((long long)(Ap[r + 1] - Ap[r]) + 3) & ~3LL;
+    plen[i] = p;
+    nch[i] = (int)((p + chunk - 1) / chunk);
+  } else if (i == n_long) {
+    plen[i] = 0;
+    nch[i] = 0;
+  }
+}
+
+__global__ void k_spmv_fill_long(int n_long, const int *__restrict__ rows,
+                                 const int *__restrict__ Ap, const int *__restrict__ Aj,
+                                 const float *__restrict__ Ax,
+                                 const long long *__restrict__ lptr, int *lcol, float *lval) {
+  int lane = threadIdx.x & 31;
+  long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long i = w; i < n_long; i += nw) {
+    int r = rows[i];
+    long long sb = Ap[r], deg = Ap[r + 1] - sb;
+    long long db = lptr[i], plen = lptr[i + 1] - db;
+    for (long long k = lane; k < plen; k += 32) {
+      bool v = k < deg;
+      lcol[db + k] = v ? Aj[sb + k] : 0;
+      lval[db + k] = v ? Ax[sb + k] : 0.0f;
+    }
+  }
+}
+
+__global__ void k_spmv_slice_lens(int m, int n_slices, const unsigned char *__restrict__ len,
+                                  long long *slen) {
+  int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s < n_slices) {
+    int mx = 0;
+    for (int l = 0; l < 32; ++l) {
+      long long r = 32LL * s + l;
+      if (r < m && len[r] != 255 && len[r] > mx) mx = len[r];
+    }
+    slen[s] = 32LL * mx;
+  } else if (s == n_slices) {
+    slen[s] = 0;
+  }
+}
+
+__global__ void k_spmv_fill_sell(int m, int n_slices, const int *__restrict__ Ap,
+                                 const int *__restrict__ Aj, const float *__restrict__ Ax,
+                                 const unsigned char *__restrict__ len,
+                                 const long long *__restrict__ sptr, int *scol, float *sval) {
+  long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= 32LL * n_slices) return;
+  int s = (int)(t >> 5), lane = (int)(t & 31);
+  long long base = sptr[s];
+  int slen = (int)((sptr[s + 1] - base) >> 5);
+  long long r = 32LL * s + lane;
+  int d = 0;
+  long long sb = 0;
+  if (r < m && len[r] != 255) {
+    d = len[r];
+    sb = Ap[r];
+  }
+  for (int j = 0; j < slen; ++j) {
+    bool v = j < d;
+    scol[base + 32LL * j + lane] = v ? Aj[sb + j] : 0;
+    sval[base + 32LL * j + lane] = v ? Ax[sb + j] : 0.0f;
+  }
+}
+
+}  // namespace
+
+int build_spmv_layout(int m, long long nnz, const int *d_Ap, const int *d_Aj,
+                      const float *d_Ax, int sell_max, int chunk, SpmvLayout *L,
+                      cudaStream_t st) {
+  *L = SpmvLayout();
+  L->m = m;
+  L->nnz = nnz;
+  L->sell_max = sell_max > 254 ? 254 : sell_max;
+  L->chunk = chunk;
+  if (m <= 0) return GPR_OK;
+  Scratch S;
+  int *is_long = nullptr, *iota = nullptr, *nsel = nullptr;
+  GPR_TRY(dalloc(&is_long, m, "long flags"));
+  S.p[0] = is_long;
+  GPR_TRY(dalloc(&iota, m, "iota"));
+  S.p[1] = iota;
+  GPR_TRY(dalloc(&nsel, 1, "selected count"));
+  S.p[2] = nsel;
+  GPR_TRY(dalloc(&L->sell_len, m, "row lengths"));
+  GPR_TRY(dalloc(&L->long_rows, m, "long rows"));
+  k_spmv_flags<<<grid_for(m), 256, 0, st>>>(m, d_Ap, L->sell_max, is_long, L->sell_len);
+  {
+    cub::CountingInputIterator<int> it(0);
+    size_t tb = 0;
+    GPR_CUDA(cub::DeviceSelect::Flagged(nullptr, tb, it, is_long, L->long_rows, nsel, m, st));
+    void *tmp = nullptr;
+    GPR_TRY(dmalloc(&tmp, tb, "select scratch"));
+    cudaError_t e = cub::DeviceSelect::Flagged(tmp, tb, it, is_long, L->long_rows, nsel, m, st);
+    cudaFree(tmp);
+    if (e != cudaSuccess) {
+      set_error("long-row select: %s", cudaGetErrorString(e));
+      return GPR_ECUDA;
+    }
+  }
+  GPR_CUDA(cudaMemcpyAsync(&L->n_long, nsel, sizeof(int), cudaMemcpyDeviceToHost, st));
+  GPR_CUDA(cudaStreamSynchronize(st));
+  GPR_TRY(dalloc(&L->long_ptr, (size_t)L->n_long + 1, "long offsets"));
+  GPR_TRY(dalloc(&L->row_cbeg, (size_t)L->n_long + 1, "long chunk offsets"));
+  k_spmv_long_lens<<<grid_for((long long)L->n_long + 1), 256, 0, st>>>(
+      L->n_long, L->long_rows, d_Ap, chunk, L->long_ptr, L->row_cbeg);
+  GPR_TRY(exclusive_scan(L->long_ptr, (long long)L->n_long + 1, st));
+  GPR_TRY(exclusive_scan(L->row_cbeg, (long long)L->n_long + 1, st));
+  GPR_CUDA(cudaMemcpyAsync(&L->long_elems, L->long_ptr + L->n_long, sizeof(long long),
+                           cudaMemcpyDeviceToHost, st));
+  GPR_CUDA(cudaMemcpyAsync(&L->n_chunks, L->row_cbeg + L->n_long, sizeof(int),
+                           cudaMemcpyDeviceToHost, st));
+  GPR_CUDA(cudaStreamSynchronize(st));
+  GPR_TRY(dalloc(&L->long_col, (size_t)L->long_elems, "long cols"));
+  GPR_TRY(dalloc(&L->long_val, (size_t)L->long_elems, "long vals"));
+  GPR_TRY(dalloc(&L->chunk_row, (size_t)L->n_chunks, "chunk rows"));
+  if (L->n_long > 0) {
+    unsigned g = grid_for(32LL * L->n_long);
+    if (g > 148u * 32u) g = 148u * 32u;
+    k_fill_chunk_row<<<g, 256, 0, st>>>(L->n_long, L->row_cbeg, L->chunk_row);
+    k_spmv_fill_long<<<g, 256, 0, st>>>(L->n_long, L->long_rows, d_Ap, d_Aj, d_Ax,
+                                        L->long_ptr, L->long_col, L->long_val);
+  }
+  L->n_slices = (int)ceil_div(m, 32);
+  GPR_TRY(dalloc(&L->slice_ptr, (size_t)L->n_slices + 1, "slice offsets"));
+  k_spmv_slice_lens<<<grid_for((long long)L->n_slices + 1), 256, 0, st>>>(
+      m, L->n_slices, L->sell_len, L->slice_ptr);
+  GPR_TRY(exclusive_scan(L->slice_ptr, (long long)L->n_slices + 1, st));
+  GPR_CUDA(cudaMemcpyAsync(&L->sell_elems, L->slice_ptr + L->n_slices, sizeof(long long),
+                           cudaMemcpyDeviceToHost, st));
+  GPR_CUDA(cudaStreamSynchronize(st));
+  GPR_TRY(dalloc(&L->sell_col, (size_t)L->sell_elems, "sell cols"));
+  GPR_TRY(dalloc(&L->sell_val, (size_t)L->sell_elems, "sell vals"));
+  k_spmv_fill_sell<<<grid_for(32LL * L->n_slices), 256, 0, st>>>(
+      m, L->n_slices, d_Ap, d_Aj, d_Ax, L->sell_len, L->slice_ptr, L->sell_col, L->sell_val);
+  GPR_CUDA(cudaGetLastError());
+  GPR_CUDA(cudaStreamSynchronize(st));
+  L->device_bytes = (long long)m * 5 + 8LL * (L->n_long + 1) * 2 + 8LL * L->long_elems +
+                    4LL * L->n_chunks + 8LL * (L->n_slices + 1) + 8LL * L->sell_elems;
+  return GPR_OK;
+}
+
+void free_spmv_layout(SpmvLayout *L) {
+  dfree(L->long_rows);
+  dfree(L->long_ptr);
+  dfree(L->long_col);
+  dfree(L->long_val);
+  dfree(L->row_cbeg);
+  dfree(L->chunk_row);
+  dfree(L->slice_ptr);
+  dfree(L->sell_col);
+  dfree(L->sell_val);
+  dfree(L->sell_len);
+  *L = SpmvLayout();
+}
+
+}  // namespace gpr

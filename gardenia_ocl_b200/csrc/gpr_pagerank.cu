@@ -1,0 +1,823 @@
+// Pull PageRank on B200: sweep kernels, graph handle and solve driver.
+//
+// One sweep is one pass of the reference's iteration body
+// (src/pr/omp_base.cc:23-44): every vertex pulls the contributions of its
+// in-neighbours, updates its score, and adds |s_new - s_old| to an FP64 L1
+// residual.  The contribution of the NEXT sweep (score / out-degree,
+// omp_base.cc:25-27) is produced in the same pass from the freshly written
+// score, so a sweep reads each per-vertex array once.  Contributions are
+// double-buffered (c0/c1 by sweep parity).
+//
+// Work units, one warp each, over the relabelled layout (gpr_internal.cuh):
+//   chunk  -- up to `chunk` edges of a long row; 128-bit index loads;
+//             partial sums of multi-chunk rows are combined by the last
+//             arriving warp in a fixed order (deterministic)
+//   slice  -- 32 consecutive short rows, one lane per row, summing its row
+//             in CSR order with one rounded float add per edge exactly like
+//             the reference's inner loop (omp_base.cc:34-37)
+//   zero   -- 128 rows without in-edges
+//
+// The score update uses explicitly rounded multiply and add
+// (base + kDamp*sum, omp_base.cc:39) so no FMA contraction changes results,
+// and the contribution uses IEEE division (omp_base.cc:26).
+#include <math.h>
+#include <string.h>
+
+#include <vector>
+
+#include "gpr_internal.cuh"
+
+using gpr::PrLayout;
+
+struct gpr_graph {
+  int device = 0;
+  PrLayout L;
+  float *s = nullptr;        // [m] scores, new order
+  float *c0 = nullptr;       // [m+1] contributions (sweep parity 0 input)
+  float *c1 = nullptr;       // [m+1]
+  float *partial = nullptr;  // [n_chunks] partial sums of long-row chunks
+  int *cnt = nullptr;        // [n_long] arrival counters of multi-chunk rows
+  double *cta_err = nullptr; // [2 * max grid] per-CTA residual partials
+  double *err_hist = nullptr;// [err_cap] residual of every sweep
+  unsigned *bar = nullptr;   // [4] grid barrier: arrivals, generation
+  int *status = nullptr;     // [4] error flags, sweeps done, done flag
+  float *scores_tmp = nullptr; // [m] device copy of host scores
+  double *res_tmp = nullptr;   // [m+1+n_long] FP64 residual scratch
+  int err_cap = 0;
+  int last_sweeps = 0;
+  int grid_persist = 0, grid_step = 0, max_grid = 0;
+  bool coop = false;
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+};
+
+namespace {
+
+struct PrArgs {
+  int m, n_long, n_nz, n_chunks, n_slices, n_zblk, chunk;
+  const long long *long_ptr;
+  const int *long_col;
+  const int *row_cbeg;
+  const int *chunk_row;
+  const long long *slice_ptr;
+  const int *sell_col;
+  const int *outdeg;
+  float *s, *c0, *c1, *partial;
+  int *cnt;
+  double *cta_err, *err_hist;
+  unsigned *bar;
+  int *status;
+  float base, damp;
+  double tol;
+  int max_iter;
+  int bar_expect;
+  long long timeout_ns;
+};
+
+constexpr unsigned kFull = 0xffffffffu;
+
+__device__ __forceinline__ uint64_t evict_first_policy() {
+  uint64_t p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+  return p;
+}
+
+// Edge indices are read exactly once per sweep: bypass L1, evict-first in L2
+// so they do not push the contributions out.
+__device__ __forceinline__ int ld_idx(const int *p, uint64_t pol) {
+  int v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"
+      : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
+__device__ __forceinline__ int4 ld_idx4(const int *p, uint64_t pol) {
+  int4 v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
+      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p), "l"(pol));
+  return v;
+}
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ float warp_sum(float v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
+  return v;
+}
+
+// Score update of row r from its pulled sum; returns |s_new - s_old|.
+__device__ __forceinline__ double row_update(const PrArgs &a, int r, float sum, float *cout) {
+  const float so = a.s[r];
+  const float sn = __fadd_rn(a.base, __fmul_rn(a.damp, sum));
+  a.s[r] = sn;
+  cout[r] = __fdiv_rn(sn, __int2float_rn(a.outdeg[r]));
+  return (double)fabsf(__fsub_rn(sn, so));
+}
+
+__device__ __forceinline__ double do_chunk(const PrArgs &a, const float *cin, float *cout,
+                                           int c, int lane, uint64_t pol) {
+  const int r = a.chunk_row[c];
+  const int cb = a.row_cbeg[r];
+  const int nc = a.row_cbeg[r + 1] - cb;
+  const long long b = a.long_ptr[r] + (long long)(c - cb) * a.chunk;
+  const long long e = min(b + (long long)a.chunk, a.long_ptr[r + 1]);
+  float acc0 = 0.f, acc1 = 0.f;
+  long long k = b + 4 * lane;
+  for (; k + 128 < e; k += 256) {
+    const int4 q0 = ld_idx4(a.long_col + k, pol);
+    const int4 q1 = ld_idx4(a.long_col + k + 128, pol);
+    const float v0 = cin[q0.x], v1 = cin[q0.y], v2 = cin[q0.z], v3 = cin[q0.w];
+    const float v4 = cin[q1.x], v5 = cin[q1.y], v6 = cin[q1.z], v7 = cin[q1.w];
+    acc0 += (v0 + v1) + (v2 + v3);
+    acc1 += (v4 + v5) + (v6 + v7);
+  }
+  if (k < e) {
+    const int4 q0 = ld_idx4(a.long_col + k, pol);
+    acc0 += (cin[q0.x] + cin[q0.y]) + (cin[q0.z] + cin[q0.w]);
+  }
+  const float acc = warp_sum(acc0 + acc1);
+  if (nc == 1) return lane == 0 ? row_update(a, r, acc, cout) : 0.0;
+  int last = 0;
+  if (lane == 0) {
+    a.partial[c] = acc;
+    __threadfence();
+    last = atomicAdd(a.cnt + r, 1) == nc - 1;
+  }
+  last = __shfl_sync(kFull, last, 0);
+  if (!last) return 0.0;
+  __threadfence();
+  float t = 0.f;
+  for (int q = lane; q < nc; q += 32) t += __ldcg(a.partial + cb + q);
+  t = warp_sum(t);
+  if (lane != 0) return 0.0;
+  atomicExch(a.cnt + r, 0);
+  return row_update(a, r, t, cout);
+}
+
+__device__ __forceinline__ double do_slice(const PrArgs &a, const float *cin, float *cout,
+                                           int sidx, int lane, uint64_t pol) {
+  const long long b = a.slice_ptr[sidx];
+  const int len = (int)((a.slice_ptr[sidx + 1] - b) >> 5);
+  const int *p = a.sell_col + b + lane;
+  float acc = 0.f;
+  int j = 0;
+  for (; j + 8 <= len; j += 8) {
+    int c[8];
+    float v[8];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) c[q] = ld_idx(p + 32 * (j + q), pol);
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = cin[c[q]];
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc = __fadd_rn(acc, v[q]);
+  }
+  for (; j + 2 <= len; j += 2) {
+    const int c0 = ld_idx(p + 32 * j, pol), c1 = ld_idx(p + 32 * (j + 1), pol);
+    const float v0 = cin[c0], v1 = cin[c1];
+    acc = __fadd_rn(acc, v0);
+    acc = __fadd_rn(acc, v1);
+  }
+  if (j < len) acc = __fadd_rn(acc, cin[ld_idx(p + 32 * j, pol)]);
+  const int r = a.n_long + sidx * 32 + lane;
+  return r < a.n_nz ? row_update(a, r, acc, cout) : 0.0;
+}
+
+__device__ __forceinline__ double do_zero(const PrArgs &a, float *cout, int z, int lane) {
+  double err = 0.0;
+  const int r0 = a.n_nz + z * gpr::kZeroRowsPerUnit;
+#pragma unroll
+  for (int q = 0; q < gpr::kZeroRowsPerUnit / 32; ++q) {
+    const int r = r0 + 32 * q + lane;
+    if (r < a.m) err += row_update(a, r, 0.f, cout);
+  }
+  return err;
+}
+
+__device__ __forceinline__ double sweep(const PrArgs &a, const float *cin, float *cout,
+                                        long long gw, long long nw, int lane, uint64_t pol) {
+  const long long u1 = a.n_chunks, u2 = u1 + a.n_slices, u3 = u2 + a.n_zblk;
+  double err = 0.0;
+  for (long long u = gw; u < u3; u += nw) {
+    if (u < u1) err += do_chunk(a, cin, cout, (int)u, lane, pol);
+    else if (u < u2) err += do_slice(a, cin, cout, (int)(u - u1), lane, pol);
+    else err += do_zero(a, cout, (int)(u - u2), lane);
+  }
+  return err;
+}
+
+// Sum over the CTA; the result is valid in thread 0.
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double red[32];
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+  return t;
+}
+
+// Grid barrier that also reduces the per-CTA residuals of sweep `it` into
+// err_hist[it].  The CTA that arrives last sums the partials in CTA order
+// (deterministic) and opens the next generation.  Every wait is bounded by
+// timeout_ns of %globaltimer; on expiry the CTA raises status[0] bit 0 and
+// the caller returns.  Requires co-resident CTAs (cooperative launch).
+__device__ bool barrier_reduce(const PrArgs &a, int it, double cta_total) {
+  __shared__ int s_state;
+  __shared__ unsigned s_gen;
+  const unsigned G = gridDim.x;
+  if (threadIdx.x == 0) {
+    a.cta_err[(size_t)(it & 1) * G + blockIdx.x] = cta_total;
+    s_gen = ld_acquire(a.bar + 1);
+    __threadfence();
+    const unsigned arrived = atomicAdd(a.bar, 1u);
+    s_state = (arrived == (unsigned)a.bar_expect - 1u) ? 1 : 0;
+  }
+  __syncthreads();
+  if (s_state == 1) {
+    if (threadIdx.x < 32) {
+      __threadfence();
+      const double *src = a.cta_err + (size_t)(it & 1) * G;
+      double t = 0.0;
+      for (unsigned i = threadIdx.x; i < G; i += 32) t += __ldcg(src + i);
+      t = warp_sum(t);
+      if (threadIdx.x == 0) {
+        a.err_hist[it] = t;
+        atomicExch(a.bar, 0u);
+        __threadfence();
+        atomicAdd(a.bar + 1, 1u);
+      }
+    }
+  } else if (threadIdx.x == 0) {
+    const long long t0 = global_ns();
+    unsigned spins = 0;
+    while (ld_acquire(a.bar + 1) == s_gen) {
+      if ((++spins & 31u) == 0 && global_ns() - t0 > a.timeout_ns) {
+        atomicOr(a.status, 1);
+        s_state = 2;
+        break;
+      }
+      __nanosleep(100);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return s_state != 2;
+}
+
+// All sweeps in one cooperative launch.
+__global__ void __launch_bounds__(gpr::kBlock) k_pr_persistent(PrArgs a) {
+  const int lane = threadIdx.x & 31;
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  const uint64_t pol = evict_first_policy();
+  int it = 0;
+  while (it < a.max_iter) {
+    const float *cin = (it & 1) ? a.c1 : a.c0;
+    float *cout = (it & 1) ? a.c0 : a.c1;
+    const double err = sweep(a, cin, cout, gw, nw, lane, pol);
+    const double tot = block_sum(err);
+    if (!barrier_reduce(a, it, tot)) return;
+    const double total = __ldcg(a.err_hist + it);
+    ++it;
+    if (total < a.tol) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.status[1] = it;
+    a.status[2] = 1;
+  }
+}
+
+// One sweep per launch (graph mode).  The sweep index and the done flag live
+// in device memory, so a captured sequence of launches needs no host input;
+// launches after convergence return at once.
+__global__ void __launch_bounds__(gpr::kBlock) k_pr_step(PrArgs a) {
+  __shared__ int s_it, s_last;
+  if (threadIdx.x == 0) {
+    const int done = *(volatile int *)(a.status + 2);
+    s_it = done ? -1 : *(volatile int *)(a.status + 1);
+  }
+  __syncthreads();
+  const int it = s_it;
+  if (it < 0) return;
+  const int lane = threadIdx.x & 31;
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  const uint64_t pol = evict_first_policy();
+  const float *cin = (it & 1) ? a.c1 : a.c0;
+  float *cout = (it & 1) ? a.c0 : a.c1;
+  const double err = sweep(a, cin, cout, gw, nw, lane, pol);
+  const double tot = block_sum(err);
+  if (threadIdx.x == 0) {
+    a.cta_err[blockIdx.x] = tot;
+    __threadfence();
+    s_last = atomicAdd(a.bar, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x < 32) {
+    __threadfence();
+    double t = 0.0;
+    for (unsigned i = threadIdx.x; i < gridDim.x; i += 32) t += __ldcg(a.cta_err + i);
+    t = warp_sum(t);
+    if (threadIdx.x == 0) {
+      a.err_hist[it] = t;
+      atomicExch(a.bar, 0u);
+      a.status[1] = it + 1;
+      if (t < a.tol || it + 1 >= a.max_iter) a.status[2] = 1;
+      __threadfence();
+    }
+  }
+}
+
+// Scores into the relabelled order and the first sweep's contributions.
+__global__ void k_pr_prologue(int m, const int *__restrict__ perm, const int *__restrict__ outdeg,
+                              const float *__restrict__ scores_in, float *s, float *c0,
+                              float *c1) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) {
+    const float v = scores_in[perm[i]];
+    s[i] = v;
+    c0[i] = __fdiv_rn(v, __int2float_rn(outdeg[i]));
+  } else if (i == m) {
+    c0[m] = 0.f;  // sentinel slots of the padding entries
+    c1[m] = 0.f;
+  }
+}
+
+__global__ void k_pr_scatter(int m, const int *__restrict__ perm, const float *__restrict__ s,
+                             float *scores_out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) scores_out[perm[i]] = s[i];
+}
+
+// ---- FP64 residual (a-posteriori bound) ------------------------------------
+__global__ void k_res_prologue(int m, const int *__restrict__ perm, const int *__restrict__ outdeg,
+                               const float *__restrict__ scores, double *cd, double *sd) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) {
+    const double v = (double)scores[perm[i]];
+    sd[i] = v;
+    cd[i] = v / (double)outdeg[i];
+  } else if (i == m) {
+    cd[m] = 0.0;
+  }
+}
+
+__global__ void k_res_sweep(PrArgs a, const double *__restrict__ cd, const double *__restrict__ sd,
+                            double d, double base, double *long_acc, double *out) {
+  const int lane = threadIdx.x & 31;
+  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  const long long u1 = a.n_chunks, u2 = u1 + a.n_slices, u3 = u2 + a.n_zblk;
+  double err = 0.0;
+  for (long long u = gw; u < u3; u += nw) {
+    if (u < u1) {
+      const int c = (int)u, r = a.chunk_row[c];
+      const int cb = a.row_cbeg[r];
+      const long long b = a.long_ptr[r] + (long long)(c - cb) * a.chunk;
+      const long long e = min(b + (long long)a.chunk, a.long_ptr[r + 1]);
+      double acc = 0.0;
+      for (long long k = b + lane; k < e; k += 32) acc += cd[a.long_col[k]];
+      acc = warp_sum(acc);
+      if (lane == 0) atomicAdd(long_acc + r, acc);
+    } else if (u < u2) {
+      const int sidx = (int)(u - u1);
+      const long long b = a.slice_ptr[sidx];
+      const int len = (int)((a.slice_ptr[sidx + 1] - b) >> 5);
+      double acc = 0.0;
+      for (int j = 0; j < len; ++j) acc += cd[a.sell_col[b + 32LL * j + lane]];
+      const int r = a.n_long + sidx * 32 + lane;
+      if (r < a.n_nz) err += fabs(base + d * acc - sd[r]);
+    } else {
+      const int r0 = a.n_nz + (int)(u - u2) * gpr::kZeroRowsPerUnit;
+      for (int q = 0; q < gpr::kZeroRowsPerUnit / 32; ++q) {
+        const int r = r0 + 32 * q + lane;
+        if (r < a.m) err += fabs(base - sd[r]);
+      }
+    }
+  }
+  err = warp_sum(err);
+  if (lane == 0) atomicAdd(out, err);
+}
+
+__global__ void k_res_long(int n_long, const double *__restrict__ long_acc,
+                           const double *__restrict__ sd, double d, double base, double *out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  double e = 0.0;
+  if (r < n_long) e = fabs(base + d * long_acc[r] - sd[r]);
+  e = warp_sum(e);
+  if ((threadIdx.x & 31) == 0) atomicAdd(out, e);
+}
+
+inline unsigned grid_for(long long n, int block = 256) {
+  long long g = (n + block - 1) / block;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+PrArgs make_args(gpr_graph *g, const gpr_pr_opts &o) {
+  const PrLayout &L = g->L;
+  PrArgs a;
+  a.m = L.m;
+  a.n_long = L.n_long;
+  a.n_nz = L.n_nz;
+  a.n_chunks = L.n_chunks;
+  a.n_slices = L.n_slices;
+  a.n_zblk = L.n_zblk;
+  a.chunk = L.chunk;
+  a.long_ptr = L.long_ptr;
+  a.long_col = L.long_col;
+  a.row_cbeg = L.row_cbeg;
+  a.chunk_row = L.chunk_row;
+  a.slice_ptr = L.slice_ptr;
+  a.sell_col = L.sell_col;
+  a.outdeg = L.outdeg;
+  a.s = g->s;
+  a.c0 = g->c0;
+  a.c1 = g->c1;
+  a.partial = g->partial;
+  a.cnt = g->cnt;
+  a.cta_err = g->cta_err;
+  a.err_hist = g->err_hist;
+  a.bar = g->bar;
+  a.status = g->status;
+  a.damp = o.damping;
+  a.base = (1.0f - o.damping) / (float)L.m;  // src/pr/omp_base.cc:16
+  a.tol = o.tol;
+  a.max_iter = o.max_iter;
+  a.bar_expect = g->grid_persist;
+  a.timeout_ns = (long long)(o.timeout_s * 1e9);
+  return a;
+}
+
+void destroy(gpr_graph *g) {
+  if (!g) return;
+  gpr::free_pr_layout(&g->L);
+  gpr::dfree(g->s);
+  gpr::dfree(g->c0);
+  gpr::dfree(g->c1);
+  gpr::dfree(g->partial);
+  gpr::dfree(g->cnt);
+  gpr::dfree(g->cta_err);
+  gpr::dfree(g->err_hist);
+  gpr::dfree(g->bar);
+  gpr::dfree(g->status);
+  gpr::dfree(g->scores_tmp);
+  gpr::dfree(g->res_tmp);
+  if (g->e0) cudaEventDestroy(g->e0);
+  if (g->e1) cudaEventDestroy(g->e1);
+  if (g->e2) cudaEventDestroy(g->e2);
+  if (g->e3) cudaEventDestroy(g->e3);
+  if (g->own_stream && g->st) cudaStreamDestroy(g->st);
+  delete g;
+}
+
+int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
+                const int *any_outdeg, gpr_graph *g) {
+  GPR_CUDA(cudaGetDevice(&g->device));
+  GPR_CUDA(cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking));
+  g->own_stream = true;
+  GPR_CUDA(cudaEventCreate(&g->e0));
+  GPR_CUDA(cudaEventCreate(&g->e1));
+  GPR_CUDA(cudaEventCreate(&g->e2));
+  GPR_CUDA(cudaEventCreate(&g->e3));
+  cudaStream_t st = g->st;
+  void *rp = nullptr, *cp = nullptr, *dp = nullptr;
+  bool orp = false, ocp = false, odp = false;
+  int rc = gpr::to_device(any_rowptr, sizeof(int) * ((size_t)m + 1), &rp, &orp, st, "rowptr");
+  if (rc == GPR_OK) rc = gpr::to_device(any_col, sizeof(int) * (size_t)nnz, &cp, &ocp, st, "col");
+  if (rc == GPR_OK)
+    rc = gpr::to_device(any_outdeg, sizeof(int) * (size_t)m, &dp, &odp, st, "outdeg");
+  if (rc == GPR_OK)
+    rc = gpr::validate_csr(m, nnz, m, (const int *)rp, (const int *)cp, (const int *)dp, st);
+  if (rc == GPR_OK)
+    rc = gpr::build_pr_layout(m, nnz, (const int *)rp, (const int *)cp, (const int *)dp,
+                              gpr::kSellMaxDefault, gpr::kChunkDefault, &g->L, st);
+  cudaStreamSynchronize(st);
+  if (orp) cudaFree(rp);
+  if (ocp) cudaFree(cp);
+  if (odp) cudaFree(dp);
+  GPR_TRY(rc);
+  const PrLayout &L = g->L;
+  GPR_TRY(gpr::dalloc(&g->s, (size_t)m, "scores"));
+  GPR_TRY(gpr::dalloc(&g->c0, (size_t)m + 1, "contrib0"));
+  GPR_TRY(gpr::dalloc(&g->c1, (size_t)m + 1, "contrib1"));
+  GPR_TRY(gpr::dalloc(&g->partial, (size_t)L.n_chunks, "chunk partials"));
+  GPR_TRY(gpr::dalloc(&g->cnt, (size_t)L.n_long, "chunk counters"));
+  GPR_TRY(gpr::dalloc(&g->bar, 4, "barrier"));
+  GPR_TRY(gpr::dalloc(&g->status, 4, "status"));
+  GPR_TRY(gpr::dalloc(&g->scores_tmp, (size_t)m, "score staging"));
+  GPR_CUDA(cudaMemsetAsync(g->cnt, 0, sizeof(int) * (L.n_long ? L.n_long : 1), st));
+
+  int sms = 0, coop = 0, per_sm = 0;
+  GPR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+  GPR_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, g->device));
+  GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pr_persistent, gpr::kBlock, 0));
+  const long long units = (long long)L.n_chunks + L.n_slices + L.n_zblk;
+  const long long warps_per_cta = gpr::kBlock / 32;
+  const long long need = gpr::ceil_div(units, warps_per_cta);
+  long long full = (long long)sms * (per_sm > 0 ? per_sm : 1);
+  g->coop = coop != 0 && per_sm > 0;
+  g->grid_persist = (int)(need < full ? (need < 1 ? 1 : need) : full);
+  long long step = need < 1 ? 1 : need;
+  if (step > full * 4) step = full * 4;
+  g->grid_step = (int)step;
+  g->max_grid = g->grid_persist > g->grid_step ? g->grid_persist : g->grid_step;
+  GPR_TRY(gpr::dalloc(&g->cta_err, 2 * (size_t)g->max_grid, "cta residuals"));
+  g->err_cap = 128;
+  GPR_TRY(gpr::dalloc(&g->err_hist, (size_t)g->err_cap, "residual history"));
+  GPR_CUDA(cudaStreamSynchronize(st));
+  return GPR_OK;
+}
+
+int pagerank_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts_in,
+                  gpr_pr_stats *stats) {
+  gpr_pr_opts o;
+  if (opts_in) o = *opts_in;
+  else gpr_pr_opts_default(&o);
+  if (!(o.damping >= 0.f && o.damping <= 1.f) || o.max_iter < 0 || !(o.tol >= 0.0) ||
+      !(o.timeout_s > 0.0)) {
+    gpr::set_error("gpr_pagerank: invalid options (damping %g, tol %g, max_iter %d, timeout %g)",
+                   (double)o.damping, o.tol, o.max_iter, o.timeout_s);
+    return GPR_EINVAL;
+  }
+  if (o.precision != GPR_PREC_FP32) {
+    gpr::set_error("gpr_pagerank: precision %d not available in this build", o.precision);
+    return GPR_EUNSUPPORTED;
+  }
+  const int m = g->L.m;
+  gpr_pr_stats st_local;
+  memset(&st_local, 0, sizeof(st_local));
+  if (m == 0 || any_scores == nullptr) {
+    if (stats) *stats = st_local;
+    if (m != 0) {
+      gpr::set_error("gpr_pagerank: NULL scores");
+      return GPR_EINVAL;
+    }
+    return GPR_OK;
+  }
+  cudaStream_t st = g->st;
+  if (o.max_iter > g->err_cap) {
+    gpr::dfree(g->err_hist);
+    g->err_hist = nullptr;
+    g->err_cap = o.max_iter;
+    GPR_TRY(gpr::dalloc(&g->err_hist, (size_t)g->err_cap, "residual history"));
+  }
+  float *d_scores = any_scores;
+  const bool host = !gpr::is_device_ptr(any_scores);
+  if (host) {
+    d_scores = g->scores_tmp;
+    GPR_CUDA(cudaMemcpyAsync(d_scores, any_scores, sizeof(float) * (size_t)m,
+                             cudaMemcpyHostToDevice, st));
+  }
+  GPR_CUDA(cudaMemsetAsync(g->bar, 0, 4 * sizeof(unsigned), st));
+  GPR_CUDA(cudaMemsetAsync(g->status, 0, 4 * sizeof(int), st));
+  if (g->L.n_long) GPR_CUDA(cudaMemsetAsync(g->cnt, 0, sizeof(int) * g->L.n_long, st));
+  PrArgs a = make_args(g, o);
+  if (o.reserved[0] > 0) a.bar_expect += o.reserved[0];  // test hook: a barrier nobody completes
+  int launches = 0;
+  GPR_CUDA(cudaEventRecord(g->e0, st));
+  k_pr_prologue<<<grid_for((long long)m + 1), 256, 0, st>>>(m, g->L.perm, g->L.outdeg, d_scores,
+                                                           g->s, g->c0, g->c1);
+  ++launches;
+  int loop = o.loop;
+  if (loop == GPR_LOOP_AUTO) loop = GPR_LOOP_PERSISTENT;
+  if (loop == GPR_LOOP_PERSISTENT && !g->coop) loop = GPR_LOOP_GRAPH;
+  GPR_CUDA(cudaEventRecord(g->e2, st));
+  if (o.max_iter > 0) {
+    if (loop == GPR_LOOP_PERSISTENT) {
+      void *args[] = {&a};
+      cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_pr_persistent,
+                                                  dim3(g->grid_persist), dim3(gpr::kBlock), args,
+                                                  0, st);
+      if (e == cudaErrorCooperativeLaunchTooLarge) {
+        cudaGetLastError();
+        loop = GPR_LOOP_GRAPH;
+      } else if (e != cudaSuccess) {
+        gpr::set_error("cooperative launch: %s", cudaGetErrorString(e));
+        return GPR_ECUDA;
+      } else {
+        ++launches;
+      }
+    }
+    if (loop == GPR_LOOP_GRAPH) {
+      const int batch = 8;
+      int done = 0, issued = 0;
+      while (!done && issued < o.max_iter) {
+        for (int q = 0; q < batch && issued < o.max_iter; ++q, ++issued) {
+          k_pr_step<<<g->grid_step, gpr::kBlock, 0, st>>>(a);
+          ++launches;
+        }
+        GPR_CUDA(cudaGetLastError());
+        GPR_CUDA(cudaMemcpyAsync(&done, g->status + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+        GPR_CUDA(cudaStreamSynchronize(st));
+      }
+    }
+  }
+  GPR_CUDA(cudaEventRecord(g->e3, st));
+  k_pr_scatter<<<grid_for(m), 256, 0, st>>>(m, g->L.perm, g->s, d_scores);
+  ++launches;
+  GPR_CUDA(cudaGetLastError());
+  GPR_CUDA(cudaEventRecord(g->e1, st));
+  int hs[4];
+  GPR_CUDA(cudaMemcpyAsync(hs, g->status, sizeof(hs), cudaMemcpyDeviceToHost, st));
+  GPR_CUDA(cudaStreamSynchronize(st));
+  float ms = 0.f, lms = 0.f;
+  GPR_CUDA(cudaEventElapsedTime(&ms, g->e0, g->e1));
+  GPR_CUDA(cudaEventElapsedTime(&lms, g->e2, g->e3));
+  st_local.loop_ms = lms;
+  st_local.iterations = hs[1];
+  g->last_sweeps = hs[1];
+  st_local.solve_ms = ms;
+  st_local.gpu_launches = launches;
+  if (hs[1] > 0)
+    GPR_CUDA(cudaMemcpy(&st_local.residual, g->err_hist + hs[1] - 1, sizeof(double),
+                        cudaMemcpyDeviceToHost));
+  if (host)
+    GPR_CUDA(cudaMemcpy(any_scores, d_scores, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost));
+  if (stats) *stats = st_local;
+  if (hs[0] & 1) {
+    gpr::set_error("grid barrier wait exceeded %.3f s (sweep loop abandoned)", o.timeout_s);
+    return GPR_ETIMEOUT;
+  }
+  return GPR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int gpr_graph_create(int m, long long nnz, const int *any_rowptr, const int *any_col,
+                     const int *any_outdeg, gpr_graph **out) {
+  if (!out) {
+    gpr::set_error("gpr_graph_create: NULL out");
+    return GPR_EINVAL;
+  }
+  *out = nullptr;
+  if (m < 0 || nnz < 0 || nnz > 0x7fffffffLL || (m > 0 && (!any_rowptr || !any_outdeg)) ||
+      (nnz > 0 && !any_col)) {
+    gpr::set_error("gpr_graph_create: invalid arguments (m=%d nnz=%lld)", m, nnz);
+    return GPR_EINVAL;
+  }
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    gpr::set_error("gpr_graph_create: no CUDA device");
+    return GPR_ENODEV;
+  }
+  gpr_graph *g = new gpr_graph();
+  int rc = create_impl(m, nnz, any_rowptr, any_col, any_outdeg, g);
+  if (rc != GPR_OK) {
+    destroy(g);
+    return rc;
+  }
+  *out = g;
+  return GPR_OK;
+}
+
+int gpr_graph_destroy(gpr_graph *g) {
+  destroy(g);
+  return GPR_OK;
+}
+
+int gpr_graph_info(const gpr_graph *g, int *m, long long *nnz, long long *device_bytes) {
+  if (!g) {
+    gpr::set_error("gpr_graph_info: NULL graph");
+    return GPR_EINVAL;
+  }
+  if (m) *m = g->L.m;
+  if (nnz) *nnz = g->L.nnz;
+  if (device_bytes) *device_bytes = g->L.device_bytes + 12LL * g->L.m;
+  return GPR_OK;
+}
+
+int gpr_graph_set_stream(gpr_graph *g, void *stream) {
+  if (!g) {
+    gpr::set_error("gpr_graph_set_stream: NULL graph");
+    return GPR_EINVAL;
+  }
+  if (g->own_stream && g->st) cudaStreamDestroy(g->st);
+  g->own_stream = false;
+  g->st = (cudaStream_t)stream;
+  return GPR_OK;
+}
+
+int gpr_graph_layout(const gpr_graph *g, int *n_long, int *n_nz, int *n_chunks, int *n_slices,
+                     long long *long_elems, long long *sell_elems) {
+  if (!g) {
+    gpr::set_error("gpr_graph_layout: NULL graph");
+    return GPR_EINVAL;
+  }
+  if (n_long) *n_long = g->L.n_long;
+  if (n_nz) *n_nz = g->L.n_nz;
+  if (n_chunks) *n_chunks = g->L.n_chunks;
+  if (n_slices) *n_slices = g->L.n_slices;
+  if (long_elems) *long_elems = g->L.long_elems;
+  if (sell_elems) *sell_elems = g->L.sell_elems;
+  return GPR_OK;
+}
+
+int gpr_graph_residuals(const gpr_graph *g, double *h_out, int n) {
+  if (!g || (n > 0 && !h_out)) {
+    gpr::set_error("gpr_graph_residuals: NULL argument");
+    return GPR_EINVAL;
+  }
+  const int k = n < g->last_sweeps ? n : g->last_sweeps;
+  if (k > 0)
+    GPR_CUDA(cudaMemcpy(h_out, g->err_hist, sizeof(double) * (size_t)k, cudaMemcpyDeviceToHost));
+  return GPR_OK;
+}
+
+int gpr_pagerank(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts, gpr_pr_stats *stats) {
+  if (!g) {
+    gpr::set_error("gpr_pagerank: NULL graph");
+    return GPR_EINVAL;
+  }
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != g->device) GPR_CUDA(cudaSetDevice(g->device));
+  int rc = pagerank_impl(g, any_scores, opts, stats);
+  if (cur != g->device && cur >= 0) cudaSetDevice(cur);
+  return rc;
+}
+
+int gpr_pr_residual_f64(gpr_graph *g, const float *any_scores, float damping, double *residual) {
+  if (!g || !any_scores || !residual) {
+    gpr::set_error("gpr_pr_residual_f64: NULL argument");
+    return GPR_EINVAL;
+  }
+  const PrLayout &L = g->L;
+  const int m = L.m;
+  cudaStream_t st = g->st;
+  void *dv = nullptr;
+  bool owned = false;
+  GPR_TRY(gpr::to_device(any_scores, sizeof(float) * (size_t)m, &dv, &owned, st, "scores"));
+  if (!g->res_tmp) {
+    int rc = gpr::dalloc(&g->res_tmp, 2 * (size_t)m + 2 + L.n_long, "residual scratch");
+    if (rc != GPR_OK) {
+      if (owned) cudaFree(dv);
+      return rc;
+    }
+  }
+  double *cd = g->res_tmp, *sd = g->res_tmp + m + 1, *acc = sd + m, *out = acc + L.n_long;
+  gpr_pr_opts o;
+  gpr_pr_opts_default(&o);
+  o.damping = damping;
+  PrArgs a = make_args(g, o);
+  const double d = (double)damping, base = (1.0 - d) / (double)m;
+  cudaMemsetAsync(acc, 0, sizeof(double) * ((size_t)L.n_long + 1), st);
+  k_res_prologue<<<grid_for((long long)m + 1), 256, 0, st>>>(m, L.perm, L.outdeg,
+                                                             (const float *)dv, cd, sd);
+  const long long units = (long long)L.n_chunks + L.n_slices + L.n_zblk;
+  k_res_sweep<<<grid_for(units * 32), 256, 0, st>>>(a, cd, sd, d, base, acc, out);
+  if (L.n_long) k_res_long<<<grid_for(L.n_long), 256, 0, st>>>(L.n_long, acc, sd, d, base, out);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(residual, out, sizeof(double), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (owned) cudaFree(dv);
+  if (e != cudaSuccess) {
+    gpr::set_error("gpr_pr_residual_f64: %s", cudaGetErrorString(e));
+    return GPR_ECUDA;
+  }
+  return GPR_OK;
+}
+
+int gpr_page_rank(int m, int nnz, const int *row_offsets, const int *column_indices,
+                  const int *degree, float *scores, const gpr_pr_opts *opts,
+                  gpr_pr_stats *stats) {
+  gpr_graph *g = nullptr;
+  GPR_TRY(gpr_graph_create(m, nnz, row_offsets, column_indices, degree, &g));
+  int rc = gpr_pagerank(g, scores, opts, stats);
+  gpr_graph_destroy(g);
+  return rc;
+}
+
+int gpr_pr_solver(int m, int nnz, const int *in_row_offsets, const int *in_column_indices,
+                  const int *out_row_offsets, const int *out_column_indices, const int *degree,
+                  float *scores, const gpr_pr_opts *opts, gpr_pr_stats *stats) {
+  (void)out_row_offsets;  // pull variants ignore the out-CSR (src/pr/gather.cu:41)
+  (void)out_column_indices;
+  return gpr_page_rank(m, nnz, in_row_offsets, in_column_indices, degree, scores, opts, stats);
+}
+
+}  // extern "C"

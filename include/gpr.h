@@ -1,0 +1,174 @@
+/*
+ * gpr.h -- C ABI of the B200 pull-PageRank / CSR-SpMV library (libgpr.so).
+ *
+ * Plain pointers and sizes only; every entry point returns a gpr_status and
+ * never exits the process.  gpr_last_error() gives a message for the last
+ * failure on the calling thread.
+ *
+ * The reference (Gardenia, src/pr and src/spmv) has no C ABI: its boundary is
+ * the link-time C++ symbol PRSolver / SpmvSolver chosen by the Makefile
+ * (src/pr/Makefile:17-47, src/spmv/Makefile:16-50).  The C++ drop-ins with
+ * those exact signatures are declared in gardenia_pr.h / gardenia_spmv.h and
+ * are thin wrappers over the functions below.  Each function here cites the
+ * reference interface it replaces.
+ *
+ * Pointers named h_* are host memory; d_* are device memory on the current
+ * CUDA device; "any" pointers may be either (the library checks with
+ * cudaPointerGetAttributes and copies when needed).  Streams are passed as
+ * void* (a cudaStream_t; NULL = the legacy default stream).
+ */
+#ifndef GPR_H_
+#define GPR_H_
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  GPR_OK = 0,
+  GPR_EINVAL = 1,     /* bad argument or malformed CSR */
+  GPR_ENOMEM = 2,     /* device or host allocation failed */
+  GPR_ECUDA = 3,      /* a CUDA runtime call failed */
+  GPR_ETIMEOUT = 4,   /* a bounded device-side wait ran out */
+  GPR_ENODEV = 5,     /* no usable CUDA device */
+  GPR_EUNSUPPORTED = 6
+} gpr_status;
+
+/* Precision of the stored / gathered contributions. */
+typedef enum {
+  GPR_PREC_FP32 = 0,  /* plain form: FP32 everywhere, FP64 residual */
+  GPR_PREC_BF16 = 1,  /* BF16 contributions, FP32 accumulation, FP32 refinement */
+  GPR_PREC_FP16 = 2   /* FP16 contributions with per-iteration power-of-two scaling */
+} gpr_precision;
+
+/* How the iteration loop is driven. */
+typedef enum {
+  GPR_LOOP_AUTO = 0,        /* pick from the graph size */
+  GPR_LOOP_PERSISTENT = 1,  /* one cooperative launch, bounded grid barrier per sweep */
+  GPR_LOOP_GRAPH = 2        /* one launch per sweep, captured into a CUDA graph */
+} gpr_loop;
+
+typedef struct {
+  float damping;        /* kDamp, include/common.h:18 (0.85f) */
+  double tol;           /* EPSILON, src/pr/pr.h:4 (1e-3); stop when the sweep's L1 change < tol */
+  int max_iter;         /* MAX_ITER, src/pr/pr.h:5 (30) */
+  int precision;        /* gpr_precision */
+  int loop;             /* gpr_loop */
+  double timeout_s;     /* bound on every device-side wait (grid barrier); default 5 s */
+  int refine_max;       /* mixed precision: max FP32 refinement sweeps (default 64) */
+  int reserved[8];
+} gpr_pr_opts;
+
+typedef struct {
+  int iterations;       /* sweeps executed (the reference prints the same number, gather.cu:83) */
+  int refine_iterations;/* FP32 sweeps spent in the refinement tail (mixed precision) */
+  double residual;      /* L1 change of the last sweep (FP64) */
+  double solve_ms;      /* device time of the solve (CUDA events), excluding copies */
+  double loop_ms;       /* device time of the sweep loop alone (persistent kernel or step launches) */
+  int gpu_launches;     /* kernels launched by this solve */
+  int reserved[5];
+} gpr_pr_stats;
+
+typedef struct gpr_graph gpr_graph;    /* device-resident pull graph (PR) */
+typedef struct gpr_matrix gpr_matrix;  /* device-resident CSR matrix (SpMV) */
+
+/* ---- library ---------------------------------------------------------- */
+const char *gpr_last_error(void);
+const char *gpr_version(void);
+int gpr_pr_opts_default(gpr_pr_opts *opts);
+
+/* ---- PageRank graph ------------------------------------------------------
+ * Pull graph from the in-CSR (row v lists the sources u of edges u->v) and
+ * the out-degree of every vertex: the arguments the reference's pull solver
+ * reads (src/pr/omp_base.cc:9, row_offsets / column_indices / degree).
+ * The library keeps its own relabelled device copy; the caller's arrays are
+ * not retained. */
+int gpr_graph_create(int m, long long nnz, const int *any_rowptr,
+                     const int *any_col, const int *any_outdeg,
+                     gpr_graph **out);
+int gpr_graph_destroy(gpr_graph *g);
+int gpr_graph_info(const gpr_graph *g, int *m, long long *nnz,
+                   long long *device_bytes);
+/* Bin sizes of the relabelled layout (rows > sell_max in-edges, rows with
+ * any in-edge, long-row chunks, SELL slices, stored edge slots). */
+int gpr_graph_layout(const gpr_graph *g, int *n_long, int *n_nz, int *n_chunks,
+                     int *n_slices, long long *long_elems, long long *sell_elems);
+/* Run later solves on `stream` (a cudaStream_t owned by the caller) instead
+ * of the graph's own stream. */
+int gpr_graph_set_stream(gpr_graph *g, void *stream);
+/* Per-sweep L1 residuals of the last solve (the numbers the reference prints
+ * each iteration, src/pr/omp_base.cc:42).  Copies min(n, sweeps) values. */
+int gpr_graph_residuals(const gpr_graph *g, double *h_out, int n);
+
+/* Solve.  scores (host or device, m floats) holds the initial scores on
+ * entry and the result on return, like the reference's scores argument
+ * (src/pr/omp_base.cc:9, src/pr/main.cc:26-29).  Synchronous. */
+int gpr_pagerank(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts,
+                 gpr_pr_stats *stats);
+
+/* FP64 L1 residual || base + d*M*s - s ||_1 of a score vector on the GPU;
+ * ||s - s*||_1 <= residual / (1 - d) bounds the distance to the fixed point. */
+int gpr_pr_residual_f64(gpr_graph *g, const float *any_scores, float damping,
+                        double *residual);
+
+/* ---- reference-shaped one-shot calls (host arrays in, results in place) -- */
+/* PRSolver, src/pr/pr.h:23.  The out-CSR is accepted and ignored, as in the
+ * pull variants (src/pr/omp_base.cc:9, src/pr/gather.cu:41). */
+int gpr_pr_solver(int m, int nnz, const int *in_row_offsets,
+                  const int *in_column_indices, const int *out_row_offsets,
+                  const int *out_column_indices, const int *degree,
+                  float *scores, const gpr_pr_opts *opts, gpr_pr_stats *stats);
+/* PageRank(m, nnz, row_offsets, column_indices, degree, scores): the pull
+ * entry point named for this path (in-CSR + out-degree), same contract. */
+int gpr_page_rank(int m, int nnz, const int *row_offsets,
+                  const int *column_indices, const int *degree, float *scores,
+                  const gpr_pr_opts *opts, gpr_pr_stats *stats);
+
+/* ---- SpMV ------------------------------------------------------------------
+ * y <- y + A*x over a CSR matrix (src/spmv/spmv.h:29, omp_base.cc:8-32). */
+int gpr_matrix_create(int m, long long nnz, const int *any_Ap,
+                      const int *any_Aj, const float *any_Ax, gpr_matrix **out);
+int gpr_matrix_destroy(gpr_matrix *A);
+int gpr_matrix_layout(const gpr_matrix *A, int *n_long, int *n_chunks,
+                      int *n_slices, long long *sell_elems);
+/* x, y on the device; asynchronous on `stream`. */
+int gpr_spmv(gpr_matrix *A, const float *d_x, float *d_y, void *stream);
+/* SpmvSolver, src/spmv/spmv.h:29: host arrays, y updated in place. */
+int gpr_spmv_solver(int m, int nnz, const int *Ap, const int *Aj,
+                    const float *Ax, const float *x, float *y);
+
+/* ---- graph construction on the GPU (inputs for the solvers) ------------- */
+/* Seeded RMAT pull graph (self-loops and duplicates removed, columns
+ * ascending): fills device arrays allocated by the library; release with
+ * gpr_free.  a,b,c are the quadrant probabilities (d = 1-a-b-c). */
+int gpr_gen_rmat(int scale, int edge_factor, double a, double b, double c,
+                 unsigned long long seed, int scramble, int **d_rowptr,
+                 int **d_col, int **d_outdeg, long long *nnz);
+/* 27-point Laplacian on an n^3 grid (26 / -1), natural ordering. */
+int gpr_gen_stencil27(int n, int **d_Ap, int **d_Aj, float **d_Ax,
+                      long long *nnz);
+/* Seeded uniform [0,1) floats (24 random bits). */
+int gpr_gen_uniform(long long n, unsigned long long seed, float *d_out);
+int gpr_free(void *d_ptr);
+/* Device allocation / copy helpers for callers without a CUDA runtime of
+ * their own (copies use cudaMemcpyDefault: any direction). */
+int gpr_malloc(void **d_ptr, size_t bytes);
+int gpr_memcpy(void *dst, const void *src, size_t bytes);
+int gpr_synchronize(void);
+
+/* ---- graph_io (host) ------------------------------------------------------
+ * read_graph of include/graph_io.h:280 for foreign callers: same parsers and
+ * flags as the C++ read_graph in gardenia_graph_io.h; arrays are malloc'd and
+ * released with gpr_read_graph_free. */
+int gpr_read_graph(const char *path, int symmetrize, int transpose, int sorted,
+                   int remove_selfloops, int remove_redundents, int *m, int *nnz,
+                   int **row_offsets, int **column_indices, int **degree,
+                   float **weight);
+void gpr_read_graph_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GPR_H_ */
