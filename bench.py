@@ -206,6 +206,7 @@ def run_ours(args):
     import gardenia_ocl_b200 as G
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
+    G.set_device(local)
     dist = None
     if world > 1:
         import datetime

@@ -38,7 +38,12 @@ class GprError(RuntimeError):
 class PrOptions(C.Structure):
     _fields_ = [("damping", C.c_float), ("tol", C.c_double), ("max_iter", C.c_int),
                 ("precision", C.c_int), ("loop", C.c_int), ("timeout_s", C.c_double),
-                ("refine_max", C.c_int), ("reserved", C.c_int * 8)]
+                ("refine_max", C.c_int), ("variant", C.c_int), ("reserved", C.c_int * 7)]
+
+
+class LayoutOptions(C.Structure):
+    _fields_ = [("sell_max", C.c_int), ("chunk", C.c_int), ("chunk_min", C.c_int),
+                ("reserved", C.c_int * 5)]
 
 
 class PrStats(C.Structure):
@@ -71,6 +76,8 @@ def lib():
         "gpr_version": (C.c_char_p, []),
         "gpr_pr_opts_default": (I, [C.POINTER(PrOptions)]),
         "gpr_graph_create": (I, [I, LL, _vp, _vp, _vp, C.POINTER(_vp)]),
+        "gpr_graph_create_ex": (I, [I, LL, _vp, _vp, _vp, C.POINTER(LayoutOptions),
+                                    C.POINTER(_vp)]),
         "gpr_graph_destroy": (I, [_vp]),
         "gpr_graph_info": (I, [_vp, C.POINTER(I), C.POINTER(LL), C.POINTER(LL)]),
         "gpr_graph_layout": (I, [_vp, C.POINTER(I), C.POINTER(I), C.POINTER(I), C.POINTER(I),
@@ -97,6 +104,7 @@ def lib():
         "gpr_malloc": (I, [C.POINTER(_vp), C.c_size_t]),
         "gpr_memcpy": (I, [_vp, _vp, C.c_size_t]),
         "gpr_synchronize": (I, []),
+        "gpr_set_device": (I, [I]),
         "gpr_read_graph": (I, [C.c_char_p, I, I, I, I, I, C.POINTER(I), C.POINTER(I),
                                C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
         "gpr_read_graph_free": (None, [_vp]),
@@ -137,11 +145,12 @@ def _ptr(a, dtype=None):
 
 
 def options(tol=EPSILON, max_iter=MAX_ITER, damping=KDAMP, precision=PREC_FP32,
-            loop=LOOP_AUTO, timeout_s=5.0, refine_max=64) -> PrOptions:
+            loop=LOOP_AUTO, timeout_s=5.0, refine_max=64, variant=0) -> PrOptions:
     o = PrOptions()
     _check(lib().gpr_pr_opts_default(C.byref(o)))
     o.tol, o.max_iter, o.damping = float(tol), int(max_iter), float(damping)
     o.precision, o.loop, o.timeout_s, o.refine_max = int(precision), int(loop), float(timeout_s), int(refine_max)
+    o.variant = int(variant)
     return o
 
 
@@ -186,7 +195,7 @@ class Graph:
     """Device-resident pull graph: in-CSR (row v = sources of edges u->v) plus
     the out-degree of every vertex (src/pr/omp_base.cc:9 arguments)."""
 
-    def __init__(self, rowptr, col, outdeg, m=None, nnz=None):
+    def __init__(self, rowptr, col, outdeg, m=None, nnz=None, sell_max=0, chunk=0, chunk_min=0):
         L = lib()
         m = int(len(rowptr) - 1) if m is None else int(m)
         nnz = int(len(col)) if nnz is None else int(nnz)
@@ -194,7 +203,8 @@ class Graph:
         pc, k1 = _ptr(col, np.int32)
         pd, k2 = _ptr(outdeg, np.int32)
         h = C.c_void_p()
-        _check(L.gpr_graph_create(m, nnz, pr, pc, pd, C.byref(h)))
+        lo = LayoutOptions(int(sell_max), int(chunk), int(chunk_min))
+        _check(L.gpr_graph_create_ex(m, nnz, pr, pc, pd, C.byref(lo), C.byref(h)))
         self._h, self.m, self.nnz = h, m, nnz
         self.last_stats = None
 
@@ -389,6 +399,10 @@ def gen_stencil27(n) -> DeviceCSR:
 
 def gen_uniform(n, seed, d_out) -> None:
     _check(lib().gpr_gen_uniform(int(n), int(seed), _ptr(d_out)[0]))
+
+
+def set_device(device: int):
+    _check(lib().gpr_set_device(int(device)))
 
 
 def synchronize():

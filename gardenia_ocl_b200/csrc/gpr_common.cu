@@ -112,6 +112,11 @@ int gpr_memcpy(void *dst, const void *src, size_t bytes) {
   return GPR_OK;
 }
 
+int gpr_set_device(int device) {
+  GPR_CUDA(cudaSetDevice(device));
+  return GPR_OK;
+}
+
 int gpr_synchronize(void) {
   GPR_CUDA(cudaDeviceSynchronize());
   return GPR_OK;

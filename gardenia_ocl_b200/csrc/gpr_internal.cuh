@@ -33,24 +33,39 @@ int to_device(const void *any, size_t bytes, void **dev, bool *owned,
 // Pull-graph layout after relabelling vertices by descending in-degree.
 //
 //   new row i  <->  old vertex perm[i]
-//   rows [0, n_long)      in-degree > sell_max: CSR whose row starts are
+//   rows [0, n_long)      in-degree > chunk_min: CSR whose row starts are
 //                         16-byte aligned, each row cut into chunks of
 //                         `chunk` edges (one warp per chunk)
-//   rows [n_long, n_nz)   1 <= in-degree <= sell_max: SELL-32 slices, one
-//                         lane per row, column-major inside the slice, so a
-//                         lane sums its row in the original CSR order
+//   rows [n_long, n_nz)   1 <= in-degree <= chunk_min: SELL-32 slices in
+//                         width classes.  A class gives every row w lanes
+//                         (w = 32, 16, 8, 4, 2, 1, widest first), w being the
+//                         smallest power of two with ceil(deg / w) <= lane_max;
+//                         a slice holds 32/w consecutive rows, column-major:
+//                         element (j, lane) = edge j*w + (lane % w) of row
+//                         lane / w.  With w = 1 a lane sums its row in the
+//                         original CSR order.
 //   rows [n_nz, m)        in-degree 0
 //
 // Every padding entry of either edge array holds the sentinel index m, whose
 // contribution slot is kept at 0.
 // ---------------------------------------------------------------------------
+constexpr int kMaxCls = 6;
+
+struct PrClasses {
+  int n_cls = 0;
+  int lw[kMaxCls] = {0};          // log2(lanes per row) of each class
+  int row[kMaxCls + 1] = {0};     // first row of each class; row[n_cls] = n_nz
+  int slice[kMaxCls + 1] = {0};   // first slice of each class; slice[n_cls] = n_slices
+};
+
 struct PrLayout {
   int m = 0;
   long long nnz = 0;
   int n_long = 0, n_nz = 0;
-  int sell_max = 0, chunk = 0;
+  int lane_max = 0, chunk_min = 0, chunk = 0;
   int n_chunks = 0, n_slices = 0, n_zblk = 0;
   int max_row_chunks = 0;         // chunks of the longest row
+  PrClasses cls;
   int *perm = nullptr;            // [m] new -> old
   int *outdeg = nullptr;          // [m] out-degree in new order
   long long *long_ptr = nullptr;  // [n_long+1] padded offsets into long_col
@@ -63,9 +78,16 @@ struct PrLayout {
   long long device_bytes = 0;
 };
 
+// Class of slice s (classes are few; the scan is warp-uniform).
+__host__ __device__ inline int slice_class(const PrClasses &c, int s) {
+  int k = 0;
+  while (k + 1 < c.n_cls && s >= c.slice[k + 1]) ++k;
+  return k;
+}
+
 int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
-                    const int *d_outdeg, int sell_max, int chunk, PrLayout *L,
-                    cudaStream_t st);
+                    const int *d_outdeg, int lane_max, int chunk_min, int chunk,
+                    PrLayout *L, cudaStream_t st);
 void free_pr_layout(PrLayout *L);
 
 // Validates a device CSR (rowptr[0] = 0, monotone, rowptr[m] = nnz, every
@@ -123,8 +145,10 @@ void free_spmv_layout(SpmvLayout *L);
 
 namespace gpr {
 constexpr int kZeroRowsPerUnit = 128;  // rows per zero-in-degree work unit
-constexpr int kSellMaxDefault = 64;    // in-degree bound of the SELL bin
-constexpr int kChunkDefault = 2048;    // edges per long-row chunk (multiple of 128)
+constexpr int kSellMaxDefault = 64;    // SpMV: row length bound of the SELL bin;
+                                       // PR: max edges per lane in a SELL slice
+constexpr int kChunkMinDefault = 4096; // PR: rows with more in-edges are chunked
+constexpr int kChunkDefault = 4096;    // edges per long-row chunk (multiple of 128)
 constexpr int kBlock = 256;            // threads per CTA of the sweep kernels
 
 __host__ __device__ inline long long ceil_div(long long a, long long b) {

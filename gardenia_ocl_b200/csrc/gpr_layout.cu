@@ -41,14 +41,15 @@ __global__ void k_indeg_iota(int m, const int *__restrict__ rowptr, int *indeg, 
   }
 }
 
-// Sorted (descending) degrees -> n_long = #rows with deg > t, n_nz = #deg > 0.
-__global__ void k_bounds(int m, const int *__restrict__ sdeg, int t, int *out) {
+// Sorted (descending) degrees -> out[k] = number of rows with degree > th[k].
+__global__ void k_bounds(int m, const int *__restrict__ sdeg, const int *__restrict__ th, int nth,
+                         int *out) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= m) return;
   int d = sdeg[i];
   int dn = (i + 1 < m) ? sdeg[i + 1] : -1;
-  if (d > t && dn <= t) out[0] = i + 1;
-  if (d > 0 && dn <= 0) out[1] = i + 1;
+  for (int k = 0; k < nth; ++k)
+    if (d > th[k] && dn <= th[k]) out[k] = i + 1;
 }
 
 __global__ void k_relabel(int m, const int *__restrict__ perm, const int *__restrict__ outdeg,
@@ -100,33 +101,45 @@ __global__ void k_fill_long(int n_long, int m, const int *__restrict__ perm,
   }
 }
 
-__global__ void k_slice_lens(int n_slices, int n_long, const int *__restrict__ sdeg,
+// Slice s of class c: 32 >> lw rows starting at row0; its length is the
+// per-lane edge count of its first (longest) row.
+__global__ void k_slice_lens(int n_slices, PrClasses cls, const int *__restrict__ sdeg,
                              long long *slen) {
   int s = blockIdx.x * blockDim.x + threadIdx.x;
-  if (s < n_slices) slen[s] = 32LL * sdeg[n_long + 32LL * s];
-  else if (s == n_slices) slen[s] = 0;
+  if (s < n_slices) {
+    const int c = slice_class(cls, s);
+    const int lw = cls.lw[c];
+    const int row0 = cls.row[c] + ((s - cls.slice[c]) << (5 - lw));
+    slen[s] = 32LL * (((long long)sdeg[row0] + (1 << lw) - 1) >> lw);
+  } else if (s == n_slices) {
+    slen[s] = 0;
+  }
 }
 
-// One thread per (slice, lane).
-__global__ void k_fill_sell(int n_slices, int n_long, int n_nz, int m,
-                            const int *__restrict__ perm, const int *__restrict__ inv,
-                            const int *__restrict__ rowptr, const int *__restrict__ col,
-                            const int *__restrict__ sdeg, const long long *__restrict__ sptr,
-                            int *sell_col) {
+// One thread per (slice, lane): lane holds edges l, l+w, l+2w, ... of its row.
+__global__ void k_fill_sell(int n_slices, int m, PrClasses cls, const int *__restrict__ perm,
+                            const int *__restrict__ inv, const int *__restrict__ rowptr,
+                            const int *__restrict__ col, const int *__restrict__ sdeg,
+                            const long long *__restrict__ sptr, int *sell_col) {
   long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (t >= 32LL * n_slices) return;
-  int s = (int)(t >> 5), lane = (int)(t & 31);
-  long long base = sptr[s];
-  int len = (int)((sptr[s + 1] - base) >> 5);
-  long long r = n_long + 32LL * s + lane;
+  const int s = (int)(t >> 5), lane = (int)(t & 31);
+  const int c = slice_class(cls, s);
+  const int lw = cls.lw[c];
+  const int row0 = cls.row[c] + ((s - cls.slice[c]) << (5 - lw));
+  const int r = row0 + (lane >> lw), l = lane & ((1 << lw) - 1);
+  const long long base = sptr[s];
+  const int len = (int)((sptr[s + 1] - base) >> 5);
   int deg = 0;
   long long sb = 0;
-  if (r < n_nz) {
+  if (r < cls.row[c + 1]) {
     deg = sdeg[r];
     sb = rowptr[perm[r]];
   }
-  for (int j = 0; j < len; ++j)
-    sell_col[base + 32LL * j + lane] = (j < deg) ? inv[col[sb + j]] : m;
+  for (int j = 0; j < len; ++j) {
+    const long long e = ((long long)j << lw) + l;
+    sell_col[base + 32LL * j + lane] = (e < deg) ? inv[col[sb + e]] : m;
+  }
 }
 
 template <typename T>
@@ -192,12 +205,13 @@ int validate_csr(int m, long long nnz, int ncols, const int *d_rowptr, const int
 }
 
 int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
-                    const int *d_outdeg, int sell_max, int chunk, PrLayout *L,
+                    const int *d_outdeg, int lane_max, int chunk_min, int chunk, PrLayout *L,
                     cudaStream_t st) {
   *L = PrLayout();
   L->m = m;
   L->nnz = nnz;
-  L->sell_max = sell_max;
+  L->lane_max = lane_max;
+  L->chunk_min = chunk_min;
   L->chunk = chunk;
   if (m <= 0) return GPR_OK;
   Scratch S;
@@ -210,7 +224,7 @@ int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
   S.p[2] = sdeg;
   GPR_TRY(dalloc(&inv, m, "inverse permutation"));
   S.p[3] = inv;
-  GPR_TRY(dalloc(&bounds, 2, "bounds"));
+  GPR_TRY(dalloc(&bounds, 16, "bounds"));
   S.p[4] = bounds;
   GPR_TRY(dalloc(&L->perm, m, "permutation"));
   GPR_TRY(dalloc(&L->outdeg, m, "out-degree"));
@@ -230,14 +244,39 @@ int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
       return GPR_ECUDA;
     }
   }
-  GPR_CUDA(cudaMemsetAsync(bounds, 0, 2 * sizeof(int), st));
-  k_bounds<<<grid_for(m), 256, 0, st>>>(m, sdeg, sell_max, bounds);
+  // Degree thresholds, descending: chunked rows, then width classes
+  // w = 32 .. 1 (class w holds lane_max*w/2 < deg <= lane_max*w), then 0.
+  int th[8], nth = 0;
+  th[nth++] = chunk_min;
+  for (int lw = 4; lw >= 0; --lw) {
+    long long t = (long long)lane_max << lw;
+    th[nth++] = (int)(t < chunk_min ? t : chunk_min);
+  }
+  th[nth++] = 0;
+  GPR_CUDA(cudaMemsetAsync(bounds, 0, 16 * sizeof(int), st));
+  GPR_CUDA(cudaMemcpyAsync(bounds + 8, th, nth * sizeof(int), cudaMemcpyHostToDevice, st));
+  k_bounds<<<grid_for(m), 256, 0, st>>>(m, sdeg, bounds + 8, nth, bounds);
   k_relabel<<<grid_for(m), 256, 0, st>>>(m, L->perm, d_outdeg, L->outdeg, inv);
-  int hb[2];
-  GPR_CUDA(cudaMemcpyAsync(hb, bounds, sizeof(hb), cudaMemcpyDeviceToHost, st));
+  int hb[8];
+  GPR_CUDA(cudaMemcpyAsync(hb, bounds, nth * sizeof(int), cudaMemcpyDeviceToHost, st));
   GPR_CUDA(cudaStreamSynchronize(st));
   L->n_long = hb[0];
-  L->n_nz = hb[1];
+  L->n_nz = hb[nth - 1];
+  // Classes: widest first; class with lw spans rows [hb[4-lw], hb[5-lw]).
+  PrClasses &C = L->cls;
+  int slices = 0;
+  for (int lw = 5; lw >= 0; --lw) {
+    const int r0 = hb[5 - lw], r1 = hb[6 - lw];
+    if (r1 <= r0) continue;
+    C.lw[C.n_cls] = lw;
+    C.row[C.n_cls] = r0;
+    C.slice[C.n_cls] = slices;
+    slices += (int)ceil_div(r1 - r0, 32 >> lw);
+    ++C.n_cls;
+  }
+  C.row[C.n_cls] = L->n_nz;
+  C.slice[C.n_cls] = slices;
+  L->n_slices = slices;
 
   // Long rows: padded CSR + chunk table.
   GPR_TRY(dalloc(&L->long_ptr, (size_t)L->n_long + 1, "long row offsets"));
@@ -267,10 +306,9 @@ int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
   }
 
   // SELL-32 slices over rows [n_long, n_nz).
-  L->n_slices = (int)ceil_div((long long)L->n_nz - L->n_long, 32);
   GPR_TRY(dalloc(&L->slice_ptr, (size_t)L->n_slices + 1, "slice offsets"));
-  k_slice_lens<<<grid_for((long long)L->n_slices + 1), 256, 0, st>>>(L->n_slices, L->n_long,
-                                                                      sdeg, L->slice_ptr);
+  k_slice_lens<<<grid_for((long long)L->n_slices + 1), 256, 0, st>>>(L->n_slices, C, sdeg,
+                                                                      L->slice_ptr);
   GPR_TRY(exclusive_scan(L->slice_ptr, (long long)L->n_slices + 1, st));
   GPR_CUDA(cudaMemcpyAsync(&L->sell_elems, L->slice_ptr + L->n_slices, sizeof(long long),
                            cudaMemcpyDeviceToHost, st));
@@ -278,8 +316,7 @@ int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
   GPR_TRY(dalloc(&L->sell_col, (size_t)L->sell_elems, "sell slices"));
   if (L->n_slices > 0)
     k_fill_sell<<<grid_for(32LL * L->n_slices), 256, 0, st>>>(
-        L->n_slices, L->n_long, L->n_nz, m, L->perm, inv, d_rowptr, d_col, sdeg, L->slice_ptr,
-        L->sell_col);
+        L->n_slices, m, C, L->perm, inv, d_rowptr, d_col, sdeg, L->slice_ptr, L->sell_col);
   L->n_zblk = (int)ceil_div((long long)m - L->n_nz, kZeroRowsPerUnit);
   GPR_CUDA(cudaGetLastError());
   GPR_CUDA(cudaStreamSynchronize(st));

@@ -45,7 +45,8 @@ struct gpr_graph {
   double *res_tmp = nullptr;   // [m+1+n_long] FP64 residual scratch
   int err_cap = 0;
   int last_sweeps = 0;
-  int grid_persist = 0, grid_step = 0, max_grid = 0;
+  int grid_persist[8] = {0};  // cooperative grid of each sweep-kernel variant
+  int grid_step = 0, max_grid = 0;
   bool coop = false;
   cudaStream_t st = nullptr;
   bool own_stream = false;
@@ -56,6 +57,7 @@ namespace {
 
 struct PrArgs {
   int m, n_long, n_nz, n_chunks, n_slices, n_zblk, chunk;
+  gpr::PrClasses cls;
   const long long *long_ptr;
   const int *long_col;
   const int *row_cbeg;
@@ -77,14 +79,20 @@ struct PrArgs {
 
 constexpr unsigned kFull = 0xffffffffu;
 
-__device__ __forceinline__ uint64_t evict_first_policy() {
-  uint64_t p;
-  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+struct Policies {
+  uint64_t stream;  // evict-first: data read or written once per sweep
+  uint64_t keep;    // evict-last: contributions, gathered many times
+};
+
+__device__ __forceinline__ Policies make_policies() {
+  Policies p;
+  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p.stream));
+  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p.keep));
   return p;
 }
 
-// Edge indices are read exactly once per sweep: bypass L1, evict-first in L2
-// so they do not push the contributions out.
+// Edge indices are read exactly once per sweep: no L1 allocation, evict-first
+// in L2 so they do not push the contributions out.
 __device__ __forceinline__ int ld_idx(const int *p, uint64_t pol) {
   int v;
   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"
@@ -97,6 +105,32 @@ __device__ __forceinline__ int4 ld_idx4(const int *p, uint64_t pol) {
   asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
       : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p), "l"(pol));
   return v;
+}
+
+// Contribution gather.  A plain (coherent, L1-cached) load: the persistent
+// kernel rewrites these buffers between sweeps, so the non-coherent path
+// must not be used; the grid barrier's fences order the accesses.
+__device__ __forceinline__ float ld_contrib(const float *p, uint64_t pol) {
+  float v;
+  asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
+__device__ __forceinline__ float ld_f32_stream(const float *p, uint64_t pol) {
+  float v;
+  asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
+__device__ __forceinline__ int ld_s32_stream(const int *p, uint64_t pol) {
+  int v;
+  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"
+      : "=r"(v) : "l"(p), "l"(pol));
+  return v;
+}
+
+__device__ __forceinline__ void st_f32(float *p, float v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" :: "l"(p), "f"(v), "l"(pol) : "memory");
 }
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
@@ -123,38 +157,52 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
-// Score update of row r from its pulled sum; returns |s_new - s_old|.
-__device__ __forceinline__ double row_update(const PrArgs &a, int r, float sum, float *cout) {
-  const float so = a.s[r];
+// Score update of row r from its pulled sum and its prefetched old score and
+// out-degree; returns |s_new - s_old|.
+__device__ __forceinline__ double row_update(const PrArgs &a, int r, float sum, float so, int od,
+                                             float *cout, const Policies &pol) {
   const float sn = __fadd_rn(a.base, __fmul_rn(a.damp, sum));
-  a.s[r] = sn;
-  cout[r] = __fdiv_rn(sn, __int2float_rn(a.outdeg[r]));
+  st_f32(a.s + r, sn, pol.stream);
+  st_f32(cout + r, __fdiv_rn(sn, __int2float_rn(od)), pol.keep);
   return (double)fabsf(__fsub_rn(sn, so));
 }
 
-__device__ __forceinline__ double do_chunk(const PrArgs &a, const float *cin, float *cout,
-                                           int c, int lane, uint64_t pol) {
+// One chunk of a long row: U4 16-byte index loads per lane in flight, then
+// 4*U4 independent gathers.
+template <int U4>
+__device__ __forceinline__ double do_chunk(const PrArgs &a, const float *cin, float *cout, int c,
+                                           int lane, const Policies &pol) {
   const int r = a.chunk_row[c];
   const int cb = a.row_cbeg[r];
   const int nc = a.row_cbeg[r + 1] - cb;
+  float so = 0.f;
+  int od = 1;
+  if (lane == 0) {
+    so = ld_f32_stream(a.s + r, pol.stream);
+    od = ld_s32_stream(a.outdeg + r, pol.stream);
+  }
   const long long b = a.long_ptr[r] + (long long)(c - cb) * a.chunk;
   const long long e = min(b + (long long)a.chunk, a.long_ptr[r + 1]);
-  float acc0 = 0.f, acc1 = 0.f;
-  long long k = b + 4 * lane;
-  for (; k + 128 < e; k += 256) {
-    const int4 q0 = ld_idx4(a.long_col + k, pol);
-    const int4 q1 = ld_idx4(a.long_col + k + 128, pol);
-    const float v0 = cin[q0.x], v1 = cin[q0.y], v2 = cin[q0.z], v3 = cin[q0.w];
-    const float v4 = cin[q1.x], v5 = cin[q1.y], v6 = cin[q1.z], v7 = cin[q1.w];
-    acc0 += (v0 + v1) + (v2 + v3);
-    acc1 += (v4 + v5) + (v6 + v7);
+  float acc = 0.f;
+  for (long long k0 = b + 4 * lane; k0 < e; k0 += 128 * U4) {
+    int4 q[U4];
+#pragma unroll
+    for (int i = 0; i < U4; ++i)
+      q[i] = (k0 + 128 * i < e) ? ld_idx4(a.long_col + k0 + 128 * i, pol.stream)
+                                : make_int4(a.m, a.m, a.m, a.m);
+    float v[4 * U4];
+#pragma unroll
+    for (int i = 0; i < U4; ++i) {
+      v[4 * i + 0] = ld_contrib(cin + q[i].x, pol.keep);
+      v[4 * i + 1] = ld_contrib(cin + q[i].y, pol.keep);
+      v[4 * i + 2] = ld_contrib(cin + q[i].z, pol.keep);
+      v[4 * i + 3] = ld_contrib(cin + q[i].w, pol.keep);
+    }
+#pragma unroll
+    for (int i = 0; i < 4 * U4; ++i) acc += v[i];
   }
-  if (k < e) {
-    const int4 q0 = ld_idx4(a.long_col + k, pol);
-    acc0 += (cin[q0.x] + cin[q0.y]) + (cin[q0.z] + cin[q0.w]);
-  }
-  const float acc = warp_sum(acc0 + acc1);
-  if (nc == 1) return lane == 0 ? row_update(a, r, acc, cout) : 0.0;
+  acc = warp_sum(acc);
+  if (nc == 1) return lane == 0 ? row_update(a, r, acc, so, od, cout, pol) : 0.0;
   int last = 0;
   if (lane == 0) {
     a.partial[c] = acc;
@@ -169,56 +217,79 @@ __device__ __forceinline__ double do_chunk(const PrArgs &a, const float *cin, fl
   t = warp_sum(t);
   if (lane != 0) return 0.0;
   atomicExch(a.cnt + r, 0);
-  return row_update(a, r, t, cout);
+  return row_update(a, r, t, so, od, cout, pol);
 }
 
+// One SELL slice: 32 >> lw rows, w = 1 << lw lanes per row.  Each lane runs
+// batches of U independent index loads followed by U independent gathers;
+// entries past the slice length read the sentinel slot (an exact +0).
+template <int U>
 __device__ __forceinline__ double do_slice(const PrArgs &a, const float *cin, float *cout,
-                                           int sidx, int lane, uint64_t pol) {
+                                           int sidx, int lane, const Policies &pol) {
+  const int c = gpr::slice_class(a.cls, sidx);
+  const int lw = a.cls.lw[c];
+  const int row0 = a.cls.row[c] + ((sidx - a.cls.slice[c]) << (5 - lw));
+  const int r = row0 + (lane >> lw);
+  const bool lead = (lane & ((1 << lw) - 1)) == 0;
+  const bool valid = r < a.cls.row[c + 1];
+  float so = 0.f;
+  int od = 1;
+  if (valid && lead) {
+    so = ld_f32_stream(a.s + r, pol.stream);
+    od = ld_s32_stream(a.outdeg + r, pol.stream);
+  }
   const long long b = a.slice_ptr[sidx];
   const int len = (int)((a.slice_ptr[sidx + 1] - b) >> 5);
   const int *p = a.sell_col + b + lane;
   float acc = 0.f;
-  int j = 0;
-  for (; j + 8 <= len; j += 8) {
-    int c[8];
-    float v[8];
+  for (int j0 = 0; j0 < len; j0 += U) {
+    int ci[U];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) c[q] = ld_idx(p + 32 * (j + q), pol);
+    for (int q = 0; q < U; ++q) ci[q] = (j0 + q < len) ? ld_idx(p + 32 * (j0 + q), pol.stream) : a.m;
+    float v[U];
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = cin[c[q]];
+    for (int q = 0; q < U; ++q) v[q] = ld_contrib(cin + ci[q], pol.keep);
 #pragma unroll
-    for (int q = 0; q < 8; ++q) acc = __fadd_rn(acc, v[q]);
+    for (int q = 0; q < U; ++q) acc = __fadd_rn(acc, v[q]);
   }
-  for (; j + 2 <= len; j += 2) {
-    const int c0 = ld_idx(p + 32 * j, pol), c1 = ld_idx(p + 32 * (j + 1), pol);
-    const float v0 = cin[c0], v1 = cin[c1];
-    acc = __fadd_rn(acc, v0);
-    acc = __fadd_rn(acc, v1);
-  }
-  if (j < len) acc = __fadd_rn(acc, cin[ld_idx(p + 32 * j, pol)]);
-  const int r = a.n_long + sidx * 32 + lane;
-  return r < a.n_nz ? row_update(a, r, acc, cout) : 0.0;
+  for (int o = (1 << lw) >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+  return (valid && lead) ? row_update(a, r, acc, so, od, cout, pol) : 0.0;
 }
 
-__device__ __forceinline__ double do_zero(const PrArgs &a, float *cout, int z, int lane) {
+// Rows without in-edges: s = base from the first sweep on, so they are
+// updated in sweep 0 and only their contribution is copied into the other
+// buffer in sweep 1; later sweeps skip them (their residual term is 0).
+__device__ __forceinline__ double do_zero(const PrArgs &a, float *cout, int z, int lane, int it,
+                                          const Policies &pol) {
   double err = 0.0;
   const int r0 = a.n_nz + z * gpr::kZeroRowsPerUnit;
 #pragma unroll
   for (int q = 0; q < gpr::kZeroRowsPerUnit / 32; ++q) {
     const int r = r0 + 32 * q + lane;
-    if (r < a.m) err += row_update(a, r, 0.f, cout);
+    if (r < a.m) {
+      const int od = ld_s32_stream(a.outdeg + r, pol.stream);
+      if (it == 0) {
+        err += row_update(a, r, 0.f, ld_f32_stream(a.s + r, pol.stream), od, cout, pol);
+      } else {
+        const float sn = __fadd_rn(a.base, __fmul_rn(a.damp, 0.f));
+        st_f32(cout + r, __fdiv_rn(sn, __int2float_rn(od)), pol.keep);
+      }
+    }
   }
   return err;
 }
 
+template <int U, int U4>
 __device__ __forceinline__ double sweep(const PrArgs &a, const float *cin, float *cout,
-                                        long long gw, long long nw, int lane, uint64_t pol) {
-  const long long u1 = a.n_chunks, u2 = u1 + a.n_slices, u3 = u2 + a.n_zblk;
+                                        long long gw, long long nw, int lane, int it,
+                                        const Policies &pol) {
+  const long long u1 = a.n_chunks, u2 = u1 + a.n_slices;
+  const long long u3 = u2 + (it < 2 ? a.n_zblk : 0);
   double err = 0.0;
   for (long long u = gw; u < u3; u += nw) {
-    if (u < u1) err += do_chunk(a, cin, cout, (int)u, lane, pol);
-    else if (u < u2) err += do_slice(a, cin, cout, (int)(u - u1), lane, pol);
-    else err += do_zero(a, cout, (int)(u - u2), lane);
+    if (u < u1) err += do_chunk<U4>(a, cin, cout, (int)u, lane, pol);
+    else if (u < u2) err += do_slice<U>(a, cin, cout, (int)(u - u1), lane, pol);
+    else err += do_zero(a, cout, (int)(u - u2), lane, it, pol);
   }
   return err;
 }
@@ -286,16 +357,17 @@ __device__ bool barrier_reduce(const PrArgs &a, int it, double cta_total) {
 }
 
 // All sweeps in one cooperative launch.
+template <int U, int U4>
 __global__ void __launch_bounds__(gpr::kBlock) k_pr_persistent(PrArgs a) {
   const int lane = threadIdx.x & 31;
   const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-  const uint64_t pol = evict_first_policy();
+  const Policies pol = make_policies();
   int it = 0;
   while (it < a.max_iter) {
     const float *cin = (it & 1) ? a.c1 : a.c0;
     float *cout = (it & 1) ? a.c0 : a.c1;
-    const double err = sweep(a, cin, cout, gw, nw, lane, pol);
+    const double err = sweep<U, U4>(a, cin, cout, gw, nw, lane, it, pol);
     const double tot = block_sum(err);
     if (!barrier_reduce(a, it, tot)) return;
     const double total = __ldcg(a.err_hist + it);
@@ -311,6 +383,7 @@ __global__ void __launch_bounds__(gpr::kBlock) k_pr_persistent(PrArgs a) {
 // One sweep per launch (graph mode).  The sweep index and the done flag live
 // in device memory, so a captured sequence of launches needs no host input;
 // launches after convergence return at once.
+template <int U, int U4>
 __global__ void __launch_bounds__(gpr::kBlock) k_pr_step(PrArgs a) {
   __shared__ int s_it, s_last;
   if (threadIdx.x == 0) {
@@ -323,10 +396,10 @@ __global__ void __launch_bounds__(gpr::kBlock) k_pr_step(PrArgs a) {
   const int lane = threadIdx.x & 31;
   const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
-  const uint64_t pol = evict_first_policy();
+  const Policies pol = make_policies();
   const float *cin = (it & 1) ? a.c1 : a.c0;
   float *cout = (it & 1) ? a.c0 : a.c1;
-  const double err = sweep(a, cin, cout, gw, nw, lane, pol);
+  const double err = sweep<U, U4>(a, cin, cout, gw, nw, lane, it, pol);
   const double tot = block_sum(err);
   if (threadIdx.x == 0) {
     a.cta_err[blockIdx.x] = tot;
@@ -402,12 +475,15 @@ __global__ void k_res_sweep(PrArgs a, const double *__restrict__ cd, const doubl
       if (lane == 0) atomicAdd(long_acc + r, acc);
     } else if (u < u2) {
       const int sidx = (int)(u - u1);
+      const int c = gpr::slice_class(a.cls, sidx);
+      const int lw = a.cls.lw[c];
+      const int r = a.cls.row[c] + ((sidx - a.cls.slice[c]) << (5 - lw)) + (lane >> lw);
       const long long b = a.slice_ptr[sidx];
       const int len = (int)((a.slice_ptr[sidx + 1] - b) >> 5);
       double acc = 0.0;
       for (int j = 0; j < len; ++j) acc += cd[a.sell_col[b + 32LL * j + lane]];
-      const int r = a.n_long + sidx * 32 + lane;
-      if (r < a.n_nz) err += fabs(base + d * acc - sd[r]);
+      for (int o = (1 << lw) >> 1; o > 0; o >>= 1) acc += __shfl_xor_sync(kFull, acc, o);
+      if (r < a.cls.row[c + 1] && (lane & ((1 << lw) - 1)) == 0) err += fabs(base + d * acc - sd[r]);
     } else {
       const int r0 = a.n_nz + (int)(u - u2) * gpr::kZeroRowsPerUnit;
       for (int q = 0; q < gpr::kZeroRowsPerUnit / 32; ++q) {
@@ -434,6 +510,20 @@ inline unsigned grid_for(long long n, int block = 256) {
   return (unsigned)(g < 1 ? 1 : g);
 }
 
+// Unroll variants of the sweep kernels: (slice batch U, int4 loads per lane
+// U4).  Variant 0 is the default; the others are the autotuner's choices.
+struct SweepKernels {
+  const void *persistent;
+  void (*step)(PrArgs);
+};
+const SweepKernels kVariants[] = {
+    {(const void *)k_pr_persistent<16, 4>, k_pr_step<16, 4>},
+    {(const void *)k_pr_persistent<8, 2>, k_pr_step<8, 2>},
+    {(const void *)k_pr_persistent<4, 2>, k_pr_step<4, 2>},
+    {(const void *)k_pr_persistent<32, 8>, k_pr_step<32, 8>},
+};
+constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+
 PrArgs make_args(gpr_graph *g, const gpr_pr_opts &o) {
   const PrLayout &L = g->L;
   PrArgs a;
@@ -444,6 +534,7 @@ PrArgs make_args(gpr_graph *g, const gpr_pr_opts &o) {
   a.n_slices = L.n_slices;
   a.n_zblk = L.n_zblk;
   a.chunk = L.chunk;
+  a.cls = L.cls;
   a.long_ptr = L.long_ptr;
   a.long_col = L.long_col;
   a.row_cbeg = L.row_cbeg;
@@ -464,7 +555,7 @@ PrArgs make_args(gpr_graph *g, const gpr_pr_opts &o) {
   a.base = (1.0f - o.damping) / (float)L.m;  // src/pr/omp_base.cc:16
   a.tol = o.tol;
   a.max_iter = o.max_iter;
-  a.bar_expect = g->grid_persist;
+  a.bar_expect = g->grid_persist[o.variant];
   a.timeout_ns = (long long)(o.timeout_s * 1e9);
   return a;
 }
@@ -492,7 +583,7 @@ void destroy(gpr_graph *g) {
 }
 
 int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
-                const int *any_outdeg, gpr_graph *g) {
+                const int *any_outdeg, int lane_max, int chunk_min, int chunk, gpr_graph *g) {
   GPR_CUDA(cudaGetDevice(&g->device));
   GPR_CUDA(cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking));
   g->own_stream = true;
@@ -511,7 +602,7 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
     rc = gpr::validate_csr(m, nnz, m, (const int *)rp, (const int *)cp, (const int *)dp, st);
   if (rc == GPR_OK)
     rc = gpr::build_pr_layout(m, nnz, (const int *)rp, (const int *)cp, (const int *)dp,
-                              gpr::kSellMaxDefault, gpr::kChunkDefault, &g->L, st);
+                              lane_max, chunk_min, chunk, &g->L, st);
   cudaStreamSynchronize(st);
   if (orp) cudaFree(rp);
   if (ocp) cudaFree(cp);
@@ -528,20 +619,29 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
   GPR_TRY(gpr::dalloc(&g->scores_tmp, (size_t)m, "score staging"));
   GPR_CUDA(cudaMemsetAsync(g->cnt, 0, sizeof(int) * (L.n_long ? L.n_long : 1), st));
 
-  int sms = 0, coop = 0, per_sm = 0;
+  int sms = 0, coop = 0;
   GPR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
   GPR_CUDA(cudaDeviceGetAttribute(&coop, cudaDevAttrCooperativeLaunch, g->device));
-  GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_pr_persistent, gpr::kBlock, 0));
   const long long units = (long long)L.n_chunks + L.n_slices + L.n_zblk;
   const long long warps_per_cta = gpr::kBlock / 32;
   const long long need = gpr::ceil_div(units, warps_per_cta);
-  long long full = (long long)sms * (per_sm > 0 ? per_sm : 1);
-  g->coop = coop != 0 && per_sm > 0;
-  g->grid_persist = (int)(need < full ? (need < 1 ? 1 : need) : full);
+  g->coop = coop != 0;
+  long long full_max = sms;
+  for (int v = 0; v < kNumVariants; ++v) {
+    int per_sm = 0;
+    GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kVariants[v].persistent,
+                                                           gpr::kBlock, 0));
+    const long long full = (long long)sms * (per_sm > 0 ? per_sm : 1);
+    if (per_sm <= 0) g->coop = false;
+    g->grid_persist[v] = (int)(need < full ? (need < 1 ? 1 : need) : full);
+    if (full > full_max) full_max = full;
+  }
   long long step = need < 1 ? 1 : need;
-  if (step > full * 4) step = full * 4;
+  if (step > full_max * 4) step = full_max * 4;
   g->grid_step = (int)step;
-  g->max_grid = g->grid_persist > g->grid_step ? g->grid_persist : g->grid_step;
+  g->max_grid = g->grid_step;
+  for (int v = 0; v < kNumVariants; ++v)
+    if (g->grid_persist[v] > g->max_grid) g->max_grid = g->grid_persist[v];
   GPR_TRY(gpr::dalloc(&g->cta_err, 2 * (size_t)g->max_grid, "cta residuals"));
   g->err_cap = 128;
   GPR_TRY(gpr::dalloc(&g->err_hist, (size_t)g->err_cap, "residual history"));
@@ -555,7 +655,7 @@ int pagerank_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts_in,
   if (opts_in) o = *opts_in;
   else gpr_pr_opts_default(&o);
   if (!(o.damping >= 0.f && o.damping <= 1.f) || o.max_iter < 0 || !(o.tol >= 0.0) ||
-      !(o.timeout_s > 0.0)) {
+      !(o.timeout_s > 0.0) || o.variant < 0 || o.variant >= kNumVariants) {
     gpr::set_error("gpr_pagerank: invalid options (damping %g, tol %g, max_iter %d, timeout %g)",
                    (double)o.damping, o.tol, o.max_iter, o.timeout_s);
     return GPR_EINVAL;
@@ -606,9 +706,9 @@ int pagerank_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts_in,
   if (o.max_iter > 0) {
     if (loop == GPR_LOOP_PERSISTENT) {
       void *args[] = {&a};
-      cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_pr_persistent,
-                                                  dim3(g->grid_persist), dim3(gpr::kBlock), args,
-                                                  0, st);
+      cudaError_t e = cudaLaunchCooperativeKernel(kVariants[o.variant].persistent,
+                                                  dim3(g->grid_persist[o.variant]),
+                                                  dim3(gpr::kBlock), args, 0, st);
       if (e == cudaErrorCooperativeLaunchTooLarge) {
         cudaGetLastError();
         loop = GPR_LOOP_GRAPH;
@@ -624,7 +724,7 @@ int pagerank_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts_in,
       int done = 0, issued = 0;
       while (!done && issued < o.max_iter) {
         for (int q = 0; q < batch && issued < o.max_iter; ++q, ++issued) {
-          k_pr_step<<<g->grid_step, gpr::kBlock, 0, st>>>(a);
+          kVariants[o.variant].step<<<g->grid_step, gpr::kBlock, 0, st>>>(a);
           ++launches;
         }
         GPR_CUDA(cudaGetLastError());
@@ -668,6 +768,21 @@ extern "C" {
 
 int gpr_graph_create(int m, long long nnz, const int *any_rowptr, const int *any_col,
                      const int *any_outdeg, gpr_graph **out) {
+  return gpr_graph_create_ex(m, nnz, any_rowptr, any_col, any_outdeg, nullptr, out);
+}
+
+int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr, const int *any_col,
+                        const int *any_outdeg, const gpr_layout_opts *lopts, gpr_graph **out) {
+  int lane_max = gpr::kSellMaxDefault, chunk = gpr::kChunkDefault,
+      chunk_min = gpr::kChunkMinDefault;
+  if (lopts && lopts->sell_max) lane_max = lopts->sell_max;
+  if (lopts && lopts->chunk) chunk = lopts->chunk;
+  if (lopts && lopts->chunk_min) chunk_min = lopts->chunk_min;
+  if (lane_max < 1 || lane_max > 1024 || chunk < 128 || chunk % 128 != 0 || chunk_min < 1) {
+    gpr::set_error("gpr_graph_create_ex: invalid layout options (lane_max %d, chunk %d, "
+                   "chunk_min %d)", lane_max, chunk, chunk_min);
+    return GPR_EINVAL;
+  }
   if (!out) {
     gpr::set_error("gpr_graph_create: NULL out");
     return GPR_EINVAL;
@@ -685,7 +800,7 @@ int gpr_graph_create(int m, long long nnz, const int *any_rowptr, const int *any
     return GPR_ENODEV;
   }
   gpr_graph *g = new gpr_graph();
-  int rc = create_impl(m, nnz, any_rowptr, any_col, any_outdeg, g);
+  int rc = create_impl(m, nnz, any_rowptr, any_col, any_outdeg, lane_max, chunk_min, chunk, g);
   if (rc != GPR_OK) {
     destroy(g);
     return rc;

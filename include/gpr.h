@@ -58,7 +58,10 @@ typedef struct {
   int loop;             /* gpr_loop */
   double timeout_s;     /* bound on every device-side wait (grid barrier); default 5 s */
   int refine_max;       /* mixed precision: max FP32 refinement sweeps (default 64) */
-  int reserved[8];
+  int variant;          /* sweep-kernel unroll variant, 0..3 (0 = default; see the autotuner) */
+  int reserved[7];      /* reserved[0] > 0: the grid barrier also waits for that many CTAs
+                           that do not exist, so its bounded wait runs out (tests of the
+                           GPR_ETIMEOUT path); keep 0 otherwise */
 } gpr_pr_opts;
 
 typedef struct {
@@ -88,6 +91,17 @@ int gpr_pr_opts_default(gpr_pr_opts *opts);
 int gpr_graph_create(int m, long long nnz, const int *any_rowptr,
                      const int *any_col, const int *any_outdeg,
                      gpr_graph **out);
+/* Layout knobs (the autotuner's search space); zero fields take defaults. */
+typedef struct {
+  int sell_max;   /* max edges per lane in a SELL slice: rows of in-degree <= sell_max get
+                     one lane, wider rows 2..32 lanes (default 64) */
+  int chunk;      /* edges per long-row chunk, multiple of 128 (default 4096) */
+  int chunk_min;  /* rows with more in-edges than this are cut into chunks (default 4096) */
+  int reserved[5];
+} gpr_layout_opts;
+int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr,
+                        const int *any_col, const int *any_outdeg,
+                        const gpr_layout_opts *lopts, gpr_graph **out);
 int gpr_graph_destroy(gpr_graph *g);
 int gpr_graph_info(const gpr_graph *g, int *m, long long *nnz,
                    long long *device_bytes);
@@ -157,6 +171,9 @@ int gpr_free(void *d_ptr);
 int gpr_malloc(void **d_ptr, size_t bytes);
 int gpr_memcpy(void *dst, const void *src, size_t bytes);
 int gpr_synchronize(void);
+/* Make `device` current for the calling thread's later gpr calls (handles
+ * remember the device they were created on). */
+int gpr_set_device(int device);
 
 /* ---- graph_io (host) ------------------------------------------------------
  * read_graph of include/graph_io.h:280 for foreign callers: same parsers and

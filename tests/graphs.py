@@ -28,7 +28,7 @@ def erdos_renyi(m, avg_deg, seed):
     return in_csr(m, rng.integers(0, m, ne), rng.integers(0, m, ne))
 
 
-def star(m, seed=0):
+def star(m=100000, seed=0):
     """Every vertex points at vertex 0 (in-degree m-1, many chunks); vertex 0
     points at 1; plus a sprinkle of random edges."""
     rng = np.random.default_rng(seed)

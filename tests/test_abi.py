@@ -65,9 +65,31 @@ def test_options_defaults_match_reference_constants(G):
     assert np.float32(o.damping) == np.float32(0.85)        # include/common.h:18
 
 
-def test_struct_layout_matches_header(G):
-    assert C.sizeof(G.PrOptions) == 8 + 8 + 4 * 4 + 8 + 4 + 4 * 8 + 4  # padded below
-    assert C.sizeof(G.PrStats) == 4 + 4 + 8 * 3 + 4 + 4 * 5
+def test_struct_layout_matches_header(G, tmp_path):
+    """The ctypes mirrors have the C compiler's sizes and field offsets."""
+    src = r"""
+#include <stddef.h>
+#include <stdio.h>
+#include "gpr.h"
+int main(void) {
+  printf("%zu %zu %zu %zu %zu %zu %zu\n", sizeof(gpr_pr_opts), sizeof(gpr_pr_stats),
+         sizeof(gpr_layout_opts), offsetof(gpr_pr_opts, variant),
+         offsetof(gpr_pr_opts, timeout_s), offsetof(gpr_pr_stats, loop_ms),
+         offsetof(gpr_pr_stats, gpu_launches));
+  return 0;
+}
+"""
+    c = tmp_path / "sz.c"
+    c.write_text(src)
+    exe = tmp_path / "sz"
+    subprocess.run(["/usr/bin/gcc", "-std=c99", str(c), "-I", os.path.join(ROOT, "include"),
+                    "-o", str(exe)], check=True)
+    got = [int(x) for x in subprocess.run([str(exe)], capture_output=True, text=True,
+                                          check=True).stdout.split()]
+    want = [C.sizeof(G.PrOptions), C.sizeof(G.PrStats), C.sizeof(G.LayoutOptions),
+            G.PrOptions.variant.offset, G.PrOptions.timeout_s.offset, G.PrStats.loop_ms.offset,
+            G.PrStats.gpu_launches.offset]
+    assert got == want
 
 
 @pytest.mark.skipif(has_gpu(), reason="checks the no-device path")

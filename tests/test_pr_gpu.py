@@ -28,7 +28,7 @@ def test_rmat_s16_matches_reference(G, O):
     rp, col, od = O.rmat_graph(16, 16, seed=1)
     ref, ref_it, ref_hist = O.pr_plain_f32(rp, col, od, tol=1e-4, max_iter=100)
     s, st, hist, lay = solve(G, rp, col, od, tol=1e-4, max_iter=100)
-    assert lay["n_long"] > 0 and lay["n_chunks"] > lay["n_long"]
+    assert lay["n_slices"] > 0
     assert abs(st.iterations - ref_it) <= 1
     assert np.abs(s - ref).max() <= ABS_TOL
     s64, _, _ = O.pr_f64(rp, col, od)
@@ -42,20 +42,32 @@ def test_short_rows_bit_identical(G, O):
     assert np.diff(rp).max() <= 64
     ref, ref_it, ref_hist = O.pr_plain_f32(rp, col, od, tol=1e-6, max_iter=100)
     s, st, hist, lay = solve(G, rp, col, od, tol=1e-6, max_iter=100)
-    assert lay["n_long"] == 0
+    assert lay["n_long"] == 0 and lay["n_slices"] > 0
     assert st.iterations == ref_it
     assert np.array_equal(s, ref)
     np.testing.assert_allclose(hist, ref_hist, rtol=1e-12)
 
 
 @pytest.mark.parametrize("maker", [star, degree_ladder])
-def test_long_rows_and_bins(G, O, maker):
+@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+def test_long_rows_and_bins(G, O, maker, variant):
+    # The tolerance sits well above the float rounding floor of the L1
+    # residual (about m * ulp(score) ~ 1e-7 here), where the sweep count is
+    # decided by the arithmetic rather than by noise.
+    # A hub with 1e5 in-edges carries a score near 0.3; the reference's own
+    # sequential float sum is then off by ~1e-5 from the exact sum, so each
+    # vertex may deviate from the reference by 1e-6 plus the reference's own
+    # distance to an FP64 run of the same number of sweeps.
     rp, col, od = maker()
-    ref, ref_it, _ = O.pr_plain_f32(rp, col, od, tol=1e-7, max_iter=60)
-    s, st, _, lay = solve(G, rp, col, od, tol=1e-7, max_iter=60)
-    assert lay["n_long"] > 0
+    ref, ref_it, _ = O.pr_plain_f32(rp, col, od, tol=1e-5, max_iter=60)
+    with G.Graph(rp, col, od, chunk=512, chunk_min=1024) as g:
+        lay = g.layout()
+        s, st = g.pagerank(tol=1e-5, max_iter=60, variant=variant)
+    assert lay["n_long"] > 0 and lay["n_chunks"] > lay["n_long"]
     assert abs(st.iterations - ref_it) <= 1
-    assert np.abs(s - ref).max() <= ABS_TOL
+    s64, _, _ = O.pr_f64(rp, col, od, tol=0.0, max_iter=st.iterations)
+    assert np.all(np.abs(s - ref) <= ABS_TOL + np.abs(ref - s64))
+    assert np.abs(s - s64).max() <= np.abs(ref - s64).max() + ABS_TOL
 
 
 def test_loop_modes_identical(G, O):
