@@ -43,7 +43,7 @@ class PrOptions(C.Structure):
 
 class LayoutOptions(C.Structure):
     _fields_ = [("sell_max", C.c_int), ("chunk", C.c_int), ("chunk_min", C.c_int),
-                ("reserved", C.c_int * 5)]
+                ("hot_entries", C.c_int), ("reserved", C.c_int * 4)]
 
 
 class PrStats(C.Structure):
@@ -195,7 +195,8 @@ class Graph:
     """Device-resident pull graph: in-CSR (row v = sources of edges u->v) plus
     the out-degree of every vertex (src/pr/omp_base.cc:9 arguments)."""
 
-    def __init__(self, rowptr, col, outdeg, m=None, nnz=None, sell_max=0, chunk=0, chunk_min=0):
+    def __init__(self, rowptr, col, outdeg, m=None, nnz=None, sell_max=0, chunk=0, chunk_min=0,
+                 hot_entries=0):
         L = lib()
         m = int(len(rowptr) - 1) if m is None else int(m)
         nnz = int(len(col)) if nnz is None else int(nnz)
@@ -203,7 +204,7 @@ class Graph:
         pc, k1 = _ptr(col, np.int32)
         pd, k2 = _ptr(outdeg, np.int32)
         h = C.c_void_p()
-        lo = LayoutOptions(int(sell_max), int(chunk), int(chunk_min))
+        lo = LayoutOptions(int(sell_max), int(chunk), int(chunk_min), int(hot_entries))
         _check(L.gpr_graph_create_ex(m, nnz, pr, pc, pd, C.byref(lo), C.byref(h)))
         self._h, self.m, self.nnz = h, m, nnz
         self.last_stats = None

@@ -149,7 +149,9 @@ constexpr int kSellMaxDefault = 64;    // SpMV: row length bound of the SELL bin
                                        // PR: max edges per lane in a SELL slice
 constexpr int kChunkMinDefault = 4096; // PR: rows with more in-edges are chunked
 constexpr int kChunkDefault = 4096;    // edges per long-row chunk (multiple of 128)
-constexpr int kBlock = 256;            // threads per CTA of the sweep kernels
+constexpr int kBlock = 256;            // threads per CTA of the per-sweep kernels
+constexpr int kHotDefault = 32768;     // contributions staged in shared memory (128 KB)
+constexpr int kHotMax = 56832;         // 222 KB: the most one CTA may take
 
 __host__ __device__ inline long long ceil_div(long long a, long long b) {
   return (a + b - 1) / b;

@@ -23,6 +23,7 @@
 #include <math.h>
 #include <string.h>
 
+#include <algorithm>
 #include <vector>
 
 #include "gpr_internal.cuh"
@@ -45,7 +46,10 @@ struct gpr_graph {
   double *res_tmp = nullptr;   // [m+1+n_long] FP64 residual scratch
   int err_cap = 0;
   int last_sweeps = 0;
-  int grid_persist[8] = {0};  // cooperative grid of each sweep-kernel variant
+  int hot = 0;                 // contributions staged in shared memory per sweep
+  int grid_hot = 0;            // cooperative grid of the hot kernel (<= 1 CTA per SM)
+  int *wq = nullptr;           // [2] work-queue heads of the hot kernel
+  bool hot_ok = false;         // every hot-kernel variant is co-resident at grid_hot
   int grid_step = 0, max_grid = 0;
   bool coop = false;
   cudaStream_t st = nullptr;
@@ -75,6 +79,9 @@ struct PrArgs {
   int max_iter;
   int bar_expect;
   long long timeout_ns;
+  int hot;                // contributions [0, hot) are staged in shared memory
+  int *wq;                // [2] work-queue heads of the hot kernel, by sweep parity
+  int batch;              // units per work-queue grab
 };
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -115,6 +122,39 @@ __device__ __forceinline__ float ld_contrib(const float *p, uint64_t pol) {
   asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
   return v;
 }
+
+__device__ __forceinline__ float4 ld_contrib4(const float4 *p, uint64_t pol) {
+  float4 v;
+  asm volatile("ld.global.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
+               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p), "l"(pol));
+  return v;
+}
+
+// Contribution sources.  GlobalGather reads the contribution array;
+// HotGather serves indices below `hot` from the copy of the array's prefix
+// in shared memory (the highest in-degree vertices, which a power-law graph
+// gathers most) and the rest with a predicated global load, branch-free.
+struct GlobalGather {
+  const float *cin;
+  uint64_t pol;
+  __device__ __forceinline__ float operator()(int idx) const { return ld_contrib(cin + idx, pol); }
+};
+
+struct HotGather {
+  const float *cin;
+  const float *hot;
+  int n_hot;
+  uint64_t pol;
+  __device__ __forceinline__ float operator()(int idx) const {
+    const float h = hot[min(idx, n_hot - 1)];
+    float g = 0.f;
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ge.s32 p, %1, %2;\n"
+        " @p ld.global.L2::cache_hint.f32 %0, [%3], %4;\n}"
+        : "+f"(g) : "r"(idx), "r"(n_hot), "l"(cin + idx), "l"(pol));
+    return idx < n_hot ? h : g;
+  }
+};
 
 __device__ __forceinline__ float ld_f32_stream(const float *p, uint64_t pol) {
   float v;
@@ -169,8 +209,8 @@ __device__ __forceinline__ double row_update(const PrArgs &a, int r, float sum, 
 
 // One chunk of a long row: U4 16-byte index loads per lane in flight, then
 // 4*U4 independent gathers.
-template <int U4>
-__device__ __forceinline__ double do_chunk(const PrArgs &a, const float *cin, float *cout, int c,
+template <int U4, typename Gather>
+__device__ __forceinline__ double do_chunk(const PrArgs &a, const Gather &gat, float *cout, int c,
                                            int lane, const Policies &pol) {
   const int r = a.chunk_row[c];
   const int cb = a.row_cbeg[r];
@@ -193,10 +233,10 @@ __device__ __forceinline__ double do_chunk(const PrArgs &a, const float *cin, fl
     float v[4 * U4];
 #pragma unroll
     for (int i = 0; i < U4; ++i) {
-      v[4 * i + 0] = ld_contrib(cin + q[i].x, pol.keep);
-      v[4 * i + 1] = ld_contrib(cin + q[i].y, pol.keep);
-      v[4 * i + 2] = ld_contrib(cin + q[i].z, pol.keep);
-      v[4 * i + 3] = ld_contrib(cin + q[i].w, pol.keep);
+      v[4 * i + 0] = gat(q[i].x);
+      v[4 * i + 1] = gat(q[i].y);
+      v[4 * i + 2] = gat(q[i].z);
+      v[4 * i + 3] = gat(q[i].w);
     }
 #pragma unroll
     for (int i = 0; i < 4 * U4; ++i) acc += v[i];
@@ -223,8 +263,8 @@ __device__ __forceinline__ double do_chunk(const PrArgs &a, const float *cin, fl
 // One SELL slice: 32 >> lw rows, w = 1 << lw lanes per row.  Each lane runs
 // batches of U independent index loads followed by U independent gathers;
 // entries past the slice length read the sentinel slot (an exact +0).
-template <int U>
-__device__ __forceinline__ double do_slice(const PrArgs &a, const float *cin, float *cout,
+template <int U, typename Gather>
+__device__ __forceinline__ double do_slice(const PrArgs &a, const Gather &gat, float *cout,
                                            int sidx, int lane, const Policies &pol) {
   const int c = gpr::slice_class(a.cls, sidx);
   const int lw = a.cls.lw[c];
@@ -248,7 +288,7 @@ __device__ __forceinline__ double do_slice(const PrArgs &a, const float *cin, fl
     for (int q = 0; q < U; ++q) ci[q] = (j0 + q < len) ? ld_idx(p + 32 * (j0 + q), pol.stream) : a.m;
     float v[U];
 #pragma unroll
-    for (int q = 0; q < U; ++q) v[q] = ld_contrib(cin + ci[q], pol.keep);
+    for (int q = 0; q < U; ++q) v[q] = gat(ci[q]);
 #pragma unroll
     for (int q = 0; q < U; ++q) acc = __fadd_rn(acc, v[q]);
   }
@@ -286,9 +326,10 @@ __device__ __forceinline__ double sweep(const PrArgs &a, const float *cin, float
   const long long u1 = a.n_chunks, u2 = u1 + a.n_slices;
   const long long u3 = u2 + (it < 2 ? a.n_zblk : 0);
   double err = 0.0;
+  const GlobalGather gat{cin, pol.keep};
   for (long long u = gw; u < u3; u += nw) {
-    if (u < u1) err += do_chunk<U4>(a, cin, cout, (int)u, lane, pol);
-    else if (u < u2) err += do_slice<U>(a, cin, cout, (int)(u - u1), lane, pol);
+    if (u < u1) err += do_chunk<U4>(a, gat, cout, (int)u, lane, pol);
+    else if (u < u2) err += do_slice<U>(a, gat, cout, (int)(u - u1), lane, pol);
     else err += do_zero(a, cout, (int)(u - u2), lane, it, pol);
   }
   return err;
@@ -334,6 +375,7 @@ __device__ bool barrier_reduce(const PrArgs &a, int it, double cta_total) {
       t = warp_sum(t);
       if (threadIdx.x == 0) {
         a.err_hist[it] = t;
+        if (a.wq) atomicExch(a.wq + (it & 1), 0);  // reused by sweep it + 2
         atomicExch(a.bar, 0u);
         __threadfence();
         atomicAdd(a.bar + 1, 1u);
@@ -356,18 +398,49 @@ __device__ bool barrier_reduce(const PrArgs &a, int it, double cta_total) {
   return s_state != 2;
 }
 
-// All sweeps in one cooperative launch.
+// All sweeps in one cooperative launch, one 1024-thread CTA per SM.
+// Each sweep first stages contributions [0, hot) -- the vertices of highest
+// in-degree, which a power-law graph gathers most -- into shared memory, so
+// those gathers never reach the L1->L2 request path.  Warps take batches of
+// kQueueBatch chunk/slice units from a global work queue (one head per sweep
+// parity, reset by the barrier); the batch size is chosen so each warp makes
+// about four grabs per sweep, which keeps the single queue head cold while
+// the light units at the end of the queue still balance the tail.
+// Zero-in-degree rows are spread over all warps in the two sweeps that need
+// them.
+
 template <int U, int U4>
-__global__ void __launch_bounds__(gpr::kBlock) k_pr_persistent(PrArgs a) {
+__global__ void __launch_bounds__(1024, 1) k_pr_hot(PrArgs a) {
+  extern __shared__ float4 s_hot4[];
+  float *s_hot = reinterpret_cast<float *>(s_hot4);
   const int lane = threadIdx.x & 31;
-  const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  const int nwarps = blockDim.x >> 5;
+  const long long gw = (long long)blockIdx.x * nwarps + (threadIdx.x >> 5);
+  const long long nw = (long long)gridDim.x * nwarps;
   const Policies pol = make_policies();
+  const int n_heavy = a.n_chunks + a.n_slices;
   int it = 0;
   while (it < a.max_iter) {
     const float *cin = (it & 1) ? a.c1 : a.c0;
     float *cout = (it & 1) ? a.c0 : a.c1;
-    const double err = sweep<U, U4>(a, cin, cout, gw, nw, lane, it, pol);
+    const float4 *src = reinterpret_cast<const float4 *>(cin);
+    for (int i = threadIdx.x; i < (a.hot >> 2); i += blockDim.x) s_hot4[i] = ld_contrib4(src + i, pol.keep);
+    __syncthreads();
+    const HotGather gat{cin, s_hot, a.hot, pol.keep};
+    double err = 0.0;
+    for (;;) {
+      int u0 = 0;
+      if (lane == 0) u0 = atomicAdd(a.wq + (it & 1), a.batch);
+      u0 = __shfl_sync(kFull, u0, 0);
+      if (u0 >= n_heavy) break;
+      const int u1 = min(u0 + a.batch, n_heavy);
+      for (int u = u0; u < u1; ++u) {
+        if (u < a.n_chunks) err += do_chunk<U4>(a, gat, cout, u, lane, pol);
+        else err += do_slice<U>(a, gat, cout, u - a.n_chunks, lane, pol);
+      }
+    }
+    if (it < 2)
+      for (long long z = gw; z < a.n_zblk; z += nw) err += do_zero(a, cout, (int)z, lane, it, pol);
     const double tot = block_sum(err);
     if (!barrier_reduce(a, it, tot)) return;
     const double total = __ldcg(a.err_hist + it);
@@ -517,11 +590,12 @@ struct SweepKernels {
   void (*step)(PrArgs);
 };
 const SweepKernels kVariants[] = {
-    {(const void *)k_pr_persistent<16, 4>, k_pr_step<16, 4>},
-    {(const void *)k_pr_persistent<8, 2>, k_pr_step<8, 2>},
-    {(const void *)k_pr_persistent<4, 2>, k_pr_step<4, 2>},
-    {(const void *)k_pr_persistent<32, 8>, k_pr_step<32, 8>},
+    {(const void *)k_pr_hot<16, 4>, k_pr_step<16, 4>},
+    {(const void *)k_pr_hot<8, 2>, k_pr_step<8, 2>},
+    {(const void *)k_pr_hot<4, 2>, k_pr_step<4, 2>},
+    {(const void *)k_pr_hot<32, 8>, k_pr_step<32, 8>},
 };
+constexpr int kHotBlock = 1024;
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
 
 PrArgs make_args(gpr_graph *g, const gpr_pr_opts &o) {
@@ -555,7 +629,14 @@ PrArgs make_args(gpr_graph *g, const gpr_pr_opts &o) {
   a.base = (1.0f - o.damping) / (float)L.m;  // src/pr/omp_base.cc:16
   a.tol = o.tol;
   a.max_iter = o.max_iter;
-  a.bar_expect = g->grid_persist[o.variant];
+  a.bar_expect = g->grid_hot;
+  a.hot = g->hot;
+  a.wq = g->wq;
+  {
+    const long long heavy = (long long)L.n_chunks + L.n_slices;
+    const long long warps = (long long)g->grid_hot * (kHotBlock / 32);
+    a.batch = (int)std::max<long long>(1, heavy / (warps * 4));
+  }
   a.timeout_ns = (long long)(o.timeout_s * 1e9);
   return a;
 }
@@ -574,6 +655,7 @@ void destroy(gpr_graph *g) {
   gpr::dfree(g->status);
   gpr::dfree(g->scores_tmp);
   gpr::dfree(g->res_tmp);
+  gpr::dfree(g->wq);
   if (g->e0) cudaEventDestroy(g->e0);
   if (g->e1) cudaEventDestroy(g->e1);
   if (g->e2) cudaEventDestroy(g->e2);
@@ -583,7 +665,8 @@ void destroy(gpr_graph *g) {
 }
 
 int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
-                const int *any_outdeg, int lane_max, int chunk_min, int chunk, gpr_graph *g) {
+                const int *any_outdeg, int lane_max, int chunk_min, int chunk, int hot_max,
+                gpr_graph *g) {
   GPR_CUDA(cudaGetDevice(&g->device));
   GPR_CUDA(cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking));
   g->own_stream = true;
@@ -610,8 +693,15 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
   GPR_TRY(rc);
   const PrLayout &L = g->L;
   GPR_TRY(gpr::dalloc(&g->s, (size_t)m, "scores"));
-  GPR_TRY(gpr::dalloc(&g->c0, (size_t)m + 1, "contrib0"));
-  GPR_TRY(gpr::dalloc(&g->c1, (size_t)m + 1, "contrib1"));
+  // Hot prefix: a multiple of 4 entries, covering the sentinel slot m when
+  // the whole array fits.  Contribution buffers are padded so the staging
+  // loads stay in bounds; the padding stays 0.
+  g->hot = (int)std::min<long long>(hot_max, ((long long)m + 1 + 3) & ~3LL);
+  const size_t cn = (size_t)std::max<long long>((long long)m + 1, g->hot) + 4;
+  GPR_TRY(gpr::dalloc(&g->c0, cn, "contrib0"));
+  GPR_TRY(gpr::dalloc(&g->c1, cn, "contrib1"));
+  GPR_CUDA(cudaMemsetAsync(g->c0, 0, sizeof(float) * cn, st));
+  GPR_CUDA(cudaMemsetAsync(g->c1, 0, sizeof(float) * cn, st));
   GPR_TRY(gpr::dalloc(&g->partial, (size_t)L.n_chunks, "chunk partials"));
   GPR_TRY(gpr::dalloc(&g->cnt, (size_t)L.n_long, "chunk counters"));
   GPR_TRY(gpr::dalloc(&g->bar, 4, "barrier"));
@@ -626,22 +716,23 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
   const long long warps_per_cta = gpr::kBlock / 32;
   const long long need = gpr::ceil_div(units, warps_per_cta);
   g->coop = coop != 0;
-  long long full_max = sms;
+  g->hot_ok = g->coop;
   for (int v = 0; v < kNumVariants; ++v) {
     int per_sm = 0;
+    GPR_CUDA(cudaFuncSetAttribute(kVariants[v].persistent,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(sizeof(float) * g->hot)));
     GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kVariants[v].persistent,
-                                                           gpr::kBlock, 0));
-    const long long full = (long long)sms * (per_sm > 0 ? per_sm : 1);
-    if (per_sm <= 0) g->coop = false;
-    g->grid_persist[v] = (int)(need < full ? (need < 1 ? 1 : need) : full);
-    if (full > full_max) full_max = full;
+                                                           kHotBlock, sizeof(float) * g->hot));
+    if (per_sm < 1) g->hot_ok = false;
   }
+  const long long heavy = (long long)L.n_chunks + L.n_slices;
+  g->grid_hot = (int)std::max<long long>(1, std::min<long long>(sms, gpr::ceil_div(heavy, 32)));
+  GPR_TRY(gpr::dalloc(&g->wq, 2, "work queue"));
   long long step = need < 1 ? 1 : need;
-  if (step > full_max * 4) step = full_max * 4;
+  if (step > (long long)sms * 32) step = (long long)sms * 32;
   g->grid_step = (int)step;
-  g->max_grid = g->grid_step;
-  for (int v = 0; v < kNumVariants; ++v)
-    if (g->grid_persist[v] > g->max_grid) g->max_grid = g->grid_persist[v];
+  g->max_grid = std::max(g->grid_step, g->grid_hot);
   GPR_TRY(gpr::dalloc(&g->cta_err, 2 * (size_t)g->max_grid, "cta residuals"));
   g->err_cap = 128;
   GPR_TRY(gpr::dalloc(&g->err_hist, (size_t)g->err_cap, "residual history"));
@@ -691,6 +782,7 @@ int pagerank_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts_in,
   }
   GPR_CUDA(cudaMemsetAsync(g->bar, 0, 4 * sizeof(unsigned), st));
   GPR_CUDA(cudaMemsetAsync(g->status, 0, 4 * sizeof(int), st));
+  GPR_CUDA(cudaMemsetAsync(g->wq, 0, 2 * sizeof(int), st));
   if (g->L.n_long) GPR_CUDA(cudaMemsetAsync(g->cnt, 0, sizeof(int) * g->L.n_long, st));
   PrArgs a = make_args(g, o);
   if (o.reserved[0] > 0) a.bar_expect += o.reserved[0];  // test hook: a barrier nobody completes
@@ -701,14 +793,14 @@ int pagerank_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts_in,
   ++launches;
   int loop = o.loop;
   if (loop == GPR_LOOP_AUTO) loop = GPR_LOOP_PERSISTENT;
-  if (loop == GPR_LOOP_PERSISTENT && !g->coop) loop = GPR_LOOP_GRAPH;
+  if (loop == GPR_LOOP_PERSISTENT && !g->hot_ok) loop = GPR_LOOP_GRAPH;
   GPR_CUDA(cudaEventRecord(g->e2, st));
   if (o.max_iter > 0) {
     if (loop == GPR_LOOP_PERSISTENT) {
       void *args[] = {&a};
       cudaError_t e = cudaLaunchCooperativeKernel(kVariants[o.variant].persistent,
-                                                  dim3(g->grid_persist[o.variant]),
-                                                  dim3(gpr::kBlock), args, 0, st);
+                                                  dim3(g->grid_hot), dim3(kHotBlock), args,
+                                                  sizeof(float) * g->hot, st);
       if (e == cudaErrorCooperativeLaunchTooLarge) {
         cudaGetLastError();
         loop = GPR_LOOP_GRAPH;
@@ -774,13 +866,15 @@ int gpr_graph_create(int m, long long nnz, const int *any_rowptr, const int *any
 int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr, const int *any_col,
                         const int *any_outdeg, const gpr_layout_opts *lopts, gpr_graph **out) {
   int lane_max = gpr::kSellMaxDefault, chunk = gpr::kChunkDefault,
-      chunk_min = gpr::kChunkMinDefault;
+      chunk_min = gpr::kChunkMinDefault, hot_max = gpr::kHotDefault;
   if (lopts && lopts->sell_max) lane_max = lopts->sell_max;
   if (lopts && lopts->chunk) chunk = lopts->chunk;
   if (lopts && lopts->chunk_min) chunk_min = lopts->chunk_min;
-  if (lane_max < 1 || lane_max > 1024 || chunk < 128 || chunk % 128 != 0 || chunk_min < 1) {
+  if (lopts && lopts->hot_entries) hot_max = lopts->hot_entries;
+  if (lane_max < 1 || lane_max > 1024 || chunk < 128 || chunk % 128 != 0 || chunk_min < 1 ||
+      hot_max < 4 || hot_max > gpr::kHotMax || hot_max % 4 != 0) {
     gpr::set_error("gpr_graph_create_ex: invalid layout options (lane_max %d, chunk %d, "
-                   "chunk_min %d)", lane_max, chunk, chunk_min);
+                   "chunk_min %d, hot_entries %d)", lane_max, chunk, chunk_min, hot_max);
     return GPR_EINVAL;
   }
   if (!out) {
@@ -800,7 +894,8 @@ int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr, const int *
     return GPR_ENODEV;
   }
   gpr_graph *g = new gpr_graph();
-  int rc = create_impl(m, nnz, any_rowptr, any_col, any_outdeg, lane_max, chunk_min, chunk, g);
+  int rc = create_impl(m, nnz, any_rowptr, any_col, any_outdeg, lane_max, chunk_min, chunk,
+                       hot_max, g);
   if (rc != GPR_OK) {
     destroy(g);
     return rc;

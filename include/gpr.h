@@ -97,7 +97,9 @@ typedef struct {
                      one lane, wider rows 2..32 lanes (default 64) */
   int chunk;      /* edges per long-row chunk, multiple of 128 (default 4096) */
   int chunk_min;  /* rows with more in-edges than this are cut into chunks (default 4096) */
-  int reserved[5];
+  int hot_entries;/* contributions of the highest in-degree vertices kept in shared memory
+                     by the persistent kernel, multiple of 4, <= 56832 (default 32768) */
+  int reserved[4];
 } gpr_layout_opts;
 int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr,
                         const int *any_col, const int *any_outdeg,
