@@ -268,8 +268,8 @@ def run_ours(args):
     alg_bytes = per_sweep * sweeps_per_solve
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / (loop_ms / 1e3) / 1e9
-    traffic = load_traffic().get(f"k_pr_persistent_rmat{args.scale}")
-    roof = {"kernel": "k_pr_persistent (all sweeps of one solve)", "bound": "hbm",
+    traffic = load_traffic().get(f"k_pr_hot_rmat{args.scale}")
+    roof = {"kernel": "k_pr_hot (persistent: all sweeps of one solve)", "bound": "hbm",
             "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
             "frac": achieved / peak,
             "traffic": (traffic["bytes_per_sweep"] * sweeps_per_solve) if traffic else None,
@@ -375,6 +375,22 @@ def spmv_leg(G, torch, dev, stream, args):
             "bytes_formula": "8*nnz + 16*m + 4"}
 
 
+def profile_solve(args):
+    """One solve of exactly N sweeps on the benchmark graph (for ncu)."""
+    import torch
+
+    import gardenia_ocl_b200 as G
+    csr = G.gen_rmat(args.scale, EDGE_FACTOR, seed=SEED, abc=ABC)
+    g = G.Graph(csr.rowptr, csr.col, csr.third, m=csr.m, nnz=csr.nnz)
+    scores = torch.full((csr.m,), float(np.float32(1.0) / np.float32(csr.m)),
+                        dtype=torch.float32, device="cuda")
+    _, st = g.pagerank(scores, G.options(tol=0.0, max_iter=args.profile_solve, damping=DAMPING))
+    log(json.dumps({"m": csr.m, "nnz": csr.nnz, "layout": g.layout(), **st.as_dict()}))
+    g.close()
+    csr.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -385,7 +401,12 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-spmv", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-solve", type=int, default=0, metavar="SWEEPS",
+                    help="build the graph and run one solve of exactly SWEEPS sweeps, "
+                         "nothing else (the case profiled with ncu)")
     args = ap.parse_args()
+    if args.profile_solve:
+        return profile_solve(args)
     if args.warmup < 3:
         log("warm-up raised to 3 steps (minimum)")
         args.warmup = 3

@@ -24,6 +24,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <vector>
 
 #include "gpr_internal.cuh"
@@ -47,7 +48,7 @@ struct gpr_graph {
   int err_cap = 0;
   int last_sweeps = 0;
   int hot = 0;                 // contributions staged in shared memory per sweep
-  int grid_hot = 0;            // cooperative grid of the hot kernel (<= 1 CTA per SM)
+  int grid_hot[8] = {0};       // cooperative grid of each persistent variant
   int *wq = nullptr;           // [2] work-queue heads of the hot kernel
   bool hot_ok = false;         // every hot-kernel variant is co-resident at grid_hot
   int grid_step = 0, max_grid = 0;
@@ -153,6 +154,22 @@ struct HotGather {
         " @p ld.global.L2::cache_hint.f32 %0, [%3], %4;\n}"
         : "+f"(g) : "r"(idx), "r"(n_hot), "l"(cin + idx), "l"(pol));
     return idx < n_hot ? h : g;
+  }
+};
+
+// Same sources through one generic-address load: a lane's pointer falls in
+// shared memory for hot indices and in global memory otherwise, so a gather
+// costs one load instruction instead of two.
+struct HotGatherGeneric {
+  const float *cin;
+  const float *hot;
+  int n_hot;
+  uint64_t pol;
+  __device__ __forceinline__ float operator()(int idx) const {
+    const float *p = idx < n_hot ? hot + idx : cin + idx;
+    float v;
+    asm volatile("ld.f32 %0, [%1];" : "=f"(v) : "l"(p));
+    return v;
   }
 };
 
@@ -409,8 +426,8 @@ __device__ bool barrier_reduce(const PrArgs &a, int it, double cta_total) {
 // Zero-in-degree rows are spread over all warps in the two sweeps that need
 // them.
 
-template <int U, int U4>
-__global__ void __launch_bounds__(1024, 1) k_pr_hot(PrArgs a) {
+template <int U, int U4, bool GENERIC, int MINB>
+__global__ void __launch_bounds__(1024, MINB) k_pr_hot(PrArgs a) {
   extern __shared__ float4 s_hot4[];
   float *s_hot = reinterpret_cast<float *>(s_hot4);
   const int lane = threadIdx.x & 31;
@@ -426,7 +443,8 @@ __global__ void __launch_bounds__(1024, 1) k_pr_hot(PrArgs a) {
     const float4 *src = reinterpret_cast<const float4 *>(cin);
     for (int i = threadIdx.x; i < (a.hot >> 2); i += blockDim.x) s_hot4[i] = ld_contrib4(src + i, pol.keep);
     __syncthreads();
-    const HotGather gat{cin, s_hot, a.hot, pol.keep};
+    using Gat = typename std::conditional<GENERIC, HotGatherGeneric, HotGather>::type;
+    const Gat gat{cin, s_hot, a.hot, pol.keep};
     double err = 0.0;
     for (;;) {
       int u0 = 0;
@@ -583,17 +601,24 @@ inline unsigned grid_for(long long n, int block = 256) {
   return (unsigned)(g < 1 ? 1 : g);
 }
 
-// Unroll variants of the sweep kernels: (slice batch U, int4 loads per lane
-// U4).  Variant 0 is the default; the others are the autotuner's choices.
+// Variants of the sweep kernels: (slice batch U, int4 loads per lane U4,
+// one generic load per gather or shared + predicated global, CTAs per SM).
+// Variant 0 is the default; the others are the autotuner's choices.
 struct SweepKernels {
   const void *persistent;
   void (*step)(PrArgs);
+  int ctas_per_sm;  // persistent kernel: co-resident 1024-thread CTAs per SM
+  int hot_cap;      // most contributions one CTA stages (shared memory per CTA)
 };
 const SweepKernels kVariants[] = {
-    {(const void *)k_pr_hot<16, 4>, k_pr_step<16, 4>},
-    {(const void *)k_pr_hot<8, 2>, k_pr_step<8, 2>},
-    {(const void *)k_pr_hot<4, 2>, k_pr_step<4, 2>},
-    {(const void *)k_pr_hot<32, 8>, k_pr_step<32, 8>},
+    {(const void *)k_pr_hot<16, 4, true, 1>, k_pr_step<16, 4>, 1, 56832},
+    {(const void *)k_pr_hot<8, 2, false, 1>, k_pr_step<8, 2>, 1, 56832},
+    {(const void *)k_pr_hot<4, 2, false, 1>, k_pr_step<4, 2>, 1, 56832},
+    {(const void *)k_pr_hot<32, 8, false, 1>, k_pr_step<32, 8>, 1, 56832},
+    {(const void *)k_pr_hot<16, 4, false, 1>, k_pr_step<16, 4>, 1, 56832},
+    {(const void *)k_pr_hot<8, 2, true, 1>, k_pr_step<8, 2>, 1, 56832},
+    {(const void *)k_pr_hot<8, 2, false, 2>, k_pr_step<8, 2>, 2, 24576},
+    {(const void *)k_pr_hot<8, 2, true, 2>, k_pr_step<8, 2>, 2, 24576},
 };
 constexpr int kHotBlock = 1024;
 constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
@@ -629,12 +654,12 @@ PrArgs make_args(gpr_graph *g, const gpr_pr_opts &o) {
   a.base = (1.0f - o.damping) / (float)L.m;  // src/pr/omp_base.cc:16
   a.tol = o.tol;
   a.max_iter = o.max_iter;
-  a.bar_expect = g->grid_hot;
-  a.hot = g->hot;
+  a.bar_expect = g->grid_hot[o.variant];
+  a.hot = std::min(g->hot, kVariants[o.variant].hot_cap);
   a.wq = g->wq;
   {
     const long long heavy = (long long)L.n_chunks + L.n_slices;
-    const long long warps = (long long)g->grid_hot * (kHotBlock / 32);
+    const long long warps = (long long)g->grid_hot[o.variant] * (kHotBlock / 32);
     a.batch = (int)std::max<long long>(1, heavy / (warps * 4));
   }
   a.timeout_ns = (long long)(o.timeout_s * 1e9);
@@ -717,22 +742,25 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
   const long long need = gpr::ceil_div(units, warps_per_cta);
   g->coop = coop != 0;
   g->hot_ok = g->coop;
+  const long long heavy = (long long)L.n_chunks + L.n_slices;
   for (int v = 0; v < kNumVariants; ++v) {
     int per_sm = 0;
+    const int hv = std::min(g->hot, kVariants[v].hot_cap);
     GPR_CUDA(cudaFuncSetAttribute(kVariants[v].persistent,
                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(sizeof(float) * g->hot)));
+                                  (int)(sizeof(float) * hv)));
     GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kVariants[v].persistent,
-                                                           kHotBlock, sizeof(float) * g->hot));
-    if (per_sm < 1) g->hot_ok = false;
+                                                           kHotBlock, sizeof(float) * hv));
+    if (per_sm < kVariants[v].ctas_per_sm) g->hot_ok = false;
+    g->grid_hot[v] = (int)std::max<long long>(
+        1, std::min<long long>((long long)sms * kVariants[v].ctas_per_sm, gpr::ceil_div(heavy, 32)));
   }
-  const long long heavy = (long long)L.n_chunks + L.n_slices;
-  g->grid_hot = (int)std::max<long long>(1, std::min<long long>(sms, gpr::ceil_div(heavy, 32)));
   GPR_TRY(gpr::dalloc(&g->wq, 2, "work queue"));
   long long step = need < 1 ? 1 : need;
   if (step > (long long)sms * 32) step = (long long)sms * 32;
   g->grid_step = (int)step;
-  g->max_grid = std::max(g->grid_step, g->grid_hot);
+  g->max_grid = g->grid_step;
+  for (int v = 0; v < kNumVariants; ++v) g->max_grid = std::max(g->max_grid, g->grid_hot[v]);
   GPR_TRY(gpr::dalloc(&g->cta_err, 2 * (size_t)g->max_grid, "cta residuals"));
   g->err_cap = 128;
   GPR_TRY(gpr::dalloc(&g->err_hist, (size_t)g->err_cap, "residual history"));
@@ -799,8 +827,8 @@ int pagerank_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts_in,
     if (loop == GPR_LOOP_PERSISTENT) {
       void *args[] = {&a};
       cudaError_t e = cudaLaunchCooperativeKernel(kVariants[o.variant].persistent,
-                                                  dim3(g->grid_hot), dim3(kHotBlock), args,
-                                                  sizeof(float) * g->hot, st);
+                                                  dim3(g->grid_hot[o.variant]), dim3(kHotBlock),
+                                                  args, sizeof(float) * a.hot, st);
       if (e == cudaErrorCooperativeLaunchTooLarge) {
         cudaGetLastError();
         loop = GPR_LOOP_GRAPH;

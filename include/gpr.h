@@ -58,7 +58,7 @@ typedef struct {
   int loop;             /* gpr_loop */
   double timeout_s;     /* bound on every device-side wait (grid barrier); default 5 s */
   int refine_max;       /* mixed precision: max FP32 refinement sweeps (default 64) */
-  int variant;          /* sweep-kernel unroll variant, 0..3 (0 = default; see the autotuner) */
+  int variant;          /* sweep-kernel variant, 0..7 (0 = default; the autotuner's choices) */
   int reserved[7];      /* reserved[0] > 0: the grid barrier also waits for that many CTAs
                            that do not exist, so its bounded wait runs out (tests of the
                            GPR_ETIMEOUT path); keep 0 otherwise */

@@ -49,7 +49,7 @@ def test_short_rows_bit_identical(G, O):
 
 
 @pytest.mark.parametrize("maker", [star, degree_ladder])
-@pytest.mark.parametrize("variant", [0, 1, 2, 3])
+@pytest.mark.parametrize("variant", list(range(8)))
 def test_long_rows_and_bins(G, O, maker, variant):
     # The tolerance sits well above the float rounding floor of the L1
     # residual (about m * ulp(score) ~ 1e-7 here), where the sweep count is
