@@ -90,6 +90,9 @@ def lib():
                               C.POINTER(PrStats)]),
         "gpr_page_rank": (I, [I, I, _vp, _vp, _vp, _vp, C.POINTER(PrOptions),
                               C.POINTER(PrStats)]),
+        "gpr_pagerank_noalloc": (I, [I, I, _vp, _vp, _vp, _vp, C.POINTER(PrOptions),
+                                     C.POINTER(PrStats), _vp]),
+        "gpr_pagerank_noalloc_max_vertices": (LL, []),
         "gpr_matrix_create": (I, [I, LL, _vp, _vp, _vp, C.POINTER(_vp)]),
         "gpr_matrix_destroy": (I, [_vp]),
         "gpr_matrix_layout": (I, [_vp, C.POINTER(I), C.POINTER(I), C.POINTER(I), C.POINTER(LL)]),
@@ -294,6 +297,23 @@ def PageRank(m, nnz, row_offsets, column_indices, degree, scores, tol=EPSILON,
         raise TypeError("scores must be float32")
     _check(lib().gpr_page_rank(int(m), int(nnz), *[p for p, _ in ptrs], ps, C.byref(o), C.byref(st)))
     return st
+
+
+def pagerank_noalloc(m, nnz, d_rowptr, d_col, d_outdeg, d_scores, stream_handle=0,
+                     tol=EPSILON, max_iter=MAX_ITER, **kw):
+    """PageRank that allocates no device memory (gpr_pagerank_noalloc): every
+    array must already be on the device; ``d_scores`` is updated in place.
+    For callers whose device memory belongs to their own allocator."""
+    o = options(tol=tol, max_iter=max_iter, **kw)
+    st = PrStats()
+    _check(lib().gpr_pagerank_noalloc(int(m), int(nnz), _ptr(d_rowptr)[0], _ptr(d_col)[0],
+                                      _ptr(d_outdeg)[0], _ptr(d_scores)[0], C.byref(o),
+                                      C.byref(st), C.c_void_p(stream_handle)))
+    return st
+
+
+def pagerank_noalloc_max_vertices() -> int:
+    return int(lib().gpr_pagerank_noalloc_max_vertices())
 
 
 # ---------------------------------------------------------------------------

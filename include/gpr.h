@@ -142,6 +142,26 @@ int gpr_page_rank(int m, int nnz, const int *row_offsets,
                   const int *column_indices, const int *degree, float *scores,
                   const gpr_pr_opts *opts, gpr_pr_stats *stats);
 
+/* ---- PageRank without any allocation ----------------------------------------
+ * No counterpart in the reference.  For callers that cannot let a library
+ * allocate device memory (their allocator owns the device heap, or the call
+ * may not take the synchronisation cudaMalloc / cudaFree can cause): solves
+ * directly on the caller's device CSR (d_rowptr / d_col = in-CSR, d_outdeg =
+ * out-degrees, d_scores in/out, all device memory) on `stream`, with its
+ * scratch in a fixed device array inside the library (about 8 MiB, held by
+ * every GPU that loads the library until exit).  Limits: m <= 1,048,576
+ * vertices (gpr_pagerank_noalloc_max_vertices) and max_iter <= 1000, else
+ * GPR_EINVAL.  The first call on a device looks up the array's device address
+ * and should come before any stream capture.  Calls share the array, so calls
+ * that overlap on the GPU race; run them one at a time.  Synchronous; scores
+ * follow the reference's float arithmetic row by row; opts->loop / variant /
+ * precision are ignored. */
+int gpr_pagerank_noalloc(int m, int nnz, const int *d_rowptr, const int *d_col,
+                         const int *d_outdeg, float *d_scores,
+                         const gpr_pr_opts *opts, gpr_pr_stats *stats,
+                         void *stream);
+long long gpr_pagerank_noalloc_max_vertices(void);
+
 /* ---- SpMV ------------------------------------------------------------------
  * y <- y + A*x over a CSR matrix (src/spmv/spmv.h:29, omp_base.cc:8-32). */
 int gpr_matrix_create(int m, long long nnz, const int *any_Ap,
