@@ -384,7 +384,9 @@ def profile_solve(args):
     g = G.Graph(csr.rowptr, csr.col, csr.third, m=csr.m, nnz=csr.nnz)
     scores = torch.full((csr.m,), float(np.float32(1.0) / np.float32(csr.m)),
                         dtype=torch.float32, device="cuda")
-    _, st = g.pagerank(scores, G.options(tol=0.0, max_iter=args.profile_solve, damping=DAMPING))
+    loop = G.LOOP_PERSISTENT if args.profile_loop == "persistent" else G.LOOP_GRAPH
+    _, st = g.pagerank(scores, G.options(tol=0.0, max_iter=args.profile_solve, damping=DAMPING,
+                                         loop=loop))
     log(json.dumps({"m": csr.m, "nnz": csr.nnz, "layout": g.layout(), **st.as_dict()}))
     g.close()
     csr.close()
@@ -404,6 +406,8 @@ def main():
     ap.add_argument("--profile-solve", type=int, default=0, metavar="SWEEPS",
                     help="build the graph and run one solve of exactly SWEEPS sweeps, "
                          "nothing else (the case profiled with ncu)")
+    ap.add_argument("--profile-loop", choices=["persistent", "graph"], default="persistent",
+                    help="sweep loop of --profile-solve")
     args = ap.parse_args()
     if args.profile_solve:
         return profile_solve(args)
