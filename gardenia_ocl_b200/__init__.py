@@ -43,7 +43,7 @@ class PrOptions(C.Structure):
 
 class LayoutOptions(C.Structure):
     _fields_ = [("sell_max", C.c_int), ("chunk", C.c_int), ("chunk_min", C.c_int),
-                ("hot_entries", C.c_int), ("reserved", C.c_int * 4)]
+                ("hot_entries", C.c_int), ("flags", C.c_int), ("reserved", C.c_int * 3)]
 
 
 class PrStats(C.Structure):
@@ -90,6 +90,7 @@ def lib():
                               C.POINTER(PrStats)]),
         "gpr_page_rank": (I, [I, I, _vp, _vp, _vp, _vp, C.POINTER(PrOptions),
                               C.POINTER(PrStats)]),
+        "gpr_ppr": (I, [_vp, I, _vp, _vp, C.POINTER(PrOptions), _vp, C.POINTER(PrStats)]),
         "gpr_pagerank_noalloc": (I, [I, I, _vp, _vp, _vp, _vp, C.POINTER(PrOptions),
                                      C.POINTER(PrStats), _vp]),
         "gpr_pagerank_noalloc_max_vertices": (LL, []),
@@ -199,7 +200,7 @@ class Graph:
     the out-degree of every vertex (src/pr/omp_base.cc:9 arguments)."""
 
     def __init__(self, rowptr, col, outdeg, m=None, nnz=None, sell_max=0, chunk=0, chunk_min=0,
-                 hot_entries=0):
+                 hot_entries=0, batched=False):
         L = lib()
         m = int(len(rowptr) - 1) if m is None else int(m)
         nnz = int(len(col)) if nnz is None else int(nnz)
@@ -207,7 +208,8 @@ class Graph:
         pc, k1 = _ptr(col, np.int32)
         pd, k2 = _ptr(outdeg, np.int32)
         h = C.c_void_p()
-        lo = LayoutOptions(int(sell_max), int(chunk), int(chunk_min), int(hot_entries))
+        lo = LayoutOptions(int(sell_max), int(chunk), int(chunk_min), int(hot_entries),
+                           1 if batched else 0)
         _check(L.gpr_graph_create_ex(m, nnz, pr, pc, pd, C.byref(lo), C.byref(h)))
         self._h, self.m, self.nnz = h, m, nnz
         self.last_stats = None
@@ -226,6 +228,21 @@ class Graph:
         _check(lib().gpr_pagerank(self._h, ps, C.byref(o), C.byref(st)))
         self.last_stats = st
         return scores, st
+
+    def ppr(self, seeds, out=None, opts: PrOptions | None = None, **kw):
+        """Batched personalized PageRank for len(seeds) <= 128 seed vertices
+        (graph created with batched=True).  Returns (x[m, k] float32, iters[k],
+        stats); ``out`` may be a device buffer of m*k floats."""
+        o = opts if opts is not None else options(**kw)
+        seeds = np.ascontiguousarray(seeds, dtype=np.int32)
+        k = len(seeds)
+        x = np.empty((self.m, k), dtype=np.float32) if out is None else out
+        iters = np.zeros(k, dtype=np.int32)
+        st = PrStats()
+        px, keep = _ptr(x)
+        _check(lib().gpr_ppr(self._h, k, C.c_void_p(seeds.ctypes.data), px, C.byref(o),
+                             C.c_void_p(iters.ctypes.data), C.byref(st)))
+        return x, iters, st
 
     def residuals(self):
         n = self.last_stats.iterations if self.last_stats else 0

@@ -74,6 +74,8 @@ struct PrLayout {
   int *chunk_row = nullptr;       // [n_chunks] row of each chunk
   long long *slice_ptr = nullptr; // [n_slices+1] offsets into sell_col
   int *sell_col = nullptr;        // relabelled sources, SELL-32 column-major
+  int *csr_ptr = nullptr;         // [m+1] relabelled CSR (batched solvers only)
+  int *csr_col = nullptr;         // [nnz]
   long long long_elems = 0, sell_elems = 0;
   long long device_bytes = 0;
 };
@@ -87,7 +89,7 @@ __host__ __device__ inline int slice_class(const PrClasses &c, int s) {
 
 int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
                     const int *d_outdeg, int lane_max, int chunk_min, int chunk,
-                    PrLayout *L, cudaStream_t st);
+                    bool keep_csr, PrLayout *L, cudaStream_t st);
 void free_pr_layout(PrLayout *L);
 
 // Validates a device CSR (rowptr[0] = 0, monotone, rowptr[m] = nnz, every
@@ -142,6 +144,38 @@ void free_spmv_layout(SpmvLayout *L);
     int s_ = (call);                                                          \
     if (s_ != GPR_OK) return s_;                                              \
   } while (0)
+
+// Device-resident pull graph behind the opaque gpr_graph handle.
+struct gpr_graph {
+  int device = 0;
+  gpr::PrLayout L;
+  float *s = nullptr;        // [m] scores, new order
+  float *c0 = nullptr;       // [m+1] contributions (sweep parity 0 input)
+  float *c1 = nullptr;       // [m+1]
+  float *partial = nullptr;  // [n_chunks] partial sums of long-row chunks
+  int *cnt = nullptr;        // [n_long] arrival counters of multi-chunk rows
+  double *cta_err = nullptr; // [2 * max grid] per-CTA residual partials
+  double *err_hist = nullptr;// [err_cap] residual of every sweep
+  unsigned *bar = nullptr;   // [4] grid barrier: arrivals, generation
+  int *status = nullptr;     // [4] error flags, sweeps done, done flag
+  float *scores_tmp = nullptr; // [m] device copy of host scores
+  double *res_tmp = nullptr;   // [m+1+n_long] FP64 residual scratch
+  int err_cap = 0;
+  int last_sweeps = 0;
+  int hot = 0;                 // contributions staged in shared memory per sweep
+  int grid_hot[8] = {0};  // cooperative grid of each persistent variant
+  int *wq = nullptr;           // [2] work-queue heads of the hot kernel
+  bool hot_ok = false;         // every hot-kernel variant is co-resident at grid_hot
+  int grid_step = 0, max_grid = 0;
+  bool coop = false;
+  cudaStream_t st = nullptr;
+  bool own_stream = false;
+  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
+  // Chunk table of the batched solver (rows above b_dmax in-edges cut into
+  // b_chunk-edge chunks), built on first use for a given (b_dmax, b_chunk).
+  int *b_cbeg = nullptr, *b_crow = nullptr;
+  int b_nlong = -1, b_nchunks = 0, b_dmax = 0, b_chunk = 0;
+};
 
 namespace gpr {
 constexpr int kZeroRowsPerUnit = 128;  // rows per zero-in-degree work unit

@@ -142,6 +142,26 @@ __global__ void k_fill_sell(int n_slices, int m, PrClasses cls, const int *__res
   }
 }
 
+__global__ void k_csr_lens(int m, const int *__restrict__ sdeg, int *len) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) len[i] = sdeg[i];
+  else if (i == m) len[i] = 0;
+}
+
+// One warp per row: relabelled CSR in new row order, edge order preserved.
+__global__ void k_fill_csr(int m, const int *__restrict__ perm, const int *__restrict__ inv,
+                           const int *__restrict__ rowptr, const int *__restrict__ col,
+                           const int *__restrict__ nptr, int *ncol) {
+  int lane = threadIdx.x & 31;
+  long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long r = w; r < m; r += nw) {
+    const long long sb = rowptr[perm[r]];
+    const long long db = nptr[r], deg = nptr[r + 1] - db;
+    for (long long k = lane; k < deg; k += 32) ncol[db + k] = inv[col[sb + k]];
+  }
+}
+
 template <typename T>
 int exclusive_scan(T *d, long long n, cudaStream_t st) {
   size_t tmp_bytes = 0;
@@ -205,8 +225,8 @@ int validate_csr(int m, long long nnz, int ncols, const int *d_rowptr, const int
 }
 
 int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
-                    const int *d_outdeg, int lane_max, int chunk_min, int chunk, PrLayout *L,
-                    cudaStream_t st) {
+                    const int *d_outdeg, int lane_max, int chunk_min, int chunk, bool keep_csr,
+                    PrLayout *L, cudaStream_t st) {
   *L = PrLayout();
   L->m = m;
   L->nnz = nnz;
@@ -318,11 +338,20 @@ int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
     k_fill_sell<<<grid_for(32LL * L->n_slices), 256, 0, st>>>(
         L->n_slices, m, C, L->perm, inv, d_rowptr, d_col, sdeg, L->slice_ptr, L->sell_col);
   L->n_zblk = (int)ceil_div((long long)m - L->n_nz, kZeroRowsPerUnit);
+  if (keep_csr) {
+    GPR_TRY(dalloc(&L->csr_ptr, (size_t)m + 1, "relabelled row offsets"));
+    GPR_TRY(dalloc(&L->csr_col, (size_t)nnz, "relabelled columns"));
+    k_csr_lens<<<grid_for((long long)m + 1), 256, 0, st>>>(m, sdeg, L->csr_ptr);
+    GPR_TRY(exclusive_scan(L->csr_ptr, (long long)m + 1, st));
+    unsigned g = grid_for(32LL * m);
+    if (g > 148u * 64u) g = 148u * 64u;
+    k_fill_csr<<<g, 256, 0, st>>>(m, L->perm, inv, d_rowptr, d_col, L->csr_ptr, L->csr_col);
+  }
   GPR_CUDA(cudaGetLastError());
   GPR_CUDA(cudaStreamSynchronize(st));
   L->device_bytes = 4LL * (2LL * m) + 8LL * (L->n_long + 1) + 4LL * L->long_elems +
                     4LL * (L->n_long + 1) + 4LL * L->n_chunks + 8LL * (L->n_slices + 1) +
-                    4LL * L->sell_elems;
+                    4LL * L->sell_elems + (keep_csr ? 4LL * (m + 1) + 4LL * nnz : 0);
   return GPR_OK;
 }
 
@@ -335,6 +364,8 @@ void free_pr_layout(PrLayout *L) {
   dfree(L->chunk_row);
   dfree(L->slice_ptr);
   dfree(L->sell_col);
+  dfree(L->csr_ptr);
+  dfree(L->csr_col);
   *L = PrLayout();
 }
 

@@ -31,32 +31,7 @@
 
 using gpr::PrLayout;
 
-struct gpr_graph {
-  int device = 0;
-  PrLayout L;
-  float *s = nullptr;        // [m] scores, new order
-  float *c0 = nullptr;       // [m+1] contributions (sweep parity 0 input)
-  float *c1 = nullptr;       // [m+1]
-  float *partial = nullptr;  // [n_chunks] partial sums of long-row chunks
-  int *cnt = nullptr;        // [n_long] arrival counters of multi-chunk rows
-  double *cta_err = nullptr; // [2 * max grid] per-CTA residual partials
-  double *err_hist = nullptr;// [err_cap] residual of every sweep
-  unsigned *bar = nullptr;   // [4] grid barrier: arrivals, generation
-  int *status = nullptr;     // [4] error flags, sweeps done, done flag
-  float *scores_tmp = nullptr; // [m] device copy of host scores
-  double *res_tmp = nullptr;   // [m+1+n_long] FP64 residual scratch
-  int err_cap = 0;
-  int last_sweeps = 0;
-  int hot = 0;                 // contributions staged in shared memory per sweep
-  int grid_hot[8] = {0};       // cooperative grid of each persistent variant
-  int *wq = nullptr;           // [2] work-queue heads of the hot kernel
-  bool hot_ok = false;         // every hot-kernel variant is co-resident at grid_hot
-  int grid_step = 0, max_grid = 0;
-  bool coop = false;
-  cudaStream_t st = nullptr;
-  bool own_stream = false;
-  cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
-};
+     
 
 namespace {
 
@@ -681,6 +656,8 @@ void destroy(gpr_graph *g) {
   gpr::dfree(g->scores_tmp);
   gpr::dfree(g->res_tmp);
   gpr::dfree(g->wq);
+  gpr::dfree(g->b_cbeg);
+  gpr::dfree(g->b_crow);
   if (g->e0) cudaEventDestroy(g->e0);
   if (g->e1) cudaEventDestroy(g->e1);
   if (g->e2) cudaEventDestroy(g->e2);
@@ -691,7 +668,7 @@ void destroy(gpr_graph *g) {
 
 int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
                 const int *any_outdeg, int lane_max, int chunk_min, int chunk, int hot_max,
-                gpr_graph *g) {
+                bool keep_csr, gpr_graph *g) {
   GPR_CUDA(cudaGetDevice(&g->device));
   GPR_CUDA(cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking));
   g->own_stream = true;
@@ -710,7 +687,7 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
     rc = gpr::validate_csr(m, nnz, m, (const int *)rp, (const int *)cp, (const int *)dp, st);
   if (rc == GPR_OK)
     rc = gpr::build_pr_layout(m, nnz, (const int *)rp, (const int *)cp, (const int *)dp,
-                              lane_max, chunk_min, chunk, &g->L, st);
+                              lane_max, chunk_min, chunk, keep_csr, &g->L, st);
   cudaStreamSynchronize(st);
   if (orp) cudaFree(rp);
   if (ocp) cudaFree(cp);
@@ -922,8 +899,9 @@ int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr, const int *
     return GPR_ENODEV;
   }
   gpr_graph *g = new gpr_graph();
+  const bool keep_csr = lopts && (lopts->flags & GPR_LAYOUT_BATCHED);
   int rc = create_impl(m, nnz, any_rowptr, any_col, any_outdeg, lane_max, chunk_min, chunk,
-                       hot_max, g);
+                       hot_max, keep_csr, g);
   if (rc != GPR_OK) {
     destroy(g);
     return rc;

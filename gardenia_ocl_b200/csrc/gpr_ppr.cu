@@ -1,0 +1,798 @@
+// Batched personalized PageRank: k seed vectors solved together as a fused
+// pull-SpMM in one persistent cooperative launch.
+//
+// No reference file: the reference computes one global PageRank
+// (src/pr/omp_base.cc).  For each vector q with seed s_q:
+//   x_new[v][q] = d * sum_{u in in(v)} x[u][q] / outdeg[u]
+//               + [v == s_q] * ((1 - d) + d * dangling_q)
+//   dangling_q  = sum over out-degree-0 vertices u of x[u][q]   (FP64)
+// x starts at e_{s_q}; vector q stops updating after the first sweep whose
+// FP64 L1 change is below tol (oracle/oracle.c orc_ppr_f64 restates this).
+//
+// Layout: the graph's relabelled CSR (descending in-degree), x[m][K] FP32,
+// contributions c[m+1][K] in FP32 or BF16 (double-buffered by sweep parity,
+// row m is a zero sentinel), K = the vector count rounded up to 8..128.  One
+// gather of an in-neighbour's row serves all K vectors, so the 4-byte index
+// stream and the per-request cost are shared by K edge-vector pairs.
+//   lanes per row L = 8 (K <= 32) or K / 4, rows per warp R = 32 / L,
+//   components per lane C = K / L <= 4 (contiguous, one vector load per
+//   gather).
+// Rows with in-degree 0 hold x = 0 except at seeds, so only rows with
+// in-edges and the k seed rows are updated.  Rows above chunk_min in-edges
+// are cut into chunks whose K-wide partial sums the last arriving warp adds
+// in a fixed order.  Residual and dangling sums are reduced per CTA and then
+// over CTAs in CTA order by the last CTA at the grid barrier (deterministic);
+// every barrier wait is bounded.
+#include <cub/cub.cuh>
+#include <cuda_bf16.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "gpr_internal.cuh"
+
+namespace {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kPprBlock = 256;
+
+struct PprArgs {
+  int m, n_long, n_nz, n_chunks, chunk, k, n_row_units;
+  const int *csr_ptr, *csr_col, *row_cbeg, *chunk_row, *outdeg;
+  float *x;              // [m][K]
+  void *c0, *c1;         // [m+1][K] of T
+  float *partial;        // [n_chunks][K]
+  int *cnt;              // [n_long]
+  const int *seed;       // [K] relabelled seed vertex (-1: padding vector)
+  double *cta_red;       // [2][G][K]: residual, dangling
+  double *seed_red;      // [2][K]: residual, dangling of in-degree-0 seed rows
+  double *res_hist;      // [max_iter][K]
+  double *dang;          // [2][K] dangling mass of the current iterate, by parity
+  unsigned *active;      // [2][4] bit q: vector q still updating, by parity
+  int *iters;            // [K]
+  unsigned *bar;         // [2] arrivals, generation
+  int *status;           // [0] error flags, [1] sweeps, [2] any active
+  int *wq;               // [2] work-queue heads by parity
+  float damp;
+  double tol;
+  int max_iter, batch, bar_expect;
+  long long timeout_ns;
+};
+
+// Lanes per row L, rows per warp R, components per lane C (<= 4, so one
+// gather is at most a 16-byte load): K=8 -> 8x4x1, 16 -> 8x4x2, 32 -> 8x4x4,
+// 64 -> 16x2x4, 128 -> 32x1x4.
+template <int K>
+struct Shape {
+  static constexpr int L = K <= 32 ? 8 : K / 4;
+  static constexpr int R = 32 / L;
+  static constexpr int C = K / L;
+};
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+
+__device__ __forceinline__ long long global_ns() {
+  long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
+__device__ __forceinline__ int ld_idx(const int *p) {
+  int v;
+  asm("ld.global.nc.L1::no_allocate.s32 %0, [%1];" : "=r"(v) : "l"(p));
+  return v;
+}
+
+// C consecutive components of one contribution row, widened to float.
+template <int C>
+__device__ __forceinline__ void load_row(const float *p, float (&v)[C]) {
+  if constexpr (C == 1) {
+    asm volatile("ld.global.f32 %0, [%1];" : "=f"(v[0]) : "l"(p));
+  } else if constexpr (C == 2) {
+    asm volatile("ld.global.v2.f32 {%0,%1}, [%2];" : "=f"(v[0]), "=f"(v[1]) : "l"(p));
+  } else {
+    asm volatile("ld.global.v4.f32 {%0,%1,%2,%3}, [%4];"
+                 : "=f"(v[0]), "=f"(v[1]), "=f"(v[2]), "=f"(v[3]) : "l"(p));
+  }
+}
+
+template <int C>
+__device__ __forceinline__ void load_row(const __nv_bfloat16 *p, float (&v)[C]) {
+  if constexpr (C == 1) {
+    unsigned short h;
+    asm volatile("ld.global.u16 %0, [%1];" : "=h"(h) : "l"(p));
+    v[0] = __uint_as_float((unsigned)h << 16);
+  } else if constexpr (C == 2) {
+    unsigned w;
+    asm volatile("ld.global.u32 %0, [%1];" : "=r"(w) : "l"(p));
+    v[0] = __uint_as_float(w << 16);
+    v[1] = __uint_as_float(w & 0xffff0000u);
+  } else {
+    unsigned w0, w1;
+    asm volatile("ld.global.v2.u32 {%0,%1}, [%2];" : "=r"(w0), "=r"(w1) : "l"(p));
+    v[0] = __uint_as_float(w0 << 16);
+    v[1] = __uint_as_float(w0 & 0xffff0000u);
+    v[2] = __uint_as_float(w1 << 16);
+    v[3] = __uint_as_float(w1 & 0xffff0000u);
+  }
+}
+
+__device__ __forceinline__ void store_c(float *p, float v) { *p = v; }
+__device__ __forceinline__ void store_c(__nv_bfloat16 *p, float v) { *p = __float2bfloat16_rn(v); }
+
+__device__ __forceinline__ bool is_active(const unsigned (&act)[4], int q) {
+  return (act[q >> 5] >> (q & 31)) & 1u;
+}
+
+// Sums in-neighbour rows over `niter` rounds; niter is warp-uniform.  In
+// round j this lane's sub-group covers edges [first + j*stride, +L) clipped
+// to `end`: each lane loads one index, the sub-group broadcasts them, and
+// every lane gathers its C components of each row.  Lanes past their
+// sub-group's end (or with no live component) gather the zero sentinel row,
+// so every shuffle runs on the full warp.
+template <int K, typename T>
+__device__ __forceinline__ void gather_edges(const PprArgs &a, const T *cin, long long first,
+                                             long long end, long long stride, int niter, int lq,
+                                             bool live, float (&acc)[Shape<K>::C]) {
+  constexpr int L = Shape<K>::L, C = Shape<K>::C;
+  int nxt = (niter > 0 && first + lq < end) ? ld_idx(a.csr_col + first + lq) : a.m;
+  for (int j = 0; j < niter; ++j) {
+    const long long eb = first + (long long)j * stride;
+    const int my = nxt;
+    // next round's indices are in flight while this round gathers
+    nxt = (j + 1 < niter && eb + stride + lq < end) ? ld_idx(a.csr_col + eb + stride + lq) : a.m;
+    const int ng = (int)max(0LL, min((long long)L, end - eb));
+    const int nmax = (int)__reduce_max_sync(kFull, (unsigned)ng);
+    // UB = 8 gathers in flight per lane (up to 32 floats of row data).
+    constexpr int UB = 8;
+    for (int t0 = 0; t0 < nmax; t0 += UB) {
+      float v[UB][C];
+#pragma unroll
+      for (int t = 0; t < UB; ++t) {
+        const int u = __shfl_sync(kFull, my, (t0 + t) & (L - 1), L);
+        const int uu = (t0 + t < ng && live) ? u : a.m;
+        load_row<C>(cin + (size_t)uu * K + lq * C, v[t]);
+      }
+#pragma unroll
+      for (int t = 0; t < UB; ++t)
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[c] += v[t][c];
+    }
+  }
+}
+
+// Update of row v from its pulled sums (acc) for this lane's components.
+template <int K, typename T>
+__device__ __forceinline__ void row_update(const PprArgs &a, T *cout, int v, int lq,
+                                           const unsigned (&act)[4], const double *dang_cur,
+                                           const float (&acc)[Shape<K>::C],
+                                           double (&err)[Shape<K>::C], double (&dng)[Shape<K>::C]) {
+  constexpr int C = Shape<K>::C;
+  const int od = a.outdeg[v];
+  const float inv = od > 0 ? 1.0f / (float)od : 0.f;
+#pragma unroll
+  for (int c = 0; c < C; ++c) {
+    const int q = lq * C + c;
+    if (!is_active(act, q)) continue;
+    float xn = a.damp * acc[c];
+    if (a.seed[q] == v) xn += (float)((1.0 - (double)a.damp) + (double)a.damp * dang_cur[q]);
+    const size_t o = (size_t)v * K + q;
+    const float xo = a.x[o];
+    a.x[o] = xn;
+    err[c] += fabs((double)xn - (double)xo);
+    store_c(cout + o, od > 0 ? xn * inv : 0.f);
+    if (od == 0) dng[c] += (double)xn;
+  }
+}
+
+template <int K, typename T>
+__global__ void __launch_bounds__(kPprBlock) k_ppr(PprArgs a) {
+  constexpr int L = Shape<K>::L, R = Shape<K>::R, C = Shape<K>::C;
+  extern __shared__ double s_red[];  // [2][warps][K]
+  __shared__ unsigned s_act[4];
+  __shared__ int s_state;
+  __shared__ unsigned s_gen;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int g = lane / L, lq = lane % L;
+  const int G = gridDim.x;
+  const int n_units = a.n_chunks + a.n_row_units;
+  int it = 0;
+  while (it < a.max_iter) {
+    const T *cin = reinterpret_cast<const T *>((it & 1) ? a.c1 : a.c0);
+    T *cout = reinterpret_cast<T *>((it & 1) ? a.c0 : a.c1);
+    const double *dang_cur = a.dang + (it & 1) * K;
+    unsigned act[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) act[i] = __ldcg(a.active + (it & 1) * 4 + i);
+    bool live = false;
+#pragma unroll
+    for (int c = 0; c < C; ++c) live |= is_active(act, lq * C + c);
+    double err[C], dng[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) err[c] = dng[c] = 0.0;
+    for (;;) {
+      int u0 = 0;
+      if (lane == 0) u0 = atomicAdd(a.wq + (it & 1), a.batch);
+      u0 = __shfl_sync(kFull, u0, 0);
+      if (u0 >= n_units) break;
+      const int u1 = min(u0 + a.batch, n_units);
+      for (int u = u0; u < u1; ++u) {
+        float acc[C];
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[c] = 0.f;
+        if (u < a.n_chunks) {
+          const int r = a.chunk_row[u];
+          const int cb = a.row_cbeg[r], nc = a.row_cbeg[r + 1] - cb;
+          const long long b = a.csr_ptr[r] + (long long)(u - cb) * a.chunk;
+          const long long e = min(b + (long long)a.chunk, (long long)a.csr_ptr[r + 1]);
+          const int niter = (int)gpr::ceil_div(e - b, (long long)R * L);
+          gather_edges<K, T>(a, cin, b + (long long)g * L, e, (long long)R * L, niter, lq, live,
+                             acc);
+#pragma unroll
+          for (int o = L; o < 32; o <<= 1)
+#pragma unroll
+            for (int c = 0; c < C; ++c) acc[c] += __shfl_xor_sync(kFull, acc[c], o);
+          if (nc == 1) {
+            if (g == 0) row_update<K, T>(a, cout, r, lq, act, dang_cur, acc, err, dng);
+            continue;
+          }
+          if (g == 0)
+#pragma unroll
+            for (int c = 0; c < C; ++c) a.partial[(size_t)u * K + lq * C + c] = acc[c];
+          __threadfence();
+          __syncwarp();
+          int last = 0;
+          if (lane == 0) last = atomicAdd(a.cnt + r, 1) == nc - 1;
+          last = __shfl_sync(kFull, last, 0);
+          if (!last) continue;
+          __threadfence();
+          // Sum the row's chunk partials in chunk order (sub-group 0).
+#pragma unroll
+          for (int c = 0; c < C; ++c) acc[c] = 0.f;
+          for (int q = 0; q < nc; ++q)
+#pragma unroll
+            for (int c = 0; c < C; ++c) acc[c] += __ldcg(a.partial + (size_t)(cb + q) * K + lq * C + c);
+          if (lane == 0) atomicExch(a.cnt + r, 0);
+          if (g == 0) row_update<K, T>(a, cout, r, lq, act, dang_cur, acc, err, dng);
+        } else {
+          const int v = a.n_long + (u - a.n_chunks) * R + g;
+          long long e0 = 0, e1 = 0;
+          if (v < a.n_nz) {
+            e0 = a.csr_ptr[v];
+            e1 = a.csr_ptr[v + 1];
+          }
+          // Rows of one warp have nearly equal degrees (degree order); the
+          // sub-groups loop to the warp's longest row.
+          long long span = e1 - e0;
+#pragma unroll
+          for (int o = L; o < 32; o <<= 1) span = max(span, __shfl_xor_sync(kFull, span, o));
+          gather_edges<K, T>(a, cin, e0, e1, (long long)L, (int)gpr::ceil_div(span, L), lq,
+                             live && v < a.n_nz, acc);
+          if (v < a.n_nz) {
+            // edges past this row's end gathered the sentinel row (zeros)
+            row_update<K, T>(a, cout, v, lq, act, dang_cur, acc, err, dng);
+          }
+        }
+      }
+    }
+    // Seed rows without in-edges: only their teleport term changes.
+    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+    if (gt < a.k) {
+      const int q = gt, v = a.seed[q];
+      double se = 0.0, sd = 0.0;
+      if (v >= a.n_nz && is_active(act, q)) {
+        const float xn = (float)((1.0 - (double)a.damp) + (double)a.damp * dang_cur[q]);
+        const size_t o = (size_t)v * K + q;
+        const float xo = a.x[o];
+        const int od = a.outdeg[v];
+        a.x[o] = xn;
+        store_c(cout + o, od > 0 ? xn * (1.0f / (float)od) : 0.f);
+        se = fabs((double)xn - (double)xo);
+        if (od == 0) sd = (double)xn;
+      }
+      a.seed_red[q] = se;
+      a.seed_red[K + q] = sd;
+    }
+    // CTA reduction: sub-groups, then warps in order.
+#pragma unroll
+    for (int o = L; o < 32; o <<= 1)
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        err[c] += __shfl_xor_sync(kFull, err[c], o);
+        dng[c] += __shfl_xor_sync(kFull, dng[c], o);
+      }
+    if (g == 0)
+#pragma unroll
+      for (int c = 0; c < C; ++c) {
+        s_red[(size_t)wid * K + lq * C + c] = err[c];
+        s_red[(size_t)(nwarps + wid) * K + lq * C + c] = dng[c];
+      }
+    __syncthreads();
+    for (int q = threadIdx.x; q < K; q += blockDim.x) {
+      double te = 0.0, td = 0.0;
+      for (int w = 0; w < nwarps; ++w) {
+        te += s_red[(size_t)w * K + q];
+        td += s_red[(size_t)(nwarps + w) * K + q];
+      }
+      a.cta_red[(size_t)blockIdx.x * K + q] = te;
+      a.cta_red[(size_t)(G + blockIdx.x) * K + q] = td;
+    }
+    __syncthreads();
+    // Grid barrier; the last CTA reduces over CTAs and decides which
+    // vectors keep updating.
+    if (threadIdx.x == 0) {
+      s_gen = ld_acquire(a.bar + 1);
+      __threadfence();
+      const unsigned arrived = atomicAdd(a.bar, 1u);
+      s_state = (arrived == (unsigned)a.bar_expect - 1u) ? 1 : 0;
+    }
+    __syncthreads();
+    if (s_state == 1) {
+      __threadfence();
+      if (threadIdx.x < 4) s_act[threadIdx.x] = act[threadIdx.x];
+      __syncthreads();
+      for (int q = threadIdx.x; q < K; q += blockDim.x) {
+        double te = __ldcg(a.seed_red + q), td = __ldcg(a.seed_red + K + q);
+        for (int c = 0; c < G; ++c) {
+          te += __ldcg(a.cta_red + (size_t)c * K + q);
+          td += __ldcg(a.cta_red + (size_t)(G + c) * K + q);
+        }
+        a.res_hist[(size_t)it * K + q] = te;
+        const bool was = is_active(act, q);
+        a.dang[((it + 1) & 1) * K + q] = was ? td : dang_cur[q];
+        if (was) {
+          a.iters[q] = it + 1;
+          if (te < a.tol) atomicAnd(&s_act[q >> 5], ~(1u << (q & 31)));
+        }
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        unsigned any = 0;
+        for (int i = 0; i < 4; ++i) {
+          a.active[((it + 1) & 1) * 4 + i] = s_act[i];
+          any |= s_act[i];
+        }
+        a.status[2] = any != 0;
+        atomicExch(a.wq + (it & 1), 0);
+        atomicExch(a.bar, 0u);
+        __threadfence();
+        atomicAdd(a.bar + 1, 1u);
+      }
+    } else if (threadIdx.x == 0) {
+      const long long t0 = global_ns();
+      unsigned spins = 0;
+      while (ld_acquire(a.bar + 1) == s_gen) {
+        if ((++spins & 31u) == 0 && global_ns() - t0 > a.timeout_ns) {
+          atomicOr(a.status, 1);
+          s_state = 2;
+          break;
+        }
+        __nanosleep(100);
+      }
+      __threadfence();
+    }
+    __syncthreads();
+    if (s_state == 2) return;
+    ++it;
+    if (!__ldcg(a.status + 2)) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) a.status[1] = it;
+}
+
+// x = e_seed, contributions of the seeds, initial dangling mass and masks.
+template <int K, typename T>
+__global__ void k_ppr_init(PprArgs a) {
+  const int q = blockIdx.x * blockDim.x + threadIdx.x;
+  if (q < K) {
+    const int v = q < a.k ? a.seed[q] : -1;
+    if (v >= 0) {
+      const int od = a.outdeg[v];
+      a.x[(size_t)v * K + q] = 1.0f;
+      store_c(reinterpret_cast<T *>(a.c0) + (size_t)v * K + q, od > 0 ? 1.0f / (float)od : 0.f);
+      a.dang[q] = od == 0 ? 1.0 : 0.0;
+    } else {
+      a.dang[q] = 0.0;
+    }
+    a.iters[q] = 0;
+  }
+  if (q < 4) {
+    unsigned w = 0;
+    for (int b = 0; b < 32; ++b)
+      if (q * 32 + b < a.k) w |= 1u << b;
+    a.active[q] = w;
+    a.active[4 + q] = w;
+  }
+}
+
+// Start of the FP32 refinement after the BF16 phase: FP32 contributions of
+// the current iterate, its dangling mass, every vector active again.
+template <int K>
+__global__ void k_ppr_refine_init(PprArgs a, const double *__restrict__ dang_src) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < (long long)a.m * K) {
+    const int v = (int)(t / K), q = (int)(t % K);
+    const int od = a.outdeg[v];
+    reinterpret_cast<float *>(a.c0)[t] = (q < a.k && od > 0) ? a.x[t] / (float)od : 0.f;
+  }
+  if (t < K) {
+    a.dang[t] = dang_src[t];
+    a.iters[t] = 0;
+  }
+  if (t < 4) {
+    unsigned w = 0;
+    for (int b = 0; b < 32; ++b)
+      if ((int)t * 32 + b < a.k) w |= 1u << b;
+    a.active[t] = w;
+    a.active[4 + t] = w;
+  }
+}
+
+template <int K>
+__global__ void k_ppr_scatter(int m, int k, const int *__restrict__ perm,
+                              const float *__restrict__ x, float *out) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)m * k) return;
+  const int v = (int)(t / k), q = (int)(t % k);
+  out[(size_t)perm[v] * k + q] = x[(size_t)v * K + q];
+}
+
+__global__ void k_invert_for_seeds(int m, const int *__restrict__ perm, int k,
+                                   const int *__restrict__ seeds_old, int *seed_new) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  if (v >= m) return;
+  const int o = perm[v];
+  for (int q = 0; q < k; ++q)
+    if (seeds_old[q] == o) seed_new[q] = v;
+}
+
+// ---- batched-solver chunk table --------------------------------------------
+__global__ void k_b_count(int n_nz, const int *__restrict__ ptr, int dmax, int *out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_nz) return;
+  const int d = ptr[r + 1] - ptr[r];
+  const int dn = r + 1 < n_nz ? ptr[r + 2] - ptr[r + 1] : -1;
+  if (d > dmax && dn <= dmax) *out = r + 1;  // rows are in descending degree order
+}
+
+__global__ void k_b_lens(int n, const int *__restrict__ ptr, int chunk, int *nch) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < n) nch[r] = (ptr[r + 1] - ptr[r] + chunk - 1) / chunk;
+  else if (r == n) nch[r] = 0;
+}
+
+__global__ void k_b_fill(int n, const int *__restrict__ cbeg, int *crow) {
+  const int lane = threadIdx.x & 31;
+  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+  for (long long r = w; r < n; r += nw)
+    for (int c = cbeg[r] + lane; c < cbeg[r + 1]; c += 32) crow[c] = (int)r;
+}
+
+int build_chunk_table(gpr_graph *g, int dmax, int chunk, cudaStream_t st) {
+  if (g->b_nlong >= 0 && g->b_dmax == dmax && g->b_chunk == chunk) return GPR_OK;
+  gpr::dfree(g->b_cbeg);
+  gpr::dfree(g->b_crow);
+  g->b_cbeg = g->b_crow = nullptr;
+  g->b_nlong = -1;
+  const gpr::PrLayout &L = g->L;
+  int *cnt = nullptr;
+  GPR_TRY(gpr::dalloc(&cnt, 1, "chunk count"));
+  cudaMemsetAsync(cnt, 0, sizeof(int), st);
+  if (L.n_nz > 0)
+    k_b_count<<<(unsigned)gpr::ceil_div(L.n_nz, 256), 256, 0, st>>>(L.n_nz, L.csr_ptr, dmax, cnt);
+  int nlong = 0;
+  cudaError_t e = cudaMemcpyAsync(&nlong, cnt, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(cnt);
+  if (e != cudaSuccess) {
+    gpr::set_error("gpr_ppr chunk table: %s", cudaGetErrorString(e));
+    return GPR_ECUDA;
+  }
+  GPR_TRY(gpr::dalloc(&g->b_cbeg, (size_t)nlong + 1, "batched chunk offsets"));
+  k_b_lens<<<(unsigned)gpr::ceil_div((long long)nlong + 1, 256), 256, 0, st>>>(nlong, L.csr_ptr,
+                                                                              chunk, g->b_cbeg);
+  size_t tb = 0;
+  GPR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, g->b_cbeg, g->b_cbeg, nlong + 1, st));
+  void *tmp = nullptr;
+  GPR_TRY(gpr::dmalloc(&tmp, tb, "scan scratch"));
+  e = cub::DeviceScan::ExclusiveSum(tmp, tb, g->b_cbeg, g->b_cbeg, nlong + 1, st);
+  int nch = 0;
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&nch, g->b_cbeg + nlong, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  cudaFree(tmp);
+  if (e != cudaSuccess) {
+    gpr::set_error("gpr_ppr chunk table: %s", cudaGetErrorString(e));
+    return GPR_ECUDA;
+  }
+  GPR_TRY(gpr::dalloc(&g->b_crow, (size_t)nch, "batched chunk rows"));
+  if (nlong > 0) {
+    unsigned gr = (unsigned)gpr::ceil_div(32LL * nlong, 256);
+    if (gr > 148u * 32u) gr = 148u * 32u;
+    k_b_fill<<<gr, 256, 0, st>>>(nlong, g->b_cbeg, g->b_crow);
+  }
+  GPR_CUDA(cudaGetLastError());
+  GPR_CUDA(cudaStreamSynchronize(st));
+  g->b_nlong = nlong;
+  g->b_nchunks = nch;
+  g->b_dmax = dmax;
+  g->b_chunk = chunk;
+  return GPR_OK;
+}
+
+struct PprKernels {
+  const void *solve;
+  void (*init)(PprArgs);
+  void (*scatter)(int, int, const int *, const float *, float *);
+  void (*refine_init)(PprArgs, const double *);
+};
+
+template <int K, typename T>
+PprKernels kernels_for() {
+  return {(const void *)k_ppr<K, T>, k_ppr_init<K, T>, k_ppr_scatter<K>, k_ppr_refine_init<K>};
+}
+
+int pick_k(int k) {
+  for (int K : {8, 16, 32, 64, 128})
+    if (k <= K) return K;
+  return -1;
+}
+
+PprKernels select(int K, bool bf16) {
+  switch (K) {
+    case 8: return bf16 ? kernels_for<8, __nv_bfloat16>() : kernels_for<8, float>();
+    case 16: return bf16 ? kernels_for<16, __nv_bfloat16>() : kernels_for<16, float>();
+    case 32: return bf16 ? kernels_for<32, __nv_bfloat16>() : kernels_for<32, float>();
+    case 64: return bf16 ? kernels_for<64, __nv_bfloat16>() : kernels_for<64, float>();
+    default: return bf16 ? kernels_for<128, __nv_bfloat16>() : kernels_for<128, float>();
+  }
+}
+
+struct Bufs {
+  void *p[32] = {nullptr};
+  int n = 0;
+  template <typename X>
+  int get(X **out, size_t count, const char *what) {
+    if (n >= 32) {
+      gpr::set_error("gpr_ppr: too many scratch buffers");
+      return GPR_ENOMEM;
+    }
+    int rc = gpr::dalloc(out, count, what);
+    if (rc == GPR_OK) p[n++] = *out;
+    return rc;
+  }
+  ~Bufs() {
+    for (int i = 0; i < n; ++i) gpr::dfree(p[i]);
+  }
+};
+
+}  // namespace
+
+extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
+                       const gpr_pr_opts *opts_in, int *h_iters, gpr_pr_stats *stats) {
+  gpr_pr_opts o;
+  if (opts_in) o = *opts_in;
+  else gpr_pr_opts_default(&o);
+  if (!g || k < 1 || !h_seeds || !any_x) {
+    gpr::set_error("gpr_ppr: invalid arguments");
+    return GPR_EINVAL;
+  }
+  const int K = pick_k(k);
+  if (K < 0) {
+    gpr::set_error("gpr_ppr: k=%d vectors exceeds 128 per call", k);
+    return GPR_EINVAL;
+  }
+  const gpr::PrLayout &L = g->L;
+  const int m = L.m;
+  if (!L.csr_ptr) {
+    gpr::set_error("gpr_ppr: the graph was created without GPR_LAYOUT_BATCHED");
+    return GPR_EINVAL;
+  }
+  if (o.precision != GPR_PREC_FP32 && o.precision != GPR_PREC_BF16) {
+    gpr::set_error("gpr_ppr: precision %d not supported (FP32 or BF16)", o.precision);
+    return GPR_EUNSUPPORTED;
+  }
+  if (o.max_iter < 0 || !(o.tol >= 0.0) || !(o.timeout_s > 0.0)) {
+    gpr::set_error("gpr_ppr: invalid options");
+    return GPR_EINVAL;
+  }
+  for (int q = 0; q < k; ++q)
+    if (h_seeds[q] < 0 || h_seeds[q] >= m) {
+      gpr::set_error("gpr_ppr: seed %d of vector %d out of range", h_seeds[q], q);
+      return GPR_EINVAL;
+    }
+  // BF16 form: BF16 contributions down to tol_lo, above the BF16 rounding
+  // floor, then FP32 refinement sweeps from that iterate down to tol.
+  const bool bf16 = o.precision == GPR_PREC_BF16;
+  const double tol_lo = std::max(o.tol, 1e-3);
+  const PprKernels k32 = select(K, false), k16 = select(K, true);
+  cudaStream_t st = g->st;
+  int sms = 0;
+  GPR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+  const size_t smem = sizeof(double) * 2 * (kPprBlock / 32) * K;
+  const int Lb = K <= 32 ? 8 : K / 4;
+  const int R = 32 / Lb;
+  // Rows above 8 rounds of one sub-group are cut into 1024-edge chunks that
+  // the whole warp works on, so no unit runs far longer than another.
+  const int b_dmax = 8 * Lb, b_chunk = 1024;
+  GPR_TRY(build_chunk_table(g, b_dmax, b_chunk, st));
+  const int n_row_units = (int)gpr::ceil_div((long long)L.n_nz - g->b_nlong, R);
+  const long long units = (long long)g->b_nchunks + n_row_units;
+  auto grid_of = [&](const PprKernels &kk, int *grid) -> int {
+    int per_sm = 0;
+    GPR_CUDA(cudaFuncSetAttribute(kk.solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kk.solve, kPprBlock, smem));
+    if (per_sm < 1) {
+      gpr::set_error("gpr_ppr: kernel cannot be resident");
+      return GPR_ECUDA;
+    }
+    *grid = (int)std::max<long long>(1, std::min<long long>((long long)sms * per_sm,
+                                                          gpr::ceil_div(units, kPprBlock / 32)));
+    return GPR_OK;
+  };
+  int G32 = 0, G16 = 0;
+  GPR_TRY(grid_of(k32, &G32));
+  if (bf16) GPR_TRY(grid_of(k16, &G16));
+  const int Gmax = std::max(G32, G16);
+  Bufs B;
+  float *x = nullptr, *partial = nullptr, *xout = nullptr;
+  void *c0 = nullptr, *c1 = nullptr, *h0 = nullptr, *h1 = nullptr;
+  int *cnt = nullptr, *seed = nullptr, *seeds_old = nullptr, *iters = nullptr, *status = nullptr,
+      *wq = nullptr;
+  double *cta_red = nullptr, *seed_red = nullptr, *res_hist = nullptr, *dang = nullptr;
+  unsigned *active = nullptr, *bar = nullptr;
+  const int max_iter = o.max_iter;
+  GPR_TRY(B.get(&x, (size_t)m * K, "ppr x"));
+  GPR_TRY(B.get((float **)&c0, ((size_t)m + 1) * K, "ppr contrib0"));
+  GPR_TRY(B.get((float **)&c1, ((size_t)m + 1) * K, "ppr contrib1"));
+  if (bf16) {
+    GPR_TRY(B.get((__nv_bfloat16 **)&h0, ((size_t)m + 1) * K, "ppr bf16 contrib0"));
+    GPR_TRY(B.get((__nv_bfloat16 **)&h1, ((size_t)m + 1) * K, "ppr bf16 contrib1"));
+    GPR_CUDA(cudaMemsetAsync(h0, 0, ((size_t)m + 1) * K * 2, st));
+    GPR_CUDA(cudaMemsetAsync(h1, 0, ((size_t)m + 1) * K * 2, st));
+  }
+  GPR_TRY(B.get(&partial, (size_t)std::max(1, g->b_nchunks) * K, "ppr partials"));
+  GPR_TRY(B.get(&cnt, (size_t)std::max(1, g->b_nlong), "ppr counters"));
+  GPR_TRY(B.get(&seed, (size_t)K, "ppr seeds"));
+  GPR_TRY(B.get(&seeds_old, (size_t)k, "ppr seeds (input)"));
+  GPR_TRY(B.get(&iters, (size_t)K, "ppr iterations"));
+  GPR_TRY(B.get(&status, 4, "ppr status"));
+  GPR_TRY(B.get(&wq, 2, "ppr queue"));
+  GPR_TRY(B.get(&cta_red, (size_t)2 * Gmax * K, "ppr cta sums"));
+  GPR_TRY(B.get(&seed_red, (size_t)2 * K, "ppr seed sums"));
+  GPR_TRY(B.get(&res_hist, (size_t)std::max(1, max_iter) * K, "ppr residuals"));
+  GPR_TRY(B.get(&dang, (size_t)2 * K, "ppr dangling"));
+  GPR_TRY(B.get(&active, 8, "ppr masks"));
+  GPR_TRY(B.get(&bar, 2, "ppr barrier"));
+  GPR_CUDA(cudaMemsetAsync(x, 0, sizeof(float) * (size_t)m * K, st));
+  GPR_CUDA(cudaMemsetAsync(c0, 0, ((size_t)m + 1) * K * 4, st));
+  GPR_CUDA(cudaMemsetAsync(c1, 0, ((size_t)m + 1) * K * 4, st));
+  GPR_CUDA(cudaMemsetAsync(cnt, 0, sizeof(int) * std::max(1, g->b_nlong), st));
+  GPR_CUDA(cudaMemsetAsync(bar, 0, sizeof(unsigned) * 2, st));
+  GPR_CUDA(cudaMemsetAsync(seed, 0xff, sizeof(int) * K, st));
+  GPR_CUDA(cudaMemsetAsync(seed_red, 0, sizeof(double) * 2 * K, st));
+  GPR_CUDA(cudaMemcpyAsync(seeds_old, h_seeds, sizeof(int) * k, cudaMemcpyHostToDevice, st));
+  k_invert_for_seeds<<<(unsigned)gpr::ceil_div(m, 256), 256, 0, st>>>(m, L.perm, k, seeds_old,
+                                                                       seed);
+  PprArgs a;
+  a.m = m;
+  a.n_long = g->b_nlong;
+  a.n_nz = L.n_nz;
+  a.n_chunks = g->b_nchunks;
+  a.chunk = b_chunk;
+  a.k = k;
+  a.n_row_units = n_row_units;
+  a.csr_ptr = L.csr_ptr;
+  a.csr_col = L.csr_col;
+  a.row_cbeg = g->b_cbeg;
+  a.chunk_row = g->b_crow;
+  a.outdeg = L.outdeg;
+  a.x = x;
+  a.partial = partial;
+  a.cnt = cnt;
+  a.seed = seed;
+  a.cta_red = cta_red;
+  a.seed_red = seed_red;
+  a.res_hist = res_hist;
+  a.dang = dang;
+  a.active = active;
+  a.iters = iters;
+  a.bar = bar;
+  a.status = status;
+  a.wq = wq;
+  a.damp = o.damping;
+  a.max_iter = max_iter;
+  a.timeout_ns = (long long)(o.timeout_s * 1e9);
+  int launches = 0;
+  // One phase: sweeps until every vector's change is below `tol`.
+  auto phase = [&](const PprKernels &kk, int G, double tol, int *sweeps,
+                   std::vector<int> *it_out) -> int {
+    a.tol = tol;
+    a.batch = (int)std::max<long long>(1, units / ((long long)G * (kPprBlock / 32) * 4));
+    a.bar_expect = G + (o.reserved[0] > 0 ? o.reserved[0] : 0);
+    GPR_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 4, st));
+    GPR_CUDA(cudaMemsetAsync(wq, 0, sizeof(int) * 2, st));
+    if (max_iter > 0) {
+      void *args[] = {&a};
+      GPR_CUDA(cudaLaunchCooperativeKernel(kk.solve, dim3(G), dim3(kPprBlock), args, smem, st));
+      ++launches;
+    }
+    int hs[4];
+    GPR_CUDA(cudaMemcpyAsync(hs, status, sizeof(hs), cudaMemcpyDeviceToHost, st));
+    it_out->assign(K, 0);
+    GPR_CUDA(cudaMemcpyAsync(it_out->data(), iters, sizeof(int) * K, cudaMemcpyDeviceToHost, st));
+    GPR_CUDA(cudaStreamSynchronize(st));
+    *sweeps = hs[1];
+    if (hs[0] & 1) {
+      gpr::set_error("gpr_ppr: grid barrier wait exceeded %.3f s", o.timeout_s);
+      return GPR_ETIMEOUT;
+    }
+    return GPR_OK;
+  };
+  GPR_CUDA(cudaEventRecord(g->e0, st));
+  int s1 = 0, s2 = 0;
+  std::vector<int> it1(K, 0), it2(K, 0);
+  if (bf16) {
+    a.c0 = h0;
+    a.c1 = h1;
+    k16.init<<<1, 128, 0, st>>>(a);
+    ++launches;
+    GPR_CUDA(cudaEventRecord(g->e2, st));
+    GPR_TRY(phase(k16, G16, tol_lo, &s1, &it1));
+    a.c0 = c0;
+    a.c1 = c1;
+    k32.refine_init<<<(unsigned)gpr::ceil_div((long long)m * K, 256), 256, 0, st>>>(
+        a, dang + (s1 & 1) * K);
+    ++launches;
+  } else {
+    a.c0 = c0;
+    a.c1 = c1;
+    k32.init<<<1, 128, 0, st>>>(a);
+    ++launches;
+    GPR_CUDA(cudaEventRecord(g->e2, st));
+  }
+  GPR_TRY(phase(k32, G32, o.tol, &s2, &it2));
+  GPR_CUDA(cudaEventRecord(g->e3, st));
+  const bool host_out = !gpr::is_device_ptr(any_x);
+  float *dout = any_x;
+  if (host_out) {
+    GPR_TRY(B.get(&xout, (size_t)m * k, "ppr output staging"));
+    dout = xout;
+  }
+  k32.scatter<<<(unsigned)gpr::ceil_div((long long)m * k, 256), 256, 0, st>>>(m, k, L.perm, x,
+                                                                              dout);
+  ++launches;
+  GPR_CUDA(cudaGetLastError());
+  GPR_CUDA(cudaEventRecord(g->e1, st));
+  GPR_CUDA(cudaStreamSynchronize(st));
+  if (host_out)
+    GPR_CUDA(cudaMemcpy(any_x, xout, sizeof(float) * (size_t)m * k, cudaMemcpyDeviceToHost));
+  float ms = 0.f, lms = 0.f;
+  GPR_CUDA(cudaEventElapsedTime(&ms, g->e0, g->e1));
+  GPR_CUDA(cudaEventElapsedTime(&lms, g->e2, g->e3));
+  if (h_iters)
+    for (int q = 0; q < k; ++q) h_iters[q] = it1[q] + it2[q];
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    stats->iterations = s1 + s2;
+    stats->refine_iterations = bf16 ? s2 : 0;
+    stats->solve_ms = ms;
+    stats->loop_ms = lms;
+    stats->gpu_launches = launches;
+    if (s2 > 0) {
+      std::vector<double> last(K);
+      GPR_CUDA(cudaMemcpy(last.data(), res_hist + (size_t)(s2 - 1) * K, sizeof(double) * K,
+                          cudaMemcpyDeviceToHost));
+      double mx = 0;
+      for (int q = 0; q < k; ++q) mx = std::max(mx, last[q]);
+      stats->residual = mx;
+    }
+  }
+  return GPR_OK;
+}

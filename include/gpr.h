@@ -92,6 +92,7 @@ int gpr_graph_create(int m, long long nnz, const int *any_rowptr,
                      const int *any_col, const int *any_outdeg,
                      gpr_graph **out);
 /* Layout knobs (the autotuner's search space); zero fields take defaults. */
+enum { GPR_LAYOUT_BATCHED = 1 /* also keep a relabelled CSR: needed by gpr_ppr */ };
 typedef struct {
   int sell_max;   /* max edges per lane in a SELL slice: rows of in-degree <= sell_max get
                      one lane, wider rows 2..32 lanes (default 64) */
@@ -99,7 +100,8 @@ typedef struct {
   int chunk_min;  /* rows with more in-edges than this are cut into chunks (default 4096) */
   int hot_entries;/* contributions of the highest in-degree vertices kept in shared memory
                      by the persistent kernel, multiple of 4, <= 56832 (default 32768) */
-  int reserved[4];
+  int flags;      /* GPR_LAYOUT_* bits */
+  int reserved[3];
 } gpr_layout_opts;
 int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr,
                         const int *any_col, const int *any_outdeg,
@@ -141,6 +143,18 @@ int gpr_pr_solver(int m, int nnz, const int *in_row_offsets,
 int gpr_page_rank(int m, int nnz, const int *row_offsets,
                   const int *column_indices, const int *degree, float *scores,
                   const gpr_pr_opts *opts, gpr_pr_stats *stats);
+
+/* ---- Batched personalized PageRank (no counterpart in the reference) ------
+ * k <= 128 seed vectors in one persistent launch: for vector q with seed
+ * h_seeds[q], x_q = d * M x_q + ((1-d) + d * dangling_q) e_{seed_q}, from
+ * x_q = e_{seed_q}; vector q stops after the first sweep whose FP64 L1 change
+ * is below opts->tol.  opts->precision: GPR_PREC_FP32 or GPR_PREC_BF16
+ * (contributions stored in BF16, FP32 accumulation).  any_x receives x as an
+ * m x k row-major array (vertex-major, host or device); h_iters (k ints, may
+ * be NULL) the sweeps of each vector.  The graph must be created with
+ * GPR_LAYOUT_BATCHED. */
+int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
+            const gpr_pr_opts *opts, int *h_iters, gpr_pr_stats *stats);
 
 /* ---- PageRank without any allocation ----------------------------------------
  * No counterpart in the reference.  For callers that cannot let a library

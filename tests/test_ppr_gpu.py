@@ -1,0 +1,67 @@
+"""Batched personalized PageRank on the GPU against the FP64 oracle.
+
+The reference has no personalized PageRank; oracle/oracle.c orc_ppr_f64
+defines the semantics (teleport mass and dangling mass returned to the
+seed, per-vector stop at L1 change < tol).  Bars: FP32 form, every vector's
+L1 error vs the FP64 oracle <= 1e-5 and its sweep count within one.  BF16
+form: BF16 contributions until the change drops below 1e-3, then FP32
+refinement sweeps to the same tolerance -- the same L1 bar, 1e-5.
+"""
+import numpy as np
+import pytest
+
+from graphs import star
+
+pytestmark = pytest.mark.gpu
+
+
+def l1_per_vector(x, ref):
+    return np.abs(x.astype(np.float64) - ref).sum(axis=0)
+
+
+@pytest.mark.parametrize("k", [1, 5, 8, 16, 32, 40, 64, 128])
+def test_ppr_fp32_matches_fp64_oracle(G, O, k):
+    rp, col, od = O.rmat_graph(12, 8, seed=31)
+    m = len(rp) - 1
+    seeds = O.uniform_int(k, 77, m)
+    ref, ref_it = O.ppr_f64(rp, col, od, seeds, tol=1e-6, max_iter=100)
+    with G.Graph(rp, col, od, batched=True) as g:
+        x, it, st = g.ppr(seeds, tol=1e-6, max_iter=100)
+    assert np.all(l1_per_vector(x, ref) <= 1e-5)
+    assert np.all(np.abs(it - ref_it) <= 1)
+    np.testing.assert_allclose(x.sum(axis=0), ref.sum(axis=0), atol=1e-5)
+
+
+def test_ppr_bf16_form(G, O):
+    rp, col, od = O.rmat_graph(12, 8, seed=32)
+    m = len(rp) - 1
+    seeds = O.uniform_int(32, 78, m)
+    ref, ref_it = O.ppr_f64(rp, col, od, seeds, tol=1e-6, max_iter=100)
+    with G.Graph(rp, col, od, batched=True) as g:
+        x, it, st = g.ppr(seeds, tol=1e-6, max_iter=100, precision=G.PREC_BF16)
+    assert st.refine_iterations > 0
+    assert np.all(l1_per_vector(x, ref) <= 1e-5)
+    assert np.all(it <= ref_it + 30)
+
+
+def test_ppr_seed_without_in_edges_and_chunked_hub(G, O):
+    rp, col, od = star(60000)
+    m = len(rp) - 1
+    indeg = np.diff(rp)
+    zero_in = int(np.flatnonzero(indeg == 0)[0])
+    seeds = np.array([0, 1, zero_in, zero_in, 12345], dtype=np.int32)
+    ref, ref_it = O.ppr_f64(rp, col, od, seeds, tol=1e-6, max_iter=100)
+    with G.Graph(rp, col, od, batched=True, chunk=512, chunk_min=1024) as g:
+        lay = g.layout()
+        x, it, st = g.ppr(seeds, tol=1e-6, max_iter=100)
+    assert lay["n_chunks"] > lay["n_long"] > 0
+    assert np.all(l1_per_vector(x, ref) <= 1e-5)
+    assert np.all(np.abs(it - ref_it) <= 1)
+
+
+def test_ppr_requires_batched_layout(G, O):
+    rp, col, od = O.rmat_graph(8, 4, seed=1)
+    with G.Graph(rp, col, od) as g:
+        with pytest.raises(G.GprError) as e:
+            g.ppr(np.array([0], np.int32))
+    assert e.value.status == G.GPR_EINVAL
