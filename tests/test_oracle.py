@@ -1,0 +1,134 @@
+"""CPU: the oracle and the host-side loader, pinned to the reference itself.
+
+The fixtures under tests/golden/ were produced by the reference's own code
+(tests/golden/make_golden.py runs oracle/_ref, compiled from the reference
+tree).  These tests hold everything a GPU result is compared against to
+those fixtures bit for bit, and, where the reference tree is present, also
+to the live reference on fresh seeded inputs.
+"""
+import itertools
+import os
+
+import numpy as np
+import pytest
+
+from conftest import ROOT
+
+GOLD = os.path.join(ROOT, "tests", "golden")
+REF_DATA = "/root/reference/datasets"
+
+
+@pytest.fixture(scope="module")
+def pr_gold():
+    return np.load(os.path.join(GOLD, "pr.npz"))
+
+
+@pytest.fixture(scope="module")
+def spmv_gold():
+    return np.load(os.path.join(GOLD, "spmv.npz"))
+
+
+@pytest.fixture(scope="module")
+def loader_gold():
+    return np.load(os.path.join(GOLD, "loader.npz"))
+
+
+def graphs(d):
+    return sorted({k.split(":")[0] for k in d.files})
+
+
+def test_pr_restatement_bit_identical_to_reference(O, pr_gold):
+    names = graphs(pr_gold)
+    assert {"test_pr.mtx", "chesapeake.mtx", "4.mtx", "4.graph", "rmat10"} <= set(names)
+    for g in names:
+        rp, col, od = (pr_gold[f"{g}:{k}"] for k in ("in_rowptr", "in_col", "outdeg"))
+        for tol, mi in ((1e-3, 30), (1e-4, 100)):
+            s, sweeps, hist = O.pr_plain_f32(rp, col, od, tol=tol, max_iter=mi)
+            gold = pr_gold[f"{g}:{tol:g}:{mi}:scores"]
+            printed = int(pr_gold[f"{g}:{tol:g}:{mi}:printed_iterations"][0])
+            assert np.array_equal(s, gold), g
+            # omp_base.cc:46 prints iter+1: the sweep count when it converged,
+            # max_iter+1 when it ran out of sweeps.
+            converged = hist[-1] < tol
+            assert printed == (sweeps if converged else sweeps + 1), g
+
+
+def test_spmv_restatement_bit_identical_to_reference(O, spmv_gold):
+    for g in graphs(spmv_gold):
+        a = {k: spmv_gold[f"{g}:{k}"] for k in ("Ap", "Aj", "Ax", "x", "y0", "y")}
+        y = O.spmv_f32(a["Ap"], a["Aj"], a["Ax"], a["x"], a["y0"])
+        assert np.array_equal(y, a["y"]), g
+        assert O.max_rel_err(y, a["y"]) == 0.0
+
+
+def test_rmat_generator_is_pinned(O, pr_gold):
+    rp, col, od = O.rmat_graph(10, 16, seed=1)
+    assert np.array_equal(rp, pr_gold["rmat10:in_rowptr"])
+    assert np.array_equal(col, pr_gold["rmat10:in_col"])
+    assert np.array_equal(od, pr_gold["rmat10:outdeg"])
+
+
+def test_reference_verifier_on_reference_scores(O, pr_gold, loader_gold):
+    # PRVerifier's push check (src/pr/verifier.cc:50-68) on the reference's
+    # own results for its datasets: the number it compares with EPSILON.
+    # 4.mtx holds non-adjacent duplicate edges; the PR driver reads it
+    # unsorted (src/pr/main.cc:23-24), so the out-CSR and the in-CSR keep
+    # different duplicates and the reference fails its own check there.
+    for ds, ok in (("test_pr.mtx", True), ("chesapeake.mtx", True), ("4.mtx", False),
+                   ("4.graph", True)):
+        orp, ocol = loader_gold[f"ref:{ds}:out_rowptr"], loader_gold[f"ref:{ds}:out_col"]
+        od = pr_gold[f"{ds}:outdeg"]
+        s = pr_gold[f"{ds}:0.001:30:scores"]
+        assert (O.push_check(orp, ocol, od, s) < 1e-3) == ok, ds
+
+
+def test_fp64_oracle_is_a_fixed_point(O, pr_gold):
+    rp, col, od = (pr_gold[f"rmat10:{k}"] for k in ("in_rowptr", "in_col", "outdeg"))
+    s64, n, err = O.pr_f64(rp, col, od)
+    assert err < 1e-14
+    # the FP32 result at tol 1e-4 lies within the a-posteriori bound of the fixed point
+    s32 = pr_gold["rmat10:0.0001:100:scores"]
+    r = O.pr_residual_f64(rp, col, od, s32)
+    mx, l1 = O.err_vs_f64(s32, s64)
+    assert l1 <= r / (1 - 0.85) * 1.0001 + 1e-12
+
+
+@pytest.mark.parametrize("name", ["graph_small", "graph_dups", "graph_simple"])
+@pytest.mark.parametrize("ext", [".mtx", ".gr", ".graph"])
+def test_read_graph_matches_reference_loader(G, loader_gold, name, ext):
+    path = os.path.join(GOLD, name + ext)
+    for fl in itertools.product([False, True], repeat=5):
+        key = name + ext + ":" + "".join(str(int(x)) for x in fl)
+        m, nnz, rp, col, deg, wt = G.read_graph(path, *fl)
+        assert np.array_equal(rp, loader_gold[key + ":rowptr"]), key
+        assert np.array_equal(col, loader_gold[key + ":col"]), key
+        assert np.array_equal(wt, loader_gold[key + ":weight"]), key
+        assert np.array_equal(deg, np.diff(rp)), key
+
+
+@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="reference datasets not present")
+@pytest.mark.parametrize("ds", ["test_pr.mtx", "chesapeake.mtx", "4.mtx", "4.graph"])
+def test_read_graph_on_reference_datasets(G, loader_gold, ds):
+    path = os.path.join(REF_DATA, ds)
+    _, _, orp, ocol, _, _ = G.read_graph(path, False, False, False)
+    _, _, irp, icol, _, _ = G.read_graph(path, False, True, False)
+    assert np.array_equal(orp, loader_gold[f"ref:{ds}:out_rowptr"])
+    assert np.array_equal(ocol, loader_gold[f"ref:{ds}:out_col"])
+    assert np.array_equal(irp, loader_gold[f"ref:{ds}:in_rowptr"])
+    assert np.array_equal(icol, loader_gold[f"ref:{ds}:in_col"])
+
+
+def test_live_reference_on_fresh_graphs(O):
+    if not O.ref_available():
+        pytest.skip("oracle/_ref not built (reference tree absent)")
+    from graphs import erdos_renyi
+    for seed in range(3):
+        rp, col, od = erdos_renyi(3000, 7, seed=seed)
+        a, na, _ = O.pr_plain_f32(rp, col, od, tol=1e-5, max_iter=60)
+        b, nb, _ = O.ref_pr_solver(rp, col, od, tol=1e-5, max_iter=60)
+        assert np.array_equal(a, b) and (nb == na or nb == na + 1)
+        x = O.uniform_f32(3000, seed + 10)
+        vals = O.uniform_f32(len(col), seed + 20)
+        y0 = np.zeros(3000, np.float32)
+        assert np.array_equal(O.spmv_f32(rp, col, vals, x, y0),
+                              O.ref_spmv_solver(rp, col, vals, x, y0)[0])
