@@ -219,7 +219,7 @@ def run_ours(args):
     t0 = time.time()
     csr = G.gen_rmat(args.scale, EDGE_FACTOR, seed=SEED, abc=ABC)
     m, nnz = csr.m, csr.nnz
-    g = G.Graph(csr.rowptr, csr.col, csr.third, m=m, nnz=nnz)
+    g = G.Graph(csr.rowptr, csr.col, csr.third, m=m, nnz=nnz, batched=not args.no_forms)
     g.set_stream(stream.cuda_stream)
     log(f"[ours] rank {rank}: graph s{args.scale} m={m} nnz={nnz} layout={g.layout()} "
         f"ready in {time.time() - t0:.2f}s")
@@ -323,6 +323,11 @@ def run_ours(args):
                        "call": "PageRank(m, nnz, row_offsets, column_indices, degree, scores) "
                                "via gpr_page_rank, pinned host buffers"}
 
+    if not args.no_forms:
+        line["forms"] = forms_leg(G, torch, dev, g, m, nnz, gteps / world, args)
+    line["forms"]["pr_bf16_refined"]["time_to_solution_vs_plain"] = (
+        (ms / args.steps) / line["forms"]["pr_bf16_refined"]["loop_ms"])
+
     if not args.no_spmv:
         line["spmv"] = spmv_leg(G, torch, dev, stream, args)
 
@@ -345,6 +350,49 @@ def run_ours(args):
     if rank == 0:
         print(json.dumps(line), flush=True)
     return 0
+
+
+def forms_leg(G, torch, dev, g, m, nnz, plain_gteps, args):
+    """The forms the metric compares with the plain FP32 path, on the same
+    graph: batched personalized PageRank (k seed vectors, one persistent
+    launch) in FP32 and in BF16 with FP32 refinement.  Rates are edge-vector
+    pairs per second over every vector of every sweep (nnz * k * sweeps /
+    time of the sweep loop); `useful` counts only sweeps in which a vector was
+    still updating."""
+    out = {"plain_fp32_gteps": plain_gteps}
+    # single-vector mixed form: BF16 contributions, then FP32 refinement
+    scores = torch.empty(m, dtype=torch.float32, device=dev)
+    best = None
+    for _ in range(3):
+        scores.fill_(float(np.float32(1.0) / np.float32(m)))
+        _, st = g.pagerank(scores, G.options(tol=TOL, max_iter=MAX_ITER, damping=DAMPING,
+                                             precision=G.PREC_BF16))
+        if best is None or st.loop_ms < best.loop_ms:
+            best = st
+    resid = g.residual_f64(scores, DAMPING)
+    out["pr_bf16_refined"] = {
+        "sweeps": best.iterations, "refine_sweeps": best.refine_iterations,
+        "loop_ms": best.loop_ms, "gteps": nnz * best.iterations / (best.loop_ms / 1e3) / 1e9,
+        "time_to_solution_vs_plain": None, "l1_error_bound_vs_fixed_point": resid / (1 - 0.85)}
+    rng = np.random.default_rng(5)
+    for k, prec, name in ((8, G.PREC_FP32, "ppr_k8_fp32"), (32, G.PREC_FP32, "ppr_k32_fp32"),
+                          (32, G.PREC_BF16, "ppr_k32_bf16_refined")):
+        seeds = rng.integers(0, m, k).astype(np.int32)
+        buf = torch.empty(m * k, dtype=torch.float32, device=dev)
+        best = None
+        for _ in range(2):
+            _, it, st = g.ppr(seeds, out=buf, tol=TOL, max_iter=MAX_ITER, precision=prec)
+            if best is None or st.loop_ms < best[0].loop_ms:
+                best = (st, it)
+        st, it = best
+        rate = nnz * k * st.iterations / (st.loop_ms / 1e3) / 1e9
+        out[name] = {"k": k,  # noqa: E501 "precision": "bf16+fp32 refinement" if prec == G.PREC_BF16 else "fp32",
+                     "sweeps": st.iterations, "refine_sweeps": st.refine_iterations,
+                     "loop_ms": st.loop_ms, "edge_vector_gteps": rate,
+                     "useful_edge_vector_gteps": nnz * float(it.sum()) / (st.loop_ms / 1e3) / 1e9,
+                     "vs_plain_fp32": rate / plain_gteps, "max_final_residual": st.residual}
+        del buf
+    return out
 
 
 def spmv_leg(G, torch, dev, stream, args):
@@ -402,6 +450,7 @@ def main():
     ap.add_argument("--scale", type=int, default=SCALE)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-spmv", action="store_true")
+    ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-solve", type=int, default=0, metavar="SWEEPS",
                     help="build the graph and run one solve of exactly SWEEPS sweeps, "

@@ -162,8 +162,10 @@ struct gpr_graph {
   double *res_tmp = nullptr;   // [m+1+n_long] FP64 residual scratch
   int err_cap = 0;
   int last_sweeps = 0;
-  int hot = 0;                 // contributions staged in shared memory per sweep
-  int grid_hot[8] = {0};  // cooperative grid of each persistent variant
+  int hot = 0;                 // FP32 contributions staged in shared memory per sweep
+  int hot_bytes = 0;           // shared-memory budget of the hot prefix
+  int grid_hot[12] = {0};      // cooperative grid of each persistent sweep kernel
+  void *h0 = nullptr, *h1 = nullptr;  // BF16 contributions of the mixed form (on first use)
   int *wq = nullptr;           // [2] work-queue heads of the hot kernel
   bool hot_ok = false;         // every hot-kernel variant is co-resident at grid_hot
   int grid_step = 0, max_grid = 0;

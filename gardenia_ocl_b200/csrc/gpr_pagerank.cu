@@ -27,6 +27,8 @@
 #include <type_traits>
 #include <vector>
 
+#include <cuda_bf16.h>
+
 #include "gpr_internal.cuh"
 
 using gpr::PrLayout;
@@ -45,7 +47,9 @@ struct PrArgs {
   const long long *slice_ptr;
   const int *sell_col;
   const int *outdeg;
-  float *s, *c0, *c1, *partial;
+  float *s;
+  void *c0, *c1;   // contributions by sweep parity: float or __nv_bfloat16
+  float *partial;
   int *cnt;
   double *cta_err, *err_hist;
   unsigned *bar;
@@ -106,17 +110,60 @@ __device__ __forceinline__ float4 ld_contrib4(const float4 *p, uint64_t pol) {
   return v;
 }
 
+// Contribution elements are FP32 (plain form) or BF16 (mixed form); the sum
+// is always FP32.
+__device__ __forceinline__ float ld_c(const float *p, uint64_t pol) { return ld_contrib(p, pol); }
+__device__ __forceinline__ float ld_c(const __nv_bfloat16 *p, uint64_t pol) {
+  unsigned short h;
+  asm volatile("ld.global.L2::cache_hint.b16 %0, [%1], %2;" : "=h"(h) : "l"(p), "l"(pol));
+  return __uint_as_float((unsigned)h << 16);
+}
+__device__ __forceinline__ float ld_c_generic(const float *p) {
+  float v;
+  asm volatile("ld.f32 %0, [%1];" : "=f"(v) : "l"(p));
+  return v;
+}
+__device__ __forceinline__ float ld_c_generic(const __nv_bfloat16 *p) {
+  unsigned short h;
+  asm volatile("ld.b16 %0, [%1];" : "=h"(h) : "l"(p));
+  return __uint_as_float((unsigned)h << 16);
+}
+__device__ __forceinline__ float from_c(float v) { return v; }
+__device__ __forceinline__ float from_c(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ void st_c(float *p, float v, uint64_t pol) {
+  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" :: "l"(p), "f"(v), "l"(pol) : "memory");
+}
+__device__ __forceinline__ void st_c(__nv_bfloat16 *p, float v, uint64_t pol) {
+  const unsigned short h = __bfloat16_as_ushort(__float2bfloat16_rn(v));
+  asm volatile("st.global.L2::cache_hint.b16 [%0], %1, %2;" :: "l"(p), "h"(h), "l"(pol) : "memory");
+}
+
 // Contribution sources.  GlobalGather reads the contribution array;
 // HotGather serves indices below `hot` from the copy of the array's prefix
 // in shared memory (the highest in-degree vertices, which a power-law graph
 // gathers most) and the rest with a predicated global load, branch-free.
+template <typename T>
 struct GlobalGather {
-  const float *cin;
+  const T *cin;
   uint64_t pol;
-  __device__ __forceinline__ float operator()(int idx) const { return ld_contrib(cin + idx, pol); }
+  __device__ __forceinline__ float operator()(int idx) const { return ld_c(cin + idx, pol); }
 };
 
+template <typename T>
 struct HotGather {
+  const T *cin;
+  const T *hot;
+  int n_hot;
+  uint64_t pol;
+  __device__ __forceinline__ float operator()(int idx) const {
+    const float h = from_c(hot[min(idx, n_hot - 1)]);
+    const float g = idx >= n_hot ? ld_c(cin + idx, pol) : 0.f;
+    return idx < n_hot ? h : g;
+  }
+};
+
+template <>
+struct HotGather<float> {
   const float *cin;
   const float *hot;
   int n_hot;
@@ -135,16 +182,14 @@ struct HotGather {
 // Same sources through one generic-address load: a lane's pointer falls in
 // shared memory for hot indices and in global memory otherwise, so a gather
 // costs one load instruction instead of two.
+template <typename T>
 struct HotGatherGeneric {
-  const float *cin;
-  const float *hot;
+  const T *cin;
+  const T *hot;
   int n_hot;
   uint64_t pol;
   __device__ __forceinline__ float operator()(int idx) const {
-    const float *p = idx < n_hot ? hot + idx : cin + idx;
-    float v;
-    asm volatile("ld.f32 %0, [%1];" : "=f"(v) : "l"(p));
-    return v;
+    return ld_c_generic(idx < n_hot ? hot + idx : cin + idx);
   }
 };
 
@@ -191,18 +236,19 @@ __device__ __forceinline__ double warp_sum(double v) {
 
 // Score update of row r from its pulled sum and its prefetched old score and
 // out-degree; returns |s_new - s_old|.
+template <typename T>
 __device__ __forceinline__ double row_update(const PrArgs &a, int r, float sum, float so, int od,
-                                             float *cout, const Policies &pol) {
+                                             T *cout, const Policies &pol) {
   const float sn = __fadd_rn(a.base, __fmul_rn(a.damp, sum));
   st_f32(a.s + r, sn, pol.stream);
-  st_f32(cout + r, __fdiv_rn(sn, __int2float_rn(od)), pol.keep);
+  st_c(cout + r, __fdiv_rn(sn, __int2float_rn(od)), pol.keep);
   return (double)fabsf(__fsub_rn(sn, so));
 }
 
 // One chunk of a long row: U4 16-byte index loads per lane in flight, then
 // 4*U4 independent gathers.
-template <int U4, typename Gather>
-__device__ __forceinline__ double do_chunk(const PrArgs &a, const Gather &gat, float *cout, int c,
+template <int U4, typename Gather, typename T>
+__device__ __forceinline__ double do_chunk(const PrArgs &a, const Gather &gat, T *cout, int c,
                                            int lane, const Policies &pol) {
   const int r = a.chunk_row[c];
   const int cb = a.row_cbeg[r];
@@ -255,8 +301,8 @@ __device__ __forceinline__ double do_chunk(const PrArgs &a, const Gather &gat, f
 // One SELL slice: 32 >> lw rows, w = 1 << lw lanes per row.  Each lane runs
 // batches of U independent index loads followed by U independent gathers;
 // entries past the slice length read the sentinel slot (an exact +0).
-template <int U, typename Gather>
-__device__ __forceinline__ double do_slice(const PrArgs &a, const Gather &gat, float *cout,
+template <int U, typename Gather, typename T>
+__device__ __forceinline__ double do_slice(const PrArgs &a, const Gather &gat, T *cout,
                                            int sidx, int lane, const Policies &pol) {
   const int c = gpr::slice_class(a.cls, sidx);
   const int lw = a.cls.lw[c];
@@ -291,7 +337,8 @@ __device__ __forceinline__ double do_slice(const PrArgs &a, const Gather &gat, f
 // Rows without in-edges: s = base from the first sweep on, so they are
 // updated in sweep 0 and only their contribution is copied into the other
 // buffer in sweep 1; later sweeps skip them (their residual term is 0).
-__device__ __forceinline__ double do_zero(const PrArgs &a, float *cout, int z, int lane, int it,
+template <typename T>
+__device__ __forceinline__ double do_zero(const PrArgs &a, T *cout, int z, int lane, int it,
                                           const Policies &pol) {
   double err = 0.0;
   const int r0 = a.n_nz + z * gpr::kZeroRowsPerUnit;
@@ -304,21 +351,21 @@ __device__ __forceinline__ double do_zero(const PrArgs &a, float *cout, int z, i
         err += row_update(a, r, 0.f, ld_f32_stream(a.s + r, pol.stream), od, cout, pol);
       } else {
         const float sn = __fadd_rn(a.base, __fmul_rn(a.damp, 0.f));
-        st_f32(cout + r, __fdiv_rn(sn, __int2float_rn(od)), pol.keep);
+        st_c(cout + r, __fdiv_rn(sn, __int2float_rn(od)), pol.keep);
       }
     }
   }
   return err;
 }
 
-template <int U, int U4>
-__device__ __forceinline__ double sweep(const PrArgs &a, const float *cin, float *cout,
+template <int U, int U4, typename T>
+__device__ __forceinline__ double sweep(const PrArgs &a, const T *cin, T *cout,
                                         long long gw, long long nw, int lane, int it,
                                         const Policies &pol) {
   const long long u1 = a.n_chunks, u2 = u1 + a.n_slices;
   const long long u3 = u2 + (it < 2 ? a.n_zblk : 0);
   double err = 0.0;
-  const GlobalGather gat{cin, pol.keep};
+  const GlobalGather<T> gat{cin, pol.keep};
   for (long long u = gw; u < u3; u += nw) {
     if (u < u1) err += do_chunk<U4>(a, gat, cout, (int)u, lane, pol);
     else if (u < u2) err += do_slice<U>(a, gat, cout, (int)(u - u1), lane, pol);
@@ -401,10 +448,10 @@ __device__ bool barrier_reduce(const PrArgs &a, int it, double cta_total) {
 // Zero-in-degree rows are spread over all warps in the two sweeps that need
 // them.
 
-template <int U, int U4, bool GENERIC, int MINB>
+template <int U, int U4, bool GENERIC, int MINB, typename T>
 __global__ void __launch_bounds__(1024, MINB) k_pr_hot(PrArgs a) {
   extern __shared__ float4 s_hot4[];
-  float *s_hot = reinterpret_cast<float *>(s_hot4);
+  T *s_hot = reinterpret_cast<T *>(s_hot4);
   const int lane = threadIdx.x & 31;
   const int nwarps = blockDim.x >> 5;
   const long long gw = (long long)blockIdx.x * nwarps + (threadIdx.x >> 5);
@@ -413,12 +460,13 @@ __global__ void __launch_bounds__(1024, MINB) k_pr_hot(PrArgs a) {
   const int n_heavy = a.n_chunks + a.n_slices;
   int it = 0;
   while (it < a.max_iter) {
-    const float *cin = (it & 1) ? a.c1 : a.c0;
-    float *cout = (it & 1) ? a.c0 : a.c1;
+    const T *cin = static_cast<const T *>((it & 1) ? a.c1 : a.c0);
+    T *cout = static_cast<T *>((it & 1) ? a.c0 : a.c1);
     const float4 *src = reinterpret_cast<const float4 *>(cin);
-    for (int i = threadIdx.x; i < (a.hot >> 2); i += blockDim.x) s_hot4[i] = ld_contrib4(src + i, pol.keep);
+    const int n16 = (int)((size_t)a.hot * sizeof(T) / 16);
+    for (int i = threadIdx.x; i < n16; i += blockDim.x) s_hot4[i] = ld_contrib4(src + i, pol.keep);
     __syncthreads();
-    using Gat = typename std::conditional<GENERIC, HotGatherGeneric, HotGather>::type;
+    using Gat = typename std::conditional<GENERIC, HotGatherGeneric<T>, HotGather<T>>::type;
     const Gat gat{cin, s_hot, a.hot, pol.keep};
     double err = 0.0;
     for (;;) {
@@ -449,7 +497,7 @@ __global__ void __launch_bounds__(1024, MINB) k_pr_hot(PrArgs a) {
 // One sweep per launch (graph mode).  The sweep index and the done flag live
 // in device memory, so a captured sequence of launches needs no host input;
 // launches after convergence return at once.
-template <int U, int U4>
+template <int U, int U4, typename T>
 __global__ void __launch_bounds__(gpr::kBlock) k_pr_step(PrArgs a) {
   __shared__ int s_it, s_last;
   if (threadIdx.x == 0) {
@@ -463,9 +511,9 @@ __global__ void __launch_bounds__(gpr::kBlock) k_pr_step(PrArgs a) {
   const long long gw = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
   const Policies pol = make_policies();
-  const float *cin = (it & 1) ? a.c1 : a.c0;
-  float *cout = (it & 1) ? a.c0 : a.c1;
-  const double err = sweep<U, U4>(a, cin, cout, gw, nw, lane, it, pol);
+  const T *cin = static_cast<const T *>((it & 1) ? a.c1 : a.c0);
+  T *cout = static_cast<T *>((it & 1) ? a.c0 : a.c1);
+  const double err = sweep<U, U4, T>(a, cin, cout, gw, nw, lane, it, pol);
   const double tot = block_sum(err);
   if (threadIdx.x == 0) {
     a.cta_err[blockIdx.x] = tot;
@@ -489,17 +537,17 @@ __global__ void __launch_bounds__(gpr::kBlock) k_pr_step(PrArgs a) {
 }
 
 // Scores into the relabelled order and the first sweep's contributions.
+template <typename T>
 __global__ void k_pr_prologue(int m, const int *__restrict__ perm, const int *__restrict__ outdeg,
-                              const float *__restrict__ scores_in, float *s, float *c0,
-                              float *c1) {
+                              const float *__restrict__ scores_in, float *s, T *c0, T *c1) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < m) {
     const float v = scores_in[perm[i]];
     s[i] = v;
-    c0[i] = __fdiv_rn(v, __int2float_rn(outdeg[i]));
+    c0[i] = (T)__fdiv_rn(v, __int2float_rn(outdeg[i]));
   } else if (i == m) {
-    c0[m] = 0.f;  // sentinel slots of the padding entries
-    c1[m] = 0.f;
+    c0[m] = (T)0.f;  // sentinel slots of the padding entries
+    c1[m] = (T)0.f;
   }
 }
 
@@ -583,22 +631,44 @@ struct SweepKernels {
   const void *persistent;
   void (*step)(PrArgs);
   int ctas_per_sm;  // persistent kernel: co-resident 1024-thread CTAs per SM
-  int hot_cap;      // most contributions one CTA stages (shared memory per CTA)
+  int hot_bytes;    // most shared memory one CTA stages
+  int elem;         // bytes per contribution: 4 (FP32) or 2 (BF16)
 };
-const SweepKernels kVariants[] = {
-    {(const void *)k_pr_hot<16, 4, true, 1>, k_pr_step<16, 4>, 1, 56832},
-    {(const void *)k_pr_hot<8, 2, false, 1>, k_pr_step<8, 2>, 1, 56832},
-    {(const void *)k_pr_hot<4, 2, false, 1>, k_pr_step<4, 2>, 1, 56832},
-    {(const void *)k_pr_hot<32, 8, false, 1>, k_pr_step<32, 8>, 1, 56832},
-    {(const void *)k_pr_hot<16, 4, false, 1>, k_pr_step<16, 4>, 1, 56832},
-    {(const void *)k_pr_hot<8, 2, true, 1>, k_pr_step<8, 2>, 1, 56832},
-    {(const void *)k_pr_hot<8, 2, false, 2>, k_pr_step<8, 2>, 2, 24576},
-    {(const void *)k_pr_hot<8, 2, true, 2>, k_pr_step<8, 2>, 2, 24576},
+using bf16 = __nv_bfloat16;
+// Indices 0..7: the FP32 variants a caller selects with opts.variant;
+// index kBf16Kernel: the BF16-contribution kernel of the mixed form.
+const SweepKernels kKernels[] = {
+    {(const void *)k_pr_hot<16, 4, true, 1, float>, k_pr_step<16, 4, float>, 1, 227328, 4},
+    {(const void *)k_pr_hot<8, 2, false, 1, float>, k_pr_step<8, 2, float>, 1, 227328, 4},
+    {(const void *)k_pr_hot<4, 2, false, 1, float>, k_pr_step<4, 2, float>, 1, 227328, 4},
+    {(const void *)k_pr_hot<32, 8, false, 1, float>, k_pr_step<32, 8, float>, 1, 227328, 4},
+    {(const void *)k_pr_hot<16, 4, false, 1, float>, k_pr_step<16, 4, float>, 1, 227328, 4},
+    {(const void *)k_pr_hot<8, 2, true, 1, float>, k_pr_step<8, 2, float>, 1, 227328, 4},
+    {(const void *)k_pr_hot<8, 2, false, 2, float>, k_pr_step<8, 2, float>, 2, 98304, 4},
+    {(const void *)k_pr_hot<8, 2, true, 2, float>, k_pr_step<8, 2, float>, 2, 98304, 4},
+    {(const void *)k_pr_hot<16, 4, true, 1, bf16>, k_pr_step<16, 4, bf16>, 1, 227328, 2},
 };
 constexpr int kHotBlock = 1024;
-constexpr int kNumVariants = sizeof(kVariants) / sizeof(kVariants[0]);
+constexpr int kNumVariants = 8;
+constexpr int kBf16Kernel = 8;
+constexpr int kNumKernels = sizeof(kKernels) / sizeof(kKernels[0]);
+// The BF16 phase of the mixed form stops once the L1 change is below this
+// (or the caller's tol if larger): about where BF16 rounding of the
+// contributions stops the residual from falling further.
+constexpr double kBf16Tol = 1e-3;
 
-PrArgs make_args(gpr_graph *g, const gpr_pr_opts &o) {
+// Contributions kernel ki stages in shared memory: the caller's hot budget in
+// bytes, covering the sentinel slot m when the whole array fits, a multiple
+// of 16 bytes.
+int hot_entries(const gpr_graph *g, int ki) {
+  const int elem = kKernels[ki].elem, per16 = 16 / elem;
+  long long n = std::min<long long>((long long)g->hot_bytes, kKernels[ki].hot_bytes) / elem;
+  const long long all = ((long long)g->L.m + 1 + per16 - 1) / per16 * per16;
+  n = std::min(n, all);
+  return (int)(n / per16 * per16);
+}
+
+PrArgs make_args(gpr_graph *g, const gpr_pr_opts &o, int ki) {
   const PrLayout &L = g->L;
   PrArgs a;
   a.m = L.m;
@@ -617,8 +687,8 @@ PrArgs make_args(gpr_graph *g, const gpr_pr_opts &o) {
   a.sell_col = L.sell_col;
   a.outdeg = L.outdeg;
   a.s = g->s;
-  a.c0 = g->c0;
-  a.c1 = g->c1;
+  a.c0 = kKernels[ki].elem == 2 ? (void *)g->h0 : (void *)g->c0;
+  a.c1 = kKernels[ki].elem == 2 ? (void *)g->h1 : (void *)g->c1;
   a.partial = g->partial;
   a.cnt = g->cnt;
   a.cta_err = g->cta_err;
@@ -629,12 +699,12 @@ PrArgs make_args(gpr_graph *g, const gpr_pr_opts &o) {
   a.base = (1.0f - o.damping) / (float)L.m;  // src/pr/omp_base.cc:16
   a.tol = o.tol;
   a.max_iter = o.max_iter;
-  a.bar_expect = g->grid_hot[o.variant];
-  a.hot = std::min(g->hot, kVariants[o.variant].hot_cap);
+  a.bar_expect = g->grid_hot[ki];
+  a.hot = hot_entries(g, ki);
   a.wq = g->wq;
   {
     const long long heavy = (long long)L.n_chunks + L.n_slices;
-    const long long warps = (long long)g->grid_hot[o.variant] * (kHotBlock / 32);
+    const long long warps = (long long)g->grid_hot[ki] * (kHotBlock / 32);
     a.batch = (int)std::max<long long>(1, heavy / (warps * 4));
   }
   a.timeout_ns = (long long)(o.timeout_s * 1e9);
@@ -647,6 +717,8 @@ void destroy(gpr_graph *g) {
   gpr::dfree(g->s);
   gpr::dfree(g->c0);
   gpr::dfree(g->c1);
+  gpr::dfree(g->h0);
+  gpr::dfree(g->h1);
   gpr::dfree(g->partial);
   gpr::dfree(g->cnt);
   gpr::dfree(g->cta_err);
@@ -695,10 +767,10 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
   GPR_TRY(rc);
   const PrLayout &L = g->L;
   GPR_TRY(gpr::dalloc(&g->s, (size_t)m, "scores"));
-  // Hot prefix: a multiple of 4 entries, covering the sentinel slot m when
-  // the whole array fits.  Contribution buffers are padded so the staging
-  // loads stay in bounds; the padding stays 0.
-  g->hot = (int)std::min<long long>(hot_max, ((long long)m + 1 + 3) & ~3LL);
+  // Hot prefix budget in bytes (FP32: hot_max entries).  Contribution
+  // buffers are padded so the staging loads stay in bounds; padding stays 0.
+  g->hot_bytes = 4 * hot_max;
+  g->hot = hot_entries(g, 0);
   const size_t cn = (size_t)std::max<long long>((long long)m + 1, g->hot) + 4;
   GPR_TRY(gpr::dalloc(&g->c0, cn, "contrib0"));
   GPR_TRY(gpr::dalloc(&g->c1, cn, "contrib1"));
@@ -720,28 +792,116 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
   g->coop = coop != 0;
   g->hot_ok = g->coop;
   const long long heavy = (long long)L.n_chunks + L.n_slices;
-  for (int v = 0; v < kNumVariants; ++v) {
+  for (int v = 0; v < kNumKernels; ++v) {
     int per_sm = 0;
-    const int hv = std::min(g->hot, kVariants[v].hot_cap);
-    GPR_CUDA(cudaFuncSetAttribute(kVariants[v].persistent,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(sizeof(float) * hv)));
-    GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kVariants[v].persistent,
-                                                           kHotBlock, sizeof(float) * hv));
-    if (per_sm < kVariants[v].ctas_per_sm) g->hot_ok = false;
+    const size_t smem = (size_t)hot_entries(g, v) * kKernels[v].elem;
+    GPR_CUDA(cudaFuncSetAttribute(kKernels[v].persistent,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kKernels[v].persistent,
+                                                           kHotBlock, smem));
+    if (per_sm < kKernels[v].ctas_per_sm) g->hot_ok = false;
     g->grid_hot[v] = (int)std::max<long long>(
-        1, std::min<long long>((long long)sms * kVariants[v].ctas_per_sm, gpr::ceil_div(heavy, 32)));
+        1, std::min<long long>((long long)sms * kKernels[v].ctas_per_sm, gpr::ceil_div(heavy, 32)));
   }
   GPR_TRY(gpr::dalloc(&g->wq, 2, "work queue"));
   long long step = need < 1 ? 1 : need;
   if (step > (long long)sms * 32) step = (long long)sms * 32;
   g->grid_step = (int)step;
   g->max_grid = g->grid_step;
-  for (int v = 0; v < kNumVariants; ++v) g->max_grid = std::max(g->max_grid, g->grid_hot[v]);
+  for (int v = 0; v < kNumKernels; ++v) g->max_grid = std::max(g->max_grid, g->grid_hot[v]);
   GPR_TRY(gpr::dalloc(&g->cta_err, 2 * (size_t)g->max_grid, "cta residuals"));
   g->err_cap = 128;
   GPR_TRY(gpr::dalloc(&g->err_hist, (size_t)g->err_cap, "residual history"));
   GPR_CUDA(cudaStreamSynchronize(st));
+  return GPR_OK;
+}
+
+// One solve with sweep kernel ki from the scores in d_scores (device, vertex
+// order); the result is written back to d_scores.
+int solve_impl(gpr_graph *g, float *d_scores, const gpr_pr_opts &o, int ki, gpr_pr_stats *out) {
+  const int m = g->L.m;
+  cudaStream_t st = g->st;
+  if (kKernels[ki].elem == 2 && !g->h0) {
+    const size_t cnh = (size_t)std::max<long long>((long long)m + 1, hot_entries(g, ki)) + 8;
+    GPR_TRY(gpr::dalloc(reinterpret_cast<bf16 **>(&g->h0), cnh, "bf16 contrib0"));
+    GPR_TRY(gpr::dalloc(reinterpret_cast<bf16 **>(&g->h1), cnh, "bf16 contrib1"));
+    GPR_CUDA(cudaMemsetAsync(g->h0, 0, 2 * cnh, st));
+    GPR_CUDA(cudaMemsetAsync(g->h1, 0, 2 * cnh, st));
+  }
+  GPR_CUDA(cudaMemsetAsync(g->bar, 0, 4 * sizeof(unsigned), st));
+  GPR_CUDA(cudaMemsetAsync(g->status, 0, 4 * sizeof(int), st));
+  GPR_CUDA(cudaMemsetAsync(g->wq, 0, 2 * sizeof(int), st));
+  if (g->L.n_long) GPR_CUDA(cudaMemsetAsync(g->cnt, 0, sizeof(int) * g->L.n_long, st));
+  PrArgs a = make_args(g, o, ki);
+  if (o.reserved[0] > 0) a.bar_expect += o.reserved[0];  // test hook: a barrier nobody completes
+  int launches = 0;
+  GPR_CUDA(cudaEventRecord(g->e0, st));
+  if (kKernels[ki].elem == 2)
+    k_pr_prologue<bf16><<<grid_for((long long)m + 1), 256, 0, st>>>(
+        m, g->L.perm, g->L.outdeg, d_scores, g->s, static_cast<bf16 *>(g->h0),
+        static_cast<bf16 *>(g->h1));
+  else
+    k_pr_prologue<float><<<grid_for((long long)m + 1), 256, 0, st>>>(
+        m, g->L.perm, g->L.outdeg, d_scores, g->s, g->c0, g->c1);
+  ++launches;
+  int loop = o.loop;
+  if (loop == GPR_LOOP_AUTO) loop = GPR_LOOP_PERSISTENT;
+  if (loop == GPR_LOOP_PERSISTENT && !g->hot_ok) loop = GPR_LOOP_GRAPH;
+  GPR_CUDA(cudaEventRecord(g->e2, st));
+  if (o.max_iter > 0) {
+    if (loop == GPR_LOOP_PERSISTENT) {
+      void *args[] = {&a};
+      cudaError_t e = cudaLaunchCooperativeKernel(kKernels[ki].persistent, dim3(g->grid_hot[ki]),
+                                                  dim3(kHotBlock), args,
+                                                  (size_t)a.hot * kKernels[ki].elem, st);
+      if (e == cudaErrorCooperativeLaunchTooLarge) {
+        cudaGetLastError();
+        loop = GPR_LOOP_GRAPH;
+      } else if (e != cudaSuccess) {
+        gpr::set_error("cooperative launch: %s", cudaGetErrorString(e));
+        return GPR_ECUDA;
+      } else {
+        ++launches;
+      }
+    }
+    if (loop == GPR_LOOP_GRAPH) {
+      const int batch = 8;
+      int done = 0, issued = 0;
+      while (!done && issued < o.max_iter) {
+        for (int q = 0; q < batch && issued < o.max_iter; ++q, ++issued) {
+          kKernels[ki].step<<<g->grid_step, gpr::kBlock, 0, st>>>(a);
+          ++launches;
+        }
+        GPR_CUDA(cudaGetLastError());
+        GPR_CUDA(cudaMemcpyAsync(&done, g->status + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
+        GPR_CUDA(cudaStreamSynchronize(st));
+      }
+    }
+  }
+  GPR_CUDA(cudaEventRecord(g->e3, st));
+  k_pr_scatter<<<grid_for(m), 256, 0, st>>>(m, g->L.perm, g->s, d_scores);
+  ++launches;
+  GPR_CUDA(cudaGetLastError());
+  GPR_CUDA(cudaEventRecord(g->e1, st));
+  int hs[4];
+  GPR_CUDA(cudaMemcpyAsync(hs, g->status, sizeof(hs), cudaMemcpyDeviceToHost, st));
+  GPR_CUDA(cudaStreamSynchronize(st));
+  float ms = 0.f, lms = 0.f;
+  GPR_CUDA(cudaEventElapsedTime(&ms, g->e0, g->e1));
+  GPR_CUDA(cudaEventElapsedTime(&lms, g->e2, g->e3));
+  memset(out, 0, sizeof(*out));
+  out->loop_ms = lms;
+  out->iterations = hs[1];
+  g->last_sweeps = hs[1];
+  out->solve_ms = ms;
+  out->gpu_launches = launches;
+  if (hs[1] > 0)
+    GPR_CUDA(cudaMemcpy(&out->residual, g->err_hist + hs[1] - 1, sizeof(double),
+                        cudaMemcpyDeviceToHost));
+  if (hs[0] & 1) {
+    gpr::set_error("grid barrier wait exceeded %.3f s (sweep loop abandoned)", o.timeout_s);
+    return GPR_ETIMEOUT;
+  }
   return GPR_OK;
 }
 
@@ -752,12 +912,13 @@ int pagerank_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts_in,
   else gpr_pr_opts_default(&o);
   if (!(o.damping >= 0.f && o.damping <= 1.f) || o.max_iter < 0 || !(o.tol >= 0.0) ||
       !(o.timeout_s > 0.0) || o.variant < 0 || o.variant >= kNumVariants) {
-    gpr::set_error("gpr_pagerank: invalid options (damping %g, tol %g, max_iter %d, timeout %g)",
-                   (double)o.damping, o.tol, o.max_iter, o.timeout_s);
+    gpr::set_error("gpr_pagerank: invalid options (damping %g, tol %g, max_iter %d, timeout %g, "
+                   "variant %d)", (double)o.damping, o.tol, o.max_iter, o.timeout_s, o.variant);
     return GPR_EINVAL;
   }
-  if (o.precision != GPR_PREC_FP32) {
-    gpr::set_error("gpr_pagerank: precision %d not available in this build", o.precision);
+  if (o.precision != GPR_PREC_FP32 && o.precision != GPR_PREC_BF16) {
+    gpr::set_error("gpr_pagerank: precision %d not supported (GPR_PREC_FP32 or GPR_PREC_BF16)",
+                   o.precision);
     return GPR_EUNSUPPORTED;
   }
   const int m = g->L.m;
@@ -785,78 +946,34 @@ int pagerank_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts_in,
     GPR_CUDA(cudaMemcpyAsync(d_scores, any_scores, sizeof(float) * (size_t)m,
                              cudaMemcpyHostToDevice, st));
   }
-  GPR_CUDA(cudaMemsetAsync(g->bar, 0, 4 * sizeof(unsigned), st));
-  GPR_CUDA(cudaMemsetAsync(g->status, 0, 4 * sizeof(int), st));
-  GPR_CUDA(cudaMemsetAsync(g->wq, 0, 2 * sizeof(int), st));
-  if (g->L.n_long) GPR_CUDA(cudaMemsetAsync(g->cnt, 0, sizeof(int) * g->L.n_long, st));
-  PrArgs a = make_args(g, o);
-  if (o.reserved[0] > 0) a.bar_expect += o.reserved[0];  // test hook: a barrier nobody completes
-  int launches = 0;
-  GPR_CUDA(cudaEventRecord(g->e0, st));
-  k_pr_prologue<<<grid_for((long long)m + 1), 256, 0, st>>>(m, g->L.perm, g->L.outdeg, d_scores,
-                                                           g->s, g->c0, g->c1);
-  ++launches;
-  int loop = o.loop;
-  if (loop == GPR_LOOP_AUTO) loop = GPR_LOOP_PERSISTENT;
-  if (loop == GPR_LOOP_PERSISTENT && !g->hot_ok) loop = GPR_LOOP_GRAPH;
-  GPR_CUDA(cudaEventRecord(g->e2, st));
-  if (o.max_iter > 0) {
-    if (loop == GPR_LOOP_PERSISTENT) {
-      void *args[] = {&a};
-      cudaError_t e = cudaLaunchCooperativeKernel(kVariants[o.variant].persistent,
-                                                  dim3(g->grid_hot[o.variant]), dim3(kHotBlock),
-                                                  args, sizeof(float) * a.hot, st);
-      if (e == cudaErrorCooperativeLaunchTooLarge) {
-        cudaGetLastError();
-        loop = GPR_LOOP_GRAPH;
-      } else if (e != cudaSuccess) {
-        gpr::set_error("cooperative launch: %s", cudaGetErrorString(e));
-        return GPR_ECUDA;
-      } else {
-        ++launches;
-      }
-    }
-    if (loop == GPR_LOOP_GRAPH) {
-      const int batch = 8;
-      int done = 0, issued = 0;
-      while (!done && issued < o.max_iter) {
-        for (int q = 0; q < batch && issued < o.max_iter; ++q, ++issued) {
-          kVariants[o.variant].step<<<g->grid_step, gpr::kBlock, 0, st>>>(a);
-          ++launches;
-        }
-        GPR_CUDA(cudaGetLastError());
-        GPR_CUDA(cudaMemcpyAsync(&done, g->status + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
-        GPR_CUDA(cudaStreamSynchronize(st));
-      }
+  int rc = GPR_OK;
+  if (o.precision == GPR_PREC_FP32) {
+    rc = solve_impl(g, d_scores, o, o.variant, &st_local);
+  } else {
+    // Mixed form: BF16 contributions (twice the entries in the shared-memory
+    // cache, half the bytes per gather) until the change is below
+    // max(tol, kBf16Tol), then plain FP32 sweeps from those scores to tol.
+    gpr_pr_opts o1 = o;
+    o1.tol = std::max(o.tol, kBf16Tol);
+    gpr_pr_stats s1, s2;
+    rc = solve_impl(g, d_scores, o1, kBf16Kernel, &s1);
+    if (rc == GPR_OK) {
+      gpr_pr_opts o2 = o;
+      o2.max_iter = std::max(0, o.max_iter - s1.iterations);
+      rc = solve_impl(g, d_scores, o2, o.variant, &s2);
+      st_local = s2;
+      st_local.iterations = s1.iterations + s2.iterations;
+      st_local.refine_iterations = s2.iterations;
+      st_local.solve_ms = s1.solve_ms + s2.solve_ms;
+      st_local.loop_ms = s1.loop_ms + s2.loop_ms;
+      st_local.gpu_launches = s1.gpu_launches + s2.gpu_launches;
+      if (s2.iterations == 0) st_local.residual = s1.residual;
     }
   }
-  GPR_CUDA(cudaEventRecord(g->e3, st));
-  k_pr_scatter<<<grid_for(m), 256, 0, st>>>(m, g->L.perm, g->s, d_scores);
-  ++launches;
-  GPR_CUDA(cudaGetLastError());
-  GPR_CUDA(cudaEventRecord(g->e1, st));
-  int hs[4];
-  GPR_CUDA(cudaMemcpyAsync(hs, g->status, sizeof(hs), cudaMemcpyDeviceToHost, st));
-  GPR_CUDA(cudaStreamSynchronize(st));
-  float ms = 0.f, lms = 0.f;
-  GPR_CUDA(cudaEventElapsedTime(&ms, g->e0, g->e1));
-  GPR_CUDA(cudaEventElapsedTime(&lms, g->e2, g->e3));
-  st_local.loop_ms = lms;
-  st_local.iterations = hs[1];
-  g->last_sweeps = hs[1];
-  st_local.solve_ms = ms;
-  st_local.gpu_launches = launches;
-  if (hs[1] > 0)
-    GPR_CUDA(cudaMemcpy(&st_local.residual, g->err_hist + hs[1] - 1, sizeof(double),
-                        cudaMemcpyDeviceToHost));
-  if (host)
+  if (host && rc == GPR_OK)
     GPR_CUDA(cudaMemcpy(any_scores, d_scores, sizeof(float) * (size_t)m, cudaMemcpyDeviceToHost));
   if (stats) *stats = st_local;
-  if (hs[0] & 1) {
-    gpr::set_error("grid barrier wait exceeded %.3f s (sweep loop abandoned)", o.timeout_s);
-    return GPR_ETIMEOUT;
-  }
-  return GPR_OK;
+  return rc;
 }
 
 }  // namespace
@@ -998,7 +1115,7 @@ int gpr_pr_residual_f64(gpr_graph *g, const float *any_scores, float damping, do
   gpr_pr_opts o;
   gpr_pr_opts_default(&o);
   o.damping = damping;
-  PrArgs a = make_args(g, o);
+  PrArgs a = make_args(g, o, 0);
   const double d = (double)damping, base = (1.0 - d) / (double)m;
   cudaMemsetAsync(acc, 0, sizeof(double) * ((size_t)L.n_long + 1), st);
   k_res_prologue<<<grid_for((long long)m + 1), 256, 0, st>>>(m, L.perm, L.outdeg,

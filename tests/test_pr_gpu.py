@@ -179,3 +179,21 @@ def test_reference_shaped_calls(G, O):
     s2 = np.full(m, np.float32(1.0) / np.float32(m), dtype=np.float32)
     G.PageRank(m, len(col), rp, col, od, s2)
     assert np.array_equal(s, s2)
+
+
+@pytest.mark.parametrize("loop", ["persistent", "graph"])
+def test_bf16_mixed_form_matches_plain_accuracy(G, O, loop):
+    """Mixed form: BF16 contributions until the change is below 1e-3, then
+    FP32 refinement sweeps to the tolerance.  Its FP64-oracle error must match
+    the plain FP32 path's (within 10% + 1e-8)."""
+    rp, col, od = O.rmat_graph(14, 16, seed=12)
+    s64, _, _ = O.pr_f64(rp, col, od)
+    lp = G.LOOP_PERSISTENT if loop == "persistent" else G.LOOP_GRAPH
+    with G.Graph(rp, col, od) as g:
+        plain, sp = g.pagerank(tol=1e-6, max_iter=100, loop=lp)
+        mixed, sm = g.pagerank(tol=1e-6, max_iter=100, loop=lp, precision=G.PREC_BF16)
+    mx_p, l1_p = O.err_vs_f64(plain, s64)
+    mx_m, l1_m = O.err_vs_f64(mixed, s64)
+    assert sm.refine_iterations > 0 and sm.iterations > sm.refine_iterations
+    assert sm.residual < 1e-6
+    assert l1_m <= 1.1 * l1_p + 1e-8 and mx_m <= 1.1 * mx_p + 1e-9
