@@ -103,6 +103,16 @@ def lib():
                              C.POINTER(_vp), C.POINTER(LL)]),
         "gpr_gen_stencil27": (I, [I, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),
                                   C.POINTER(LL)]),
+        "gpr_gen_multigraph": (I, [I, I, I, I, I, D, C.c_ulonglong, _vp, C.POINTER(_vp),
+                                   C.POINTER(_vp), C.POINTER(_vp), C.POINTER(LL)]),
+        "gpr_multigraph_create": (I, [I, _vp, LL, _vp, _vp, _vp, C.POINTER(LayoutOptions),
+                                      C.POINTER(_vp)]),
+        "gpr_multigraph_destroy": (I, [_vp]),
+        "gpr_multigraph_info": (I, [_vp, C.POINTER(I), C.POINTER(I), C.POINTER(LL),
+                                    C.POINTER(I), C.POINTER(LL)]),
+        "gpr_multigraph_set_stream": (I, [_vp, _vp]),
+        "gpr_multigraph_pagerank": (I, [_vp, _vp, C.POINTER(PrOptions), _vp, _vp,
+                                        C.POINTER(PrStats)]),
         "gpr_gen_uniform": (I, [LL, C.c_ulonglong, _vp]),
         "gpr_free": (I, [_vp]),
         "gpr_malloc": (I, [C.POINTER(_vp), C.c_size_t]),
@@ -288,6 +298,93 @@ class Graph:
         self.close()
 
 
+class MultiGraph:
+    """Uneven batch of independent pull graphs stored as one block-diagonal
+    graph: graph g owns vertices [voff[g], voff[g+1]) and the in-edges of its
+    rows come from that range (global vertex ids).  ``layouts``: None, or one
+    dict per graph with any of sell_max / chunk / chunk_min (each graph's own
+    bins).  Every graph is solved as ``Graph.pagerank`` solves it alone, all
+    in one persistent launch."""
+
+    def __init__(self, rowptr, col, outdeg, voff, nnz=None, layouts=None):
+        L = lib()
+        self.voff = np.ascontiguousarray(voff, dtype=np.int32)
+        self.n_graphs = len(self.voff) - 1
+        self.m = int(self.voff[-1])
+        nnz = int(len(col)) if nnz is None else int(nnz)
+        lo = None
+        if layouts is not None:
+            if len(layouts) != self.n_graphs:
+                raise ValueError("one layout per graph")
+            lo = (LayoutOptions * self.n_graphs)()
+            for i, d in enumerate(layouts):
+                d = d or {}
+                lo[i] = LayoutOptions(int(d.get("sell_max", 0)), int(d.get("chunk", 0)),
+                                      int(d.get("chunk_min", 0)), 0, 0)
+        pr, k0 = _ptr(rowptr, np.int32)
+        pc, k1 = _ptr(col, np.int32)
+        pd, k2 = _ptr(outdeg, np.int32)
+        h = C.c_void_p()
+        _check(L.gpr_multigraph_create(self.n_graphs, C.c_void_p(self.voff.ctypes.data), nnz,
+                                       pr, pc, pd, lo, C.byref(h)))
+        self._h, self.nnz = h, nnz
+        self.last_stats = None
+
+    def initial_scores(self):
+        """1/m_g on every vertex of graph g (src/pr/main.cc:27-28, per graph)."""
+        sizes = np.diff(self.voff)
+        vals = np.where(sizes > 0, np.float32(1.0) / np.maximum(sizes, 1).astype(np.float32),
+                        np.float32(0.0)).astype(np.float32)
+        return np.repeat(vals, sizes)
+
+    def pagerank(self, scores=None, opts: PrOptions | None = None, **kw):
+        """Returns (scores, iters[n_graphs], residuals[n_graphs], stats);
+        ``scores`` host float32 (new array of 1/m_g when None) or device
+        memory updated in place."""
+        o = opts if opts is not None else options(**kw)
+        if scores is None:
+            scores = self.initial_scores()
+        if isinstance(scores, np.ndarray) and (scores.dtype != np.float32 or
+                                               not scores.flags.c_contiguous):
+            raise TypeError("scores must be a contiguous float32 array")
+        iters = np.zeros(self.n_graphs, dtype=np.int32)
+        res = np.zeros(self.n_graphs, dtype=np.float64)
+        ps, keep = _ptr(scores)
+        st = PrStats()
+        _check(lib().gpr_multigraph_pagerank(self._h, ps, C.byref(o),
+                                             C.c_void_p(iters.ctypes.data),
+                                             C.c_void_p(res.ctypes.data), C.byref(st)))
+        self.last_stats = st
+        return scores, iters, res, st
+
+    def info(self):
+        g, m, nnz, u, es = C.c_int(), C.c_int(), C.c_longlong(), C.c_int(), C.c_longlong()
+        _check(lib().gpr_multigraph_info(self._h, C.byref(g), C.byref(m), C.byref(nnz),
+                                         C.byref(u), C.byref(es)))
+        return {"n_graphs": g.value, "m": m.value, "nnz": nnz.value, "units": u.value,
+                "edge_slots": es.value}
+
+    def set_stream(self, stream_handle: int):
+        _check(lib().gpr_multigraph_set_stream(self._h, C.c_void_p(stream_handle)))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gpr_multigraph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def PRSolver(m, nnz, in_row_offsets, in_column_indices, out_row_offsets, out_column_indices,
              degree, scores, tol=EPSILON, max_iter=MAX_ITER, **kw):
     """src/pr/pr.h:23.  ``scores`` (float32, host or device) is updated in
@@ -433,6 +530,19 @@ def gen_stencil27(n) -> DeviceCSR:
     ap, aj, ax, nnz = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_longlong()
     _check(lib().gpr_gen_stencil27(int(n), C.byref(ap), C.byref(aj), C.byref(ax), C.byref(nnz)))
     return DeviceCSR(n ** 3, nnz.value, ap.value, aj.value, ax.value, np.float32)
+
+
+def gen_multigraph(n_graphs, m_min=1000, m_max=500000, seed=1, er_deg=8, cl_deg=16,
+                   gamma=2.1):
+    """Seeded uneven batch on the GPU (gpr_gen_multigraph): returns
+    (DeviceCSR with third = out-degree, voff[n_graphs + 1] numpy)."""
+    voff = np.zeros(n_graphs + 1, dtype=np.int32)
+    rp, cp, dp, nnz = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_longlong()
+    _check(lib().gpr_gen_multigraph(int(n_graphs), int(m_min), int(m_max), int(er_deg),
+                                    int(cl_deg), float(gamma), int(seed),
+                                    C.c_void_p(voff.ctypes.data), C.byref(rp), C.byref(cp),
+                                    C.byref(dp), C.byref(nnz)))
+    return DeviceCSR(int(voff[-1]), nnz.value, rp.value, cp.value, dp.value, np.int32), voff
 
 
 def gen_uniform(n, seed, d_out) -> None:

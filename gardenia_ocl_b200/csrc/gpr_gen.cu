@@ -6,6 +6,11 @@
 // the SplitMix64 finaliser (Steele, Lea, Flood 2014), so the same graph can
 // be rebuilt anywhere from its parameters.
 #include <cub/cub.cuh>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
 
 #include "gpr_internal.cuh"
 
@@ -129,6 +134,127 @@ unsigned capped_grid(long long n) {
   return (unsigned)g;
 }
 
+// Keys (dst << 32 | src, kDropKey for dropped draws) -> in-CSR with ascending
+// distinct sources per row, and out-degrees.  k0 holds the keys; k1 is
+// scratch of the same size.  Allocates the three outputs.
+int csr_from_keys(long long ne, int m, uint64_t *k0, uint64_t *k1, int **d_rowptr, int **d_col,
+                  int **d_outdeg, long long *nnz_out) {
+  cudaStream_t st = 0;
+  int *nsel = nullptr;
+  void *tmp = nullptr;
+  int rc = GPR_OK;
+  long long nnz = 0;
+  int *rowptr = nullptr, *col = nullptr, *outdeg = nullptr;
+  do {
+    if ((rc = gpr::dalloc(&nsel, 1, "unique count")) != GPR_OK) break;
+    cub::DoubleBuffer<uint64_t> db(k0, k1);
+    size_t tb = 0, tb2 = 0;
+    cub::DeviceRadixSort::SortKeys(nullptr, tb, db, (int)ne, 0, 64, st);
+    cub::DeviceSelect::Unique(nullptr, tb2, k0, k1, nsel, (int)ne, st);
+    if (tb2 > tb) tb = tb2;
+    if ((rc = gpr::dmalloc(&tmp, tb, "sort scratch")) != GPR_OK) break;
+    cudaError_t e = cub::DeviceRadixSort::SortKeys(tmp, tb, db, (int)ne, 0, 64, st);
+    uint64_t *sorted = db.Current(), *uniq = db.Alternate();
+    if (e == cudaSuccess) e = cub::DeviceSelect::Unique(tmp, tb, sorted, uniq, nsel, (int)ne, st);
+    int nu = 0;
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&nu, nsel, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    uint64_t lastkey = 0;
+    if (e == cudaSuccess && nu > 0)
+      e = cudaMemcpy(&lastkey, uniq + nu - 1, sizeof(uint64_t), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) {
+      gpr::set_error("edge sort: %s", cudaGetErrorString(e));
+      rc = GPR_ECUDA;
+      break;
+    }
+    nnz = (nu > 0 && lastkey == kDropKey) ? nu - 1 : nu;
+    if ((rc = gpr::dalloc(&rowptr, (size_t)m + 1, "rowptr")) != GPR_OK) break;
+    if ((rc = gpr::dalloc(&col, (size_t)nnz, "col")) != GPR_OK) break;
+    if ((rc = gpr::dalloc(&outdeg, (size_t)m, "outdeg")) != GPR_OK) break;
+    cudaMemsetAsync(rowptr, 0, sizeof(int) * ((size_t)m + 1), st);
+    cudaMemsetAsync(outdeg, 0, sizeof(int) * (size_t)m, st);
+    k_split_keys<<<capped_grid(nnz), 256, 0, st>>>(nnz, uniq, col, rowptr, outdeg);
+    cudaFree(tmp);
+    tmp = nullptr;
+    size_t ts = 0;
+    cub::DeviceScan::ExclusiveSum(nullptr, ts, rowptr, rowptr, m + 1, st);
+    if ((rc = gpr::dmalloc(&tmp, ts, "scan scratch")) != GPR_OK) break;
+    e = cub::DeviceScan::ExclusiveSum(tmp, ts, rowptr, rowptr, m + 1, st);
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) {
+      gpr::set_error("CSR from edges: %s", cudaGetErrorString(e));
+      rc = GPR_ECUDA;
+      break;
+    }
+  } while (0);
+  gpr::dfree(nsel);
+  gpr::dfree(tmp);
+  if (rc != GPR_OK) {
+    gpr::dfree(rowptr);
+    gpr::dfree(col);
+    gpr::dfree(outdeg);
+    return rc;
+  }
+  *d_rowptr = rowptr;
+  *d_col = col;
+  *d_outdeg = outdeg;
+  *nnz_out = nnz;
+  return GPR_OK;
+}
+
+// Size of graph g of a multi-graph batch: log-uniform in [m_min, m_max].
+int multigraph_size(int g, int m_min, int m_max, uint64_t seed) {
+  const uint64_t h = hash3(seed, (uint64_t)g, 0x6d67u);
+  const double u = (double)(h >> 11) * 0x1.0p-53;
+  const double lo = log((double)m_min), hi = log((double)m_max);
+  const double t = u * (hi - lo);
+  int m = (int)floor(exp(lo + t));
+  return std::min(std::max(m, m_min), m_max);
+}
+
+// Draw of a Chung-Lu endpoint: first i in [0, m) with P[i] > x * P[m - 1].
+__device__ __forceinline__ int cl_draw(uint64_t h, const double *__restrict__ P, int m) {
+  const double x = (double)(h >> 11) * 0x1.0p-53;
+  const double y = __dmul_rn(x, P[m - 1]);
+  int lo = 0, hi = m;
+  while (lo < hi) {
+    const int mid = lo + (hi - lo) / 2;
+    if (P[mid] > y) hi = mid;
+    else lo = mid + 1;
+  }
+  return lo < m ? lo : m - 1;
+}
+
+// Draw e of the batch (graph found by binary search over the draw offsets)
+// -> global key (dst << 32 | src), self-loops -> kDropKey.  Odd graphs are
+// Chung-Lu, even graphs Erdos-Renyi.
+__global__ void k_multi_keys(long long ne, int G, const long long *__restrict__ eoff,
+                             const int *__restrict__ voff, const unsigned long long *__restrict__ gs,
+                             const double *__restrict__ P, uint64_t *keys) {
+  const long long stride = (long long)gridDim.x * blockDim.x;
+  for (long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x; e < ne; e += stride) {
+    int lo = 0, hi = G;  // last g with eoff[g] <= e
+    while (hi - lo > 1) {
+      const int mid = (lo + hi) >> 1;
+      if (eoff[mid] <= e) lo = mid;
+      else hi = mid;
+    }
+    const int g = lo, v0 = voff[g], mg = voff[g + 1] - v0;
+    const uint64_t le = (uint64_t)(e - eoff[g]);
+    const uint64_t h = hash3(gs[g], le, 0);
+    uint32_t s, t;
+    if (g & 1) {
+      s = (uint32_t)cl_draw(h, P, mg);
+      t = (uint32_t)cl_draw(hash3(gs[g], le, 1), P, mg);
+    } else {
+      s = (uint32_t)(((h >> 32) * (uint64_t)mg) >> 32);
+      t = (uint32_t)(((h & 0xffffffffULL) * (uint64_t)mg) >> 32);
+    }
+    keys[e] = (s == t) ? kDropKey : (((uint64_t)(v0 + t) << 32) | (uint64_t)(v0 + s));
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -153,75 +279,87 @@ int gpr_gen_rmat(int scale, int edge_factor, double a, double b, double c,
   const uint32_t t0 = (uint32_t)(a * 4294967296.0);
   const uint32_t t1 = (uint32_t)((a + b) * 4294967296.0);
   const uint32_t t2 = (uint32_t)((a + b + c) * 4294967296.0);
-  cudaStream_t st = 0;
   uint64_t *k0 = nullptr, *k1 = nullptr;
-  int *nsel = nullptr;
-  void *tmp = nullptr;
-  int rc = GPR_OK;
-  long long nnz = 0;
-  int *rowptr = nullptr, *col = nullptr, *outdeg = nullptr;
-  do {
-    if ((rc = gpr::dalloc(&k0, (size_t)ne, "rmat keys")) != GPR_OK) break;
-    if ((rc = gpr::dalloc(&k1, (size_t)ne, "rmat keys (alt)")) != GPR_OK) break;
-    if ((rc = gpr::dalloc(&nsel, 1, "unique count")) != GPR_OK) break;
-    k_rmat_keys<<<capped_grid(ne), 256, 0, st>>>(ne, scale, t0, t1, t2, seed, do_scramble,
-                                                  make_scramble(scale, seed), k0);
-    cub::DoubleBuffer<uint64_t> db(k0, k1);
-    size_t tb = 0, tb2 = 0;
-    cub::DeviceRadixSort::SortKeys(nullptr, tb, db, (int)ne, 0, 64, st);
-    cub::DeviceSelect::Unique(nullptr, tb2, k0, k1, nsel, (int)ne, st);
-    if (tb2 > tb) tb = tb2;
-    if ((rc = gpr::dmalloc(&tmp, tb, "sort scratch")) != GPR_OK) break;
-    cudaError_t e = cub::DeviceRadixSort::SortKeys(tmp, tb, db, (int)ne, 0, 64, st);
-    uint64_t *sorted = db.Current(), *uniq = db.Alternate();
-    if (e == cudaSuccess) e = cub::DeviceSelect::Unique(tmp, tb, sorted, uniq, nsel, (int)ne, st);
-    int nu = 0;
-    if (e == cudaSuccess) e = cudaMemcpyAsync(&nu, nsel, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    uint64_t lastkey = 0;
-    if (e == cudaSuccess && nu > 0)
-      e = cudaMemcpy(&lastkey, uniq + nu - 1, sizeof(uint64_t), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess) {
-      gpr::set_error("gpr_gen_rmat: %s", cudaGetErrorString(e));
-      rc = GPR_ECUDA;
-      break;
-    }
-    nnz = (nu > 0 && lastkey == kDropKey) ? nu - 1 : nu;
-    if ((rc = gpr::dalloc(&rowptr, (size_t)m + 1, "rowptr")) != GPR_OK) break;
-    if ((rc = gpr::dalloc(&col, (size_t)nnz, "col")) != GPR_OK) break;
-    if ((rc = gpr::dalloc(&outdeg, (size_t)m, "outdeg")) != GPR_OK) break;
-    cudaMemsetAsync(rowptr, 0, sizeof(int) * ((size_t)m + 1), st);
-    cudaMemsetAsync(outdeg, 0, sizeof(int) * (size_t)m, st);
-    k_split_keys<<<capped_grid(nnz), 256, 0, st>>>(nnz, uniq, col, rowptr, outdeg);
-    cudaFree(tmp);
-    tmp = nullptr;
-    size_t ts = 0;
-    cub::DeviceScan::ExclusiveSum(nullptr, ts, rowptr, rowptr, m + 1, st);
-    if ((rc = gpr::dmalloc(&tmp, ts, "scan scratch")) != GPR_OK) break;
-    e = cub::DeviceScan::ExclusiveSum(tmp, ts, rowptr, rowptr, m + 1, st);
-    if (e == cudaSuccess) e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) {
-      gpr::set_error("gpr_gen_rmat: %s", cudaGetErrorString(e));
-      rc = GPR_ECUDA;
-      break;
-    }
-  } while (0);
+  int rc = gpr::dalloc(&k0, (size_t)ne, "rmat keys");
+  if (rc == GPR_OK) rc = gpr::dalloc(&k1, (size_t)ne, "rmat keys (alt)");
+  if (rc == GPR_OK) {
+    k_rmat_keys<<<capped_grid(ne), 256>>>(ne, scale, t0, t1, t2, seed, do_scramble,
+                                           make_scramble(scale, seed), k0);
+    rc = csr_from_keys(ne, m, k0, k1, d_rowptr, d_col, d_outdeg, nnz_out);
+  }
   gpr::dfree(k0);
   gpr::dfree(k1);
-  gpr::dfree(nsel);
-  gpr::dfree(tmp);
-  if (rc != GPR_OK) {
-    gpr::dfree(rowptr);
-    gpr::dfree(col);
-    gpr::dfree(outdeg);
-    return rc;
+  return rc;
+}
+
+int gpr_gen_multigraph(int n_graphs, int m_min, int m_max, int er_deg, int cl_deg, double gamma,
+                       unsigned long long seed, int *h_voff, int **d_rowptr, int **d_col,
+                       int **d_outdeg, long long *nnz_out) {
+  if (n_graphs < 1 || m_min < 1 || m_max < m_min || er_deg < 1 || cl_deg < 1 ||
+      !(gamma > 1.0) || !h_voff || !d_rowptr || !d_col || !d_outdeg || !nnz_out) {
+    gpr::set_error("gpr_gen_multigraph: invalid arguments");
+    return GPR_EINVAL;
   }
-  *d_rowptr = rowptr;
-  *d_col = col;
-  *d_outdeg = outdeg;
-  *nnz_out = nnz;
-  return GPR_OK;
+  *d_rowptr = nullptr;
+  *d_col = nullptr;
+  *d_outdeg = nullptr;
+  std::vector<int> voff(n_graphs + 1, 0);
+  std::vector<long long> eoff(n_graphs + 1, 0);
+  std::vector<unsigned long long> gs(n_graphs);
+  int m_big = 1;
+  for (int g = 0; g < n_graphs; ++g) {
+    const int mg = multigraph_size(g, m_min, m_max, seed);
+    m_big = std::max(m_big, mg);
+    if ((long long)voff[g] + mg > 0x7fffffffLL) {
+      gpr::set_error("gpr_gen_multigraph: more than 2^31-1 vertices");
+      return GPR_EINVAL;
+    }
+    voff[g + 1] = voff[g] + mg;
+    eoff[g + 1] = eoff[g] + (long long)mg * ((g & 1) ? cl_deg : er_deg);
+    gs[g] = hash3(seed, (uint64_t)g, 0x9e37u);
+  }
+  const long long ne = eoff[n_graphs];
+  if (ne > 0x7fffffffLL) {
+    gpr::set_error("gpr_gen_multigraph: %lld edge draws exceed int32 CSR", ne);
+    return GPR_EINVAL;
+  }
+  // Chung-Lu weights (j + 1)^(-1/(gamma - 1)), prefix-summed in index order.
+  std::vector<double> P(m_big);
+  {
+    const double alpha = -1.0 / (gamma - 1.0);
+    double acc = 0.0;
+    for (int i = 0; i < m_big; ++i) {
+      acc += pow((double)(i + 1), alpha);
+      P[i] = acc;
+    }
+  }
+  uint64_t *k0 = nullptr, *k1 = nullptr;
+  int *dvoff = nullptr;
+  long long *deoff = nullptr;
+  unsigned long long *dgs = nullptr;
+  double *dP = nullptr;
+  int rc = gpr::dalloc(&k0, (size_t)ne, "multigraph keys");
+  if (rc == GPR_OK) rc = gpr::dalloc(&k1, (size_t)ne, "multigraph keys (alt)");
+  if (rc == GPR_OK) rc = gpr::dalloc(&dvoff, (size_t)n_graphs + 1, "vertex offsets");
+  if (rc == GPR_OK) rc = gpr::dalloc(&deoff, (size_t)n_graphs + 1, "draw offsets");
+  if (rc == GPR_OK) rc = gpr::dalloc(&dgs, (size_t)n_graphs, "graph seeds");
+  if (rc == GPR_OK) rc = gpr::dalloc(&dP, (size_t)m_big, "Chung-Lu prefix");
+  if (rc == GPR_OK) {
+    cudaMemcpy(dvoff, voff.data(), sizeof(int) * voff.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(deoff, eoff.data(), sizeof(long long) * eoff.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(dgs, gs.data(), sizeof(unsigned long long) * gs.size(), cudaMemcpyHostToDevice);
+    cudaMemcpy(dP, P.data(), sizeof(double) * P.size(), cudaMemcpyHostToDevice);
+    k_multi_keys<<<capped_grid(ne), 256>>>(ne, n_graphs, deoff, dvoff, dgs, dP, k0);
+    rc = csr_from_keys(ne, voff[n_graphs], k0, k1, d_rowptr, d_col, d_outdeg, nnz_out);
+  }
+  gpr::dfree(k0);
+  gpr::dfree(k1);
+  gpr::dfree(dvoff);
+  gpr::dfree(deoff);
+  gpr::dfree(dgs);
+  gpr::dfree(dP);
+  if (rc == GPR_OK) memcpy(h_voff, voff.data(), sizeof(int) * voff.size());
+  return rc;
 }
 
 int gpr_gen_stencil27(int n, int **d_Ap, int **d_Aj, float **d_Ax, long long *nnz_out) {

@@ -29,11 +29,10 @@
 
 #include <cuda_bf16.h>
 
+#include "gpr_device.cuh"
 #include "gpr_internal.cuh"
 
 using gpr::PrLayout;
-
-     
 
 namespace {
 
@@ -64,175 +63,7 @@ struct PrArgs {
   int batch;              // units per work-queue grab
 };
 
-constexpr unsigned kFull = 0xffffffffu;
-
-struct Policies {
-  uint64_t stream;  // evict-first: data read or written once per sweep
-  uint64_t keep;    // evict-last: contributions, gathered many times
-};
-
-__device__ __forceinline__ Policies make_policies() {
-  Policies p;
-  asm("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p.stream));
-  asm("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p.keep));
-  return p;
-}
-
-// Edge indices are read exactly once per sweep: no L1 allocation, evict-first
-// in L2 so they do not push the contributions out.
-__device__ __forceinline__ int ld_idx(const int *p, uint64_t pol) {
-  int v;
-  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"
-      : "=r"(v) : "l"(p), "l"(pol));
-  return v;
-}
-
-__device__ __forceinline__ int4 ld_idx4(const int *p, uint64_t pol) {
-  int4 v;
-  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v4.s32 {%0,%1,%2,%3}, [%4], %5;"
-      : "=r"(v.x), "=r"(v.y), "=r"(v.z), "=r"(v.w) : "l"(p), "l"(pol));
-  return v;
-}
-
-// Contribution gather.  A plain (coherent, L1-cached) load: the persistent
-// kernel rewrites these buffers between sweeps, so the non-coherent path
-// must not be used; the grid barrier's fences order the accesses.
-__device__ __forceinline__ float ld_contrib(const float *p, uint64_t pol) {
-  float v;
-  asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
-  return v;
-}
-
-__device__ __forceinline__ float4 ld_contrib4(const float4 *p, uint64_t pol) {
-  float4 v;
-  asm volatile("ld.global.L2::cache_hint.v4.f32 {%0,%1,%2,%3}, [%4], %5;"
-               : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p), "l"(pol));
-  return v;
-}
-
-// Contribution elements are FP32 (plain form) or BF16 (mixed form); the sum
-// is always FP32.
-__device__ __forceinline__ float ld_c(const float *p, uint64_t pol) { return ld_contrib(p, pol); }
-__device__ __forceinline__ float ld_c(const __nv_bfloat16 *p, uint64_t pol) {
-  unsigned short h;
-  asm volatile("ld.global.L2::cache_hint.b16 %0, [%1], %2;" : "=h"(h) : "l"(p), "l"(pol));
-  return __uint_as_float((unsigned)h << 16);
-}
-__device__ __forceinline__ float ld_c_generic(const float *p) {
-  float v;
-  asm volatile("ld.f32 %0, [%1];" : "=f"(v) : "l"(p));
-  return v;
-}
-__device__ __forceinline__ float ld_c_generic(const __nv_bfloat16 *p) {
-  unsigned short h;
-  asm volatile("ld.b16 %0, [%1];" : "=h"(h) : "l"(p));
-  return __uint_as_float((unsigned)h << 16);
-}
-__device__ __forceinline__ float from_c(float v) { return v; }
-__device__ __forceinline__ float from_c(__nv_bfloat16 v) { return __bfloat162float(v); }
-__device__ __forceinline__ void st_c(float *p, float v, uint64_t pol) {
-  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" :: "l"(p), "f"(v), "l"(pol) : "memory");
-}
-__device__ __forceinline__ void st_c(__nv_bfloat16 *p, float v, uint64_t pol) {
-  const unsigned short h = __bfloat16_as_ushort(__float2bfloat16_rn(v));
-  asm volatile("st.global.L2::cache_hint.b16 [%0], %1, %2;" :: "l"(p), "h"(h), "l"(pol) : "memory");
-}
-
-// Contribution sources.  GlobalGather reads the contribution array;
-// HotGather serves indices below `hot` from the copy of the array's prefix
-// in shared memory (the highest in-degree vertices, which a power-law graph
-// gathers most) and the rest with a predicated global load, branch-free.
-template <typename T>
-struct GlobalGather {
-  const T *cin;
-  uint64_t pol;
-  __device__ __forceinline__ float operator()(int idx) const { return ld_c(cin + idx, pol); }
-};
-
-template <typename T>
-struct HotGather {
-  const T *cin;
-  const T *hot;
-  int n_hot;
-  uint64_t pol;
-  __device__ __forceinline__ float operator()(int idx) const {
-    const float h = from_c(hot[min(idx, n_hot - 1)]);
-    const float g = idx >= n_hot ? ld_c(cin + idx, pol) : 0.f;
-    return idx < n_hot ? h : g;
-  }
-};
-
-template <>
-struct HotGather<float> {
-  const float *cin;
-  const float *hot;
-  int n_hot;
-  uint64_t pol;
-  __device__ __forceinline__ float operator()(int idx) const {
-    const float h = hot[min(idx, n_hot - 1)];
-    float g = 0.f;
-    asm volatile(
-        "{\n .reg .pred p;\n setp.ge.s32 p, %1, %2;\n"
-        " @p ld.global.L2::cache_hint.f32 %0, [%3], %4;\n}"
-        : "+f"(g) : "r"(idx), "r"(n_hot), "l"(cin + idx), "l"(pol));
-    return idx < n_hot ? h : g;
-  }
-};
-
-// Same sources through one generic-address load: a lane's pointer falls in
-// shared memory for hot indices and in global memory otherwise, so a gather
-// costs one load instruction instead of two.
-template <typename T>
-struct HotGatherGeneric {
-  const T *cin;
-  const T *hot;
-  int n_hot;
-  uint64_t pol;
-  __device__ __forceinline__ float operator()(int idx) const {
-    return ld_c_generic(idx < n_hot ? hot + idx : cin + idx);
-  }
-};
-
-__device__ __forceinline__ float ld_f32_stream(const float *p, uint64_t pol) {
-  float v;
-  asm volatile("ld.global.L2::cache_hint.f32 %0, [%1], %2;" : "=f"(v) : "l"(p), "l"(pol));
-  return v;
-}
-
-__device__ __forceinline__ int ld_s32_stream(const int *p, uint64_t pol) {
-  int v;
-  asm("ld.global.nc.L1::no_allocate.L2::cache_hint.s32 %0, [%1], %2;"
-      : "=r"(v) : "l"(p), "l"(pol));
-  return v;
-}
-
-__device__ __forceinline__ void st_f32(float *p, float v, uint64_t pol) {
-  asm volatile("st.global.L2::cache_hint.f32 [%0], %1, %2;" :: "l"(p), "f"(v), "l"(pol) : "memory");
-}
-
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-__device__ __forceinline__ long long global_ns() {
-  long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
-
-__device__ __forceinline__ float warp_sum(float v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-  return v;
-}
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(kFull, v, o);
-  return v;
-}
+using namespace gpr::dev;
 
 // Score update of row r from its pulled sum and its prefetched old score and
 // out-degree; returns |s_new - s_old|.

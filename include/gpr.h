@@ -156,6 +156,40 @@ int gpr_page_rank(int m, int nnz, const int *row_offsets,
 int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
             const gpr_pr_opts *opts, int *h_iters, gpr_pr_stats *stats);
 
+/* ---- uneven multi-graph batch ------------------------------------------------
+ * No counterpart in the reference (each reference run solves one graph read
+ * from one file, src/pr/main.cc:14-34).  A batch of independent graphs stored
+ * as one block-diagonal pull graph: graph g owns vertices
+ * [h_voff[g], h_voff[g+1]) (h_voff: n_graphs + 1 host ints, h_voff[0] = 0),
+ * and every in-edge of its rows comes from that range (global vertex ids;
+ * GPR_EINVAL otherwise).  rowptr / col / outdeg are the usual in-CSR and
+ * out-degrees over all h_voff[n_graphs] vertices.  h_lopts (n_graphs entries,
+ * or NULL for the defaults) gives each graph its own bins: sell_max, chunk,
+ * chunk_min as in gpr_graph_create_ex (hot_entries and flags are ignored).
+ *
+ * gpr_multigraph_pagerank solves every graph as gpr_pagerank would solve it
+ * alone -- base (1 - kDamp) / m_g, its own L1 residual, stop after its first
+ * sweep with residual < tol or after max_iter sweeps -- all graphs in one
+ * persistent launch.  any_scores: all vertices, initialised by the caller
+ * (the reference uses 1/m_g, src/pr/main.cc:27-28), updated in place.
+ * h_iters / h_residuals (n_graphs entries each, may be NULL) receive each
+ * graph's sweeps and last residual.  precision GPR_PREC_FP32, or
+ * GPR_PREC_BF16 (BF16 contributions to max(tol, 1e-3), then FP32 sweeps to
+ * tol); stats->iterations is the launch's sweep count (the largest graph
+ * count per phase). */
+typedef struct gpr_multigraph gpr_multigraph;
+int gpr_multigraph_create(int n_graphs, const int *h_voff, long long nnz,
+                          const int *any_rowptr, const int *any_col,
+                          const int *any_outdeg, const gpr_layout_opts *h_lopts,
+                          gpr_multigraph **out);
+int gpr_multigraph_destroy(gpr_multigraph *mg);
+int gpr_multigraph_info(const gpr_multigraph *mg, int *n_graphs, int *m,
+                        long long *nnz, int *n_units, long long *edge_slots);
+int gpr_multigraph_set_stream(gpr_multigraph *mg, void *stream);
+int gpr_multigraph_pagerank(gpr_multigraph *mg, float *any_scores,
+                            const gpr_pr_opts *opts, int *h_iters,
+                            double *h_residuals, gpr_pr_stats *stats);
+
 /* ---- PageRank without any allocation ----------------------------------------
  * No counterpart in the reference.  For callers that cannot let a library
  * allocate device memory (their allocator owns the device heap, or the call
@@ -196,6 +230,17 @@ int gpr_spmv_solver(int m, int nnz, const int *Ap, const int *Aj,
 int gpr_gen_rmat(int scale, int edge_factor, double a, double b, double c,
                  unsigned long long seed, int scramble, int **d_rowptr,
                  int **d_col, int **d_outdeg, long long *nnz);
+/* Seeded uneven batch of n_graphs graphs as one block-diagonal pull graph:
+ * graph g owns vertices [h_voff[g], h_voff[g+1]) (h_voff: n_graphs + 1 ints,
+ * filled by the call), with m_g log-uniform in [m_min, m_max]; odd g are
+ * Chung-Lu power-law graphs (cl_deg edge draws per vertex, degree exponent
+ * gamma), even g Erdos-Renyi graphs (er_deg draws per vertex); self-loops and
+ * duplicate edges dropped, global vertex ids, columns ascending.  The draws
+ * are a pure function of (seed, g, edge index), restated in the oracle. */
+int gpr_gen_multigraph(int n_graphs, int m_min, int m_max, int er_deg,
+                       int cl_deg, double gamma, unsigned long long seed,
+                       int *h_voff, int **d_rowptr, int **d_col,
+                       int **d_outdeg, long long *nnz);
 /* 27-point Laplacian on an n^3 grid (26 / -1), natural ordering. */
 int gpr_gen_stencil27(int n, int **d_Ap, int **d_Aj, float **d_Ax,
                       long long *nnz);

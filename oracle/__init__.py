@@ -81,6 +81,13 @@ def lib():
         L.orc_uniform_int.restype = None
         L.orc_uniform_int.argtypes = [C.c_longlong, C.c_ulonglong, C.c_int, _i32p]
         L.orc_num_threads.restype = C.c_int
+        L.orc_multigraph_size.restype = C.c_int
+        L.orc_multigraph_size.argtypes = [C.c_int, C.c_int, C.c_int, C.c_ulonglong]
+        L.orc_chung_lu_prefix.restype = None
+        L.orc_chung_lu_prefix.argtypes = [C.c_int, C.c_double, _f64p]
+        L.orc_multigraph_edges.restype = None
+        L.orc_multigraph_edges.argtypes = [C.c_int, C.c_int, C.c_int, C.c_ulonglong, _f64p,
+                                           _i32p, _i32p]
         _LIB = L
     return _LIB
 
@@ -189,6 +196,37 @@ def rmat_graph(scale, edge_factor=16, seed=1, abc=RMAT_ABC, scramble=True):
     duplicates removed, columns ascending within each row."""
     src, dst = rmat_edges(scale, edge_factor, seed, abc, scramble)
     return in_csr_from_edges(1 << scale, src, dst)
+
+
+MULTI_ER_DEG, MULTI_CL_DEG, MULTI_GAMMA = 8, 16, 2.1
+
+
+def multigraph(n_graphs, m_min=1000, m_max=500000, seed=1, er_deg=MULTI_ER_DEG,
+               cl_deg=MULTI_CL_DEG, gamma=MULTI_GAMMA):
+    """Seeded uneven batch of graphs as one block-diagonal pull graph
+    (oracle.c orc_multigraph_*): graph g owns vertices [voff[g], voff[g+1]),
+    odd g Chung-Lu power law (cl_deg draws per vertex, exponent gamma), even
+    g Erdos-Renyi (er_deg draws per vertex).  Returns
+    (in_rowptr, in_col, outdeg, voff) with global vertex ids."""
+    L = lib()
+    sizes = [int(L.orc_multigraph_size(g, m_min, m_max, seed)) for g in range(n_graphs)]
+    voff = np.zeros(n_graphs + 1, dtype=np.int64)
+    np.cumsum(sizes, out=voff[1:])
+    P = np.empty(max(sizes) if sizes else 1, dtype=np.float64)
+    L.orc_chung_lu_prefix(len(P), float(gamma), P)
+    srcs, dsts = [], []
+    for g, mg in enumerate(sizes):
+        deg = cl_deg if g & 1 else er_deg
+        s = np.empty(mg * deg, dtype=np.int32)
+        d = np.empty(mg * deg, dtype=np.int32)
+        L.orc_multigraph_edges(g, mg, deg, seed, P, s, d)
+        srcs.append(s + np.int32(voff[g]))
+        dsts.append(d + np.int32(voff[g]))
+    M = int(voff[-1])
+    src = np.concatenate(srcs) if srcs else np.zeros(0, np.int32)
+    dst = np.concatenate(dsts) if dsts else np.zeros(0, np.int32)
+    rp, col, od = in_csr_from_edges(M, src, dst)
+    return rp, col, od, voff.astype(np.int32)
 
 
 def stencil27(n):

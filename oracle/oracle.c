@@ -461,3 +461,80 @@ int orc_num_threads(void)
     return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------------ */
+/* Uneven multi-graph batch (a batch of independent graphs solved together; */
+/* the reference has no counterpart -- each of its runs reads one file).    */
+/*                                                                          */
+/* Graph g of a batch with seed S:                                          */
+/*   size   m_g = floor(exp(ln m_min + u (ln m_max - ln m_min))), clamped,  */
+/*          u = top 53 bits of hash3(S, g, 0x6d67) / 2^53 (log-uniform)     */
+/*   type   g odd: Chung-Lu power law, g even: Erdos-Renyi                  */
+/*   edges  m_g * deg raw draws e = 0.. with h = hash3(G_g, e, 0),          */
+/*          G_g = hash3(S, g, 0x9e37):                                      */
+/*     Erdos-Renyi: src = (h >> 32) * m_g >> 32, dst = (h & 0xffffffff) *   */
+/*                  m_g >> 32 (both uniform in [0, m_g))                    */
+/*     Chung-Lu:    src = first i with P[i] > x * P[m_g - 1], x = top 53    */
+/*                  bits of h / 2^53; dst the same with hash3(G_g, e, 1);   */
+/*                  P[i] = sum_{j <= i} (j + 1)^(-1 / (gamma - 1)), summed  */
+/*                  in double in index order (weights of a power-law degree */
+/*                  sequence with exponent gamma, Chung & Lu 2002)          */
+/*   then self-loops and duplicate edges are dropped (orc_build_in_csr).    */
+/* The batch is one block-diagonal graph: graph g owns vertices             */
+/* [voff[g], voff[g+1]), in the order g = 0, 1, ...                         */
+/* ------------------------------------------------------------------------ */
+int orc_multigraph_size(int g, int m_min, int m_max, unsigned long long seed)
+{
+    const uint64_t h = orc_hash3(seed, (uint64_t)g, 0x6d67u);
+    const double u = (double)(h >> 11) * 0x1.0p-53;
+    const double lo = log((double)m_min), hi = log((double)m_max);
+    const double t = u * (hi - lo);
+    int m = (int)floor(exp(lo + t));
+    if (m < m_min) m = m_min;
+    if (m > m_max) m = m_max;
+    return m;
+}
+
+void orc_chung_lu_prefix(int n, double gamma, double *P)
+{
+    const double alpha = -1.0 / (gamma - 1.0);
+    double acc = 0.0;
+    int i;
+    for (i = 0; i < n; i++) {
+        acc += pow((double)(i + 1), alpha);
+        P[i] = acc;
+    }
+}
+
+static inline int orc_cl_draw(uint64_t h, const double *P, int m)
+{
+    const double x = (double)(h >> 11) * 0x1.0p-53;
+    const double y = x * P[m - 1];
+    int lo = 0, hi = m;  /* first i in [0, m) with P[i] > y */
+    while (lo < hi) {
+        const int mid = lo + (hi - lo) / 2;
+        if (P[mid] > y) hi = mid;
+        else lo = mid + 1;
+    }
+    return lo < m ? lo : m - 1;
+}
+
+/* Raw edge draws of graph g (local vertex ids), m_g * deg of them. */
+void orc_multigraph_edges(int g, int m_g, int deg, unsigned long long seed,
+                          const double *P, int *src, int *dst)
+{
+    const uint64_t gs = orc_hash3(seed, (uint64_t)g, 0x9e37u);
+    const long long ne = (long long)m_g * deg;
+    long long e;
+#pragma omp parallel for schedule(static)
+    for (e = 0; e < ne; e++) {
+        const uint64_t h = orc_hash3(gs, (uint64_t)e, 0);
+        if (g & 1) {
+            src[e] = orc_cl_draw(h, P, m_g);
+            dst[e] = orc_cl_draw(orc_hash3(gs, (uint64_t)e, 1), P, m_g);
+        } else {
+            src[e] = (int)(((h >> 32) * (uint64_t)m_g) >> 32);
+            dst[e] = (int)(((h & 0xffffffffULL) * (uint64_t)m_g) >> 32);
+        }
+    }
+}

@@ -132,3 +132,34 @@ def test_live_reference_on_fresh_graphs(O):
         y0 = np.zeros(3000, np.float32)
         assert np.array_equal(O.spmv_f32(rp, col, vals, x, y0),
                               O.ref_spmv_solver(rp, col, vals, x, y0)[0])
+
+
+def test_multigraph_generator_properties(O):
+    rp, col, od, voff = O.multigraph(16, 1000, 50000, seed=1)
+    sizes = np.diff(voff)
+    assert sizes.min() >= 1000 and sizes.max() <= 50000
+    m = len(rp) - 1
+    assert voff[-1] == m and np.array_equal(od, np.bincount(col, minlength=m))
+    for g in range(16):
+        a, b = voff[g], voff[g + 1]
+        c = col[rp[a]:rp[b]]
+        assert c.min() >= a and c.max() < b  # block-diagonal
+        deg = np.diff(rp[a:b + 1])
+        avg = (rp[b] - rp[a]) / (b - a)
+        if g % 2 == 0:  # Erdos-Renyi, 8 draws per vertex, few collisions
+            assert 7.5 < avg <= 8.0 and deg.max() < 40
+        else:           # Chung-Lu power law, 16 draws per vertex
+            assert avg < 16.0 and deg.max() > 30 * avg
+    for g in range(m and 16):
+        r = rp[voff[g]:voff[g + 1] + 1]
+        for v in range(0, len(r) - 1, 97):  # columns ascending, no self-loops
+            cc = col[r[v]:r[v + 1]]
+            assert np.all(np.diff(cc) > 0) and not np.any(cc == voff[g] + v)
+
+
+def test_multigraph_sizes_log_uniform(O):
+    L = O.lib()
+    sizes = np.array([L.orc_multigraph_size(g, 1000, 500000, 7) for g in range(4000)])
+    assert sizes.min() >= 1000 and sizes.max() <= 500000
+    frac = np.mean(np.log(sizes) < 0.5 * (np.log(1000) + np.log(500000)))
+    assert abs(frac - 0.5) < 0.03
