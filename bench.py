@@ -219,13 +219,25 @@ def run_ours(args):
     t0 = time.time()
     csr = G.gen_rmat(args.scale, EDGE_FACTOR, seed=SEED, abc=ABC)
     m, nnz = csr.m, csr.nnz
-    g = G.Graph(csr.rowptr, csr.col, csr.third, m=m, nnz=nnz, batched=not args.no_forms)
+    # The project autotuner picks the bins, hot prefix and kernel variant for
+    # this degree distribution (timed on the graph, outside the timed region).
+    tuned = None
+    layout = {}
+    variant = 0
+    if not args.no_tune:
+        tuned = G.tune_graph(csr.rowptr, csr.col, csr.third, m=m, nnz=nnz, cache=args.tune_cache,
+                             sweeps=5)
+        layout = {k: tuned[k] for k in ("sell_max", "chunk", "chunk_min", "hot_entries")}
+        variant = tuned["variant"]
+        log(f"[ours] tuned: {tuned}")
+    g = G.Graph(csr.rowptr, csr.col, csr.third, m=m, nnz=nnz, batched=not args.no_forms,
+                **layout)
     g.set_stream(stream.cuda_stream)
     log(f"[ours] rank {rank}: graph s{args.scale} m={m} nnz={nnz} layout={g.layout()} "
         f"ready in {time.time() - t0:.2f}s")
     scores = torch.empty(m, dtype=torch.float32, device=dev)
     init = float(np.float32(1.0) / np.float32(m))
-    opts = G.options(tol=TOL, max_iter=MAX_ITER, damping=DAMPING)
+    opts = G.options(tol=TOL, max_iter=MAX_ITER, damping=DAMPING, variant=variant)
 
     def step():
         scores.fill_(init)
@@ -286,7 +298,8 @@ def run_ours(args):
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded RMAT generated on the GPU)",
             "config": workload_config(args.scale, m, nnz), "roofline": roof,
-            "gpu_launches": launches, "clocks": clocks, "accuracy": accuracy}
+            "gpu_launches": launches, "clocks": clocks, "accuracy": accuracy,
+            "tuning": tuned}
 
     # End to end through the reference-shaped C-ABI call with host buffers:
     # PageRank(m, nnz, row_offsets, column_indices, degree, scores) copies the
@@ -411,7 +424,12 @@ def multigraph_leg(G, torch, dev, stream, plain_gteps, args):
     sweeps_g."""
     t0 = time.time()
     A, voff = G.gen_multigraph(MG_GRAPHS, MG_MMIN, MG_MMAX, seed=MG_SEED)
-    mg = G.MultiGraph(A.rowptr, A.col, A.third, voff, nnz=A.nnz)
+    layouts, tuned = None, None
+    if not args.no_tune:
+        layouts, tuned = G.tune_multigraph(A.rowptr, A.col, A.third, voff, nnz=A.nnz,
+                                           cache=args.tune_cache, sweeps=5)
+        log(f"[ours] multigraph tuned: {tuned}")
+    mg = G.MultiGraph(A.rowptr, A.col, A.third, voff, nnz=A.nnz, layouts=layouts)
     mg.set_stream(stream.cuda_stream)
     info = mg.info()
     rp = A.rowptr.to_numpy()
@@ -423,7 +441,10 @@ def multigraph_leg(G, torch, dev, stream, plain_gteps, args):
     peak, peak_kind = load_peaks()
     out = {"workload": f"multigraph_{MG_GRAPHS}_m{MG_MMIN}-{MG_MMAX}_tol1e-6",
            "graphs": MG_GRAPHS, "m": A.m, "nnz": A.nnz, "units": info["units"],
-           "edge_slots": info["edge_slots"], "tol": TOL, "max_iter": MG_MAX_ITER}
+           "edge_slots": info["edge_slots"], "tol": TOL, "max_iter": MG_MAX_ITER,
+           "tuning": tuned,
+           "bins": sorted({(d["sell_max"], d["chunk_min"], d["chunk"]) for d in layouts})
+           if layouts else "defaults"}
     for prec, name in ((G.PREC_FP32, "fp32"), (G.PREC_BF16, "bf16_refined")):
         best = None
         for _ in range(3):
@@ -494,6 +515,23 @@ def profile_solve(args):
     return 0
 
 
+def profile_multigraph(args):
+    """One FP32 solve of exactly --profile-solve sweeps (tol 0) on the first
+    --profile-multigraph graphs of the multi-graph batch (for ncu)."""
+    import torch
+
+    import gardenia_ocl_b200 as G
+    A, voff = G.gen_multigraph(args.profile_multigraph, MG_MMIN, MG_MMAX, seed=MG_SEED)
+    mg = G.MultiGraph(A.rowptr, A.col, A.third, voff, nnz=A.nnz)
+    scores = torch.from_numpy(mg.initial_scores()).cuda()
+    _, it, _, st = mg.pagerank(scores, tol=0.0, max_iter=args.profile_solve or 10,
+                               damping=DAMPING)
+    log(json.dumps({"info": mg.info(), **st.as_dict()}))
+    mg.close()
+    A.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -506,12 +544,20 @@ def main():
     ap.add_argument("--no-forms", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-multigraph", action="store_true")
+    ap.add_argument("--no-tune", action="store_true", help="default bins and kernel variant")
+    ap.add_argument("--tune-cache", default=None, metavar="PATH",
+                    help="autotuner cache file (default: none, tune on every run)")
     ap.add_argument("--profile-solve", type=int, default=0, metavar="SWEEPS",
                     help="build the graph and run one solve of exactly SWEEPS sweeps, "
                          "nothing else (the case profiled with ncu)")
     ap.add_argument("--profile-loop", choices=["persistent", "graph"], default="persistent",
                     help="sweep loop of --profile-solve")
+    ap.add_argument("--profile-multigraph", type=int, default=0, metavar="GRAPHS",
+                    help="build the first GRAPHS graphs of the multi-graph batch and run one "
+                         "solve of --profile-solve sweeps (the case profiled with ncu)")
     args = ap.parse_args()
+    if args.profile_multigraph:
+        return profile_multigraph(args)
     if args.profile_solve:
         return profile_solve(args)
     if args.warmup < 3:

@@ -57,6 +57,21 @@ class PrStats(C.Structure):
                 "gpu_launches": self.gpu_launches}
 
 
+class TuneResult(C.Structure):
+    _fields_ = [("layout", LayoutOptions), ("variant", C.c_int), ("from_cache", C.c_int),
+                ("candidates", C.c_int), ("ms_per_sweep", C.c_double),
+                ("default_ms_per_sweep", C.c_double), ("signature", C.c_char * 48)]
+
+    def as_dict(self):
+        lo = self.layout
+        return {"sell_max": lo.sell_max, "chunk": lo.chunk, "chunk_min": lo.chunk_min,
+                "hot_entries": lo.hot_entries, "variant": self.variant,
+                "from_cache": bool(self.from_cache), "candidates": self.candidates,
+                "ms_per_sweep": self.ms_per_sweep,
+                "default_ms_per_sweep": self.default_ms_per_sweep,
+                "signature": self.signature.decode()}
+
+
 _LIB = None
 _vp = C.c_void_p
 
@@ -115,6 +130,8 @@ def lib():
                                         C.POINTER(PrStats)]),
         "gpr_gen_uniform": (I, [LL, C.c_ulonglong, _vp]),
         "gpr_free": (I, [_vp]),
+        "gpr_release_cached": (I, [C.POINTER(LL)]),
+        "gpr_cached_bytes": (I, [C.POINTER(LL)]),
         "gpr_malloc": (I, [C.POINTER(_vp), C.c_size_t]),
         "gpr_memcpy": (I, [_vp, _vp, C.c_size_t]),
         "gpr_synchronize": (I, []),
@@ -122,6 +139,11 @@ def lib():
         "gpr_read_graph": (I, [C.c_char_p, I, I, I, I, I, C.POINTER(I), C.POINTER(I),
                                C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
         "gpr_read_graph_free": (None, [_vp]),
+        "gpr_tune_graph": (I, [I, LL, _vp, _vp, _vp, C.c_char_p, I, C.POINTER(TuneResult)]),
+        "gpr_tune_multigraph": (I, [I, _vp, LL, _vp, _vp, _vp, C.c_char_p, I,
+                                    C.POINTER(LayoutOptions), C.POINTER(TuneResult)]),
+        "gpr_tune_signature": (I, [I, LL, _vp, I, C.c_char_p, I]),
+        "gpr_tune_cache_lookup": (I, [C.c_char_p, C.c_char_p, C.POINTER(TuneResult)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -549,8 +571,72 @@ def gen_uniform(n, seed, d_out) -> None:
     _check(lib().gpr_gen_uniform(int(n), int(seed), _ptr(d_out)[0]))
 
 
+# ---------------------------------------------------------------------------
+# Autotuner
+# ---------------------------------------------------------------------------
+def tune_graph(rowptr, col, outdeg, m=None, nnz=None, cache=None, sweeps=5) -> dict:
+    """Layout bins, hot prefix and kernel variant for this graph's in-degree
+    distribution (gpr_tune_graph).  Pass the result to ``Graph(**layout)`` and
+    ``pagerank(variant=...)``; ``cache``: path of the text cache (or None)."""
+    m = int(len(rowptr) - 1) if m is None else int(m)
+    nnz = int(len(col)) if nnz is None else int(nnz)
+    pr, k0 = _ptr(rowptr, np.int32)
+    pc, k1 = _ptr(col, np.int32)
+    pd, k2 = _ptr(outdeg, np.int32)
+    r = TuneResult()
+    _check(lib().gpr_tune_graph(m, nnz, pr, pc, pd, os.fsencode(cache) if cache else None,
+                                int(sweeps), C.byref(r)))
+    return r.as_dict()
+
+
+def tune_multigraph(rowptr, col, outdeg, voff, nnz=None, cache=None, sweeps=5):
+    """Per-graph bins for a batch (gpr_tune_multigraph): returns (layouts, summary),
+    ``layouts`` ready for ``MultiGraph(..., layouts=layouts)``."""
+    voff = np.ascontiguousarray(voff, dtype=np.int32)
+    n = len(voff) - 1
+    nnz = int(len(col)) if nnz is None else int(nnz)
+    pr, k0 = _ptr(rowptr, np.int32)
+    pc, k1 = _ptr(col, np.int32)
+    pd, k2 = _ptr(outdeg, np.int32)
+    lo = (LayoutOptions * n)()
+    r = TuneResult()
+    _check(lib().gpr_tune_multigraph(n, C.c_void_p(voff.ctypes.data), nnz, pr, pc, pd,
+                                     os.fsencode(cache) if cache else None, int(sweeps), lo,
+                                     C.byref(r)))
+    layouts = [{"sell_max": x.sell_max, "chunk": x.chunk, "chunk_min": x.chunk_min} for x in lo]
+    return layouts, r.as_dict()
+
+
+def tune_signature(rowptr, batch=False) -> str:
+    """Distribution signature (the cache key) of a host row-offset array."""
+    rp = np.ascontiguousarray(rowptr, dtype=np.int32)
+    buf = C.create_string_buffer(64)
+    _check(lib().gpr_tune_signature(len(rp) - 1, int(rp[-1] - rp[0]) if len(rp) else 0,
+                                    C.c_void_p(rp.ctypes.data), 1 if batch else 0, buf, 64))
+    return buf.value.decode()
+
+
+def tune_cache_lookup(cache, signature):
+    r = TuneResult()
+    st = lib().gpr_tune_cache_lookup(os.fsencode(cache), signature.encode(), C.byref(r))
+    return r.as_dict() if st == GPR_OK else None
+
+
 def set_device(device: int):
     _check(lib().gpr_set_device(int(device)))
+
+
+def release_cached() -> int:
+    """Return the library's cached device blocks to the driver; returns bytes."""
+    n = C.c_longlong()
+    _check(lib().gpr_release_cached(C.byref(n)))
+    return n.value
+
+
+def cached_bytes() -> int:
+    n = C.c_longlong()
+    _check(lib().gpr_cached_bytes(C.byref(n)))
+    return n.value
 
 
 def synchronize():

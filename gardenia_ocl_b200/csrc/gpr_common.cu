@@ -2,6 +2,10 @@
 #include <stdarg.h>
 #include <string.h>
 
+#include <mutex>
+#include <unordered_map>
+#include <vector>
+
 #include "gpr_internal.cuh"
 
 namespace gpr {
@@ -15,23 +19,134 @@ void set_error(const char *fmt, ...) {
   va_end(ap);
 }
 
+// Block cache of large device allocations.  One-shot solver calls (the
+// reference's PRSolver shape: copy in, build, solve, free) allocate and free
+// gigabytes per call; mapping and unmapping that much memory makes cudaMalloc
+// / cudaFree slow and erratic.  Blocks of at least kCacheMin bytes are kept
+// after dfree (which first synchronises the device, as cudaFree does, so no
+// kernel still uses the block) and handed out again to requests that fit
+// them within 1/8.  At most kCacheCap bytes stay cached; an allocation that
+// fails releases the cache and retries; gpr_release_cached() empties it.
+namespace {
+
+constexpr size_t kCacheMin = size_t(1) << 20;
+constexpr size_t kCacheCap = size_t(24) << 30;
+
+struct Block {
+  void *p;
+  size_t bytes;
+  int device;
+};
+
+std::mutex g_mu;
+std::unordered_map<void *, Block> g_live;  // cached-class blocks handed out
+std::vector<Block> g_free;                // cached, unused
+size_t g_free_bytes = 0;
+
+void release_free_locked(int device) {
+  for (size_t i = 0; i < g_free.size();) {
+    if (device < 0 || g_free[i].device == device) {
+      int cur = -1;
+      cudaGetDevice(&cur);
+      if (cur != g_free[i].device) cudaSetDevice(g_free[i].device);
+      cudaFree(g_free[i].p);
+      if (cur >= 0 && cur != g_free[i].device) cudaSetDevice(cur);
+      g_free_bytes -= g_free[i].bytes;
+      g_free[i] = g_free.back();
+      g_free.pop_back();
+    } else {
+      ++i;
+    }
+  }
+}
+
+}  // namespace
+
 int dmalloc(void **p, size_t bytes, const char *what) {
   *p = nullptr;
+  int dev = 0;
+  cudaGetDevice(&dev);
+  if (bytes >= kCacheMin) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    int best = -1;
+    for (size_t i = 0; i < g_free.size(); ++i) {
+      const Block &b = g_free[i];
+      if (b.device == dev && b.bytes >= bytes && b.bytes - bytes <= bytes / 8 &&
+          (best < 0 || b.bytes < g_free[best].bytes))
+        best = (int)i;
+    }
+    if (best >= 0) {
+      Block b = g_free[best];
+      g_free[best] = g_free.back();
+      g_free.pop_back();
+      g_free_bytes -= b.bytes;
+      g_live[b.p] = b;
+      *p = b.p;
+      return GPR_OK;
+    }
+  }
   cudaError_t e = cudaMalloc(p, bytes);
   if (e == cudaErrorMemoryAllocation) {
     cudaGetLastError();
+    {
+      std::lock_guard<std::mutex> lk(g_mu);
+      release_free_locked(dev);
+    }
+    e = cudaMalloc(p, bytes);
+  }
+  if (e == cudaErrorMemoryAllocation) {
+    cudaGetLastError();
+    *p = nullptr;
     set_error("cudaMalloc(%zu bytes) for %s: out of device memory", bytes, what);
     return GPR_ENOMEM;
   }
   if (e != cudaSuccess) {
+    *p = nullptr;
     set_error("cudaMalloc(%zu bytes) for %s: %s", bytes, what, cudaGetErrorString(e));
     return GPR_ECUDA;
+  }
+  if (bytes >= kCacheMin) {
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_live[*p] = Block{*p, bytes, dev};
   }
   return GPR_OK;
 }
 
 void dfree(void *p) {
-  if (p) cudaFree(p);
+  if (!p) return;
+  std::unique_lock<std::mutex> lk(g_mu);
+  auto it = g_live.find(p);
+  if (it == g_live.end()) {
+    lk.unlock();
+    cudaFree(p);
+    return;
+  }
+  Block b = it->second;
+  g_live.erase(it);
+  int cur = -1;
+  cudaGetDevice(&cur);
+  if (cur != b.device) cudaSetDevice(b.device);
+  cudaDeviceSynchronize();  // what cudaFree would wait for
+  if (cur >= 0 && cur != b.device) cudaSetDevice(cur);
+  g_free.push_back(b);
+  g_free_bytes += b.bytes;
+  while (g_free_bytes > kCacheCap && !g_free.empty()) {
+    size_t big = 0;
+    for (size_t i = 1; i < g_free.size(); ++i)
+      if (g_free[i].bytes > g_free[big].bytes) big = i;
+    Block v = g_free[big];
+    g_free[big] = g_free.back();
+    g_free.pop_back();
+    g_free_bytes -= v.bytes;
+    if (cur != v.device) cudaSetDevice(v.device);
+    cudaFree(v.p);
+    if (cur >= 0 && cur != v.device) cudaSetDevice(cur);
+  }
+}
+
+size_t cached_bytes() {
+  std::lock_guard<std::mutex> lk(g_mu);
+  return g_free_bytes;
 }
 
 bool is_device_ptr(const void *p) {
@@ -56,7 +171,7 @@ int to_device(const void *any, size_t bytes, void **dev, bool *owned,
     cudaError_t e = cudaMemcpyAsync(*dev, any, bytes, cudaMemcpyHostToDevice, st);
     if (e != cudaSuccess) {
       set_error("copy of %s to the device: %s", what, cudaGetErrorString(e));
-      cudaFree(*dev);
+      dfree(*dev);
       *dev = nullptr;
       *owned = false;
       return GPR_ECUDA;
@@ -90,7 +205,27 @@ int gpr_pr_opts_default(gpr_pr_opts *o) {
 }
 
 int gpr_free(void *d_ptr) {
-  if (d_ptr) GPR_CUDA(cudaFree(d_ptr));
+  gpr::dfree(d_ptr);
+  GPR_CUDA(cudaGetLastError());
+  return GPR_OK;
+}
+
+int gpr_release_cached(long long *released_bytes) {
+  {
+    std::lock_guard<std::mutex> lk(gpr::g_mu);
+    if (released_bytes) *released_bytes = (long long)gpr::g_free_bytes;
+    gpr::release_free_locked(-1);
+  }
+  GPR_CUDA(cudaGetLastError());
+  return GPR_OK;
+}
+
+int gpr_cached_bytes(long long *bytes) {
+  if (!bytes) {
+    gpr::set_error("gpr_cached_bytes: NULL out");
+    return GPR_EINVAL;
+  }
+  *bytes = (long long)gpr::cached_bytes();
   return GPR_OK;
 }
 

@@ -174,7 +174,7 @@ int csr_from_keys(long long ne, int m, uint64_t *k0, uint64_t *k1, int **d_rowpt
     cudaMemsetAsync(rowptr, 0, sizeof(int) * ((size_t)m + 1), st);
     cudaMemsetAsync(outdeg, 0, sizeof(int) * (size_t)m, st);
     k_split_keys<<<capped_grid(nnz), 256, 0, st>>>(nnz, uniq, col, rowptr, outdeg);
-    cudaFree(tmp);
+    gpr::dfree(tmp);
     tmp = nullptr;
     size_t ts = 0;
     cub::DeviceScan::ExclusiveSum(nullptr, ts, rowptr, rowptr, m + 1, st);

@@ -177,6 +177,12 @@ struct gpr_graph {
   // b_chunk-edge chunks), built on first use for a given (b_dmax, b_chunk).
   int *b_cbeg = nullptr, *b_crow = nullptr;
   int b_nlong = -1, b_nchunks = 0, b_dmax = 0, b_chunk = 0;
+  // Graph mode: the instantiated sweep-loop graph and the kernel and
+  // arguments it was built for.
+  cudaGraph_t loop_graph = nullptr;
+  cudaGraphExec_t loop_exec = nullptr;
+  int loop_ki = -1;
+  alignas(8) unsigned char loop_args[512] = {0};
 };
 
 namespace gpr {

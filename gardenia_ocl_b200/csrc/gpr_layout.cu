@@ -169,7 +169,7 @@ int exclusive_scan(T *d, long long n, cudaStream_t st) {
   void *tmp = nullptr;
   GPR_TRY(dmalloc(&tmp, tmp_bytes, "scan scratch"));
   cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, tmp_bytes, d, d, (int)n, st);
-  cudaFree(tmp);
+  gpr::dfree(tmp);
   if (e != cudaSuccess) {
     set_error("DeviceScan::ExclusiveSum: %s", cudaGetErrorString(e));
     return GPR_ECUDA;
@@ -211,7 +211,7 @@ int validate_csr(int m, long long nnz, int ncols, const int *d_rowptr, const int
   int h = 0;
   cudaError_t e = cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFree(flag);
+  gpr::dfree(flag);
   if (e != cudaSuccess) {
     set_error("CSR validation: %s", cudaGetErrorString(e));
     return GPR_ECUDA;
@@ -258,7 +258,7 @@ int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
     GPR_TRY(dmalloc(&tmp, tb, "sort scratch"));
     cudaError_t e = cub::DeviceRadixSort::SortPairsDescending(tmp, tb, indeg, sdeg, iota,
                                                               L->perm, m, 0, 32, st);
-    cudaFree(tmp);
+    gpr::dfree(tmp);
     if (e != cudaSuccess) {
       set_error("degree sort: %s", cudaGetErrorString(e));
       return GPR_ECUDA;
@@ -486,7 +486,7 @@ int build_spmv_layout(int m, long long nnz, const int *d_Ap, const int *d_Aj,
     void *tmp = nullptr;
     GPR_TRY(dmalloc(&tmp, tb, "select scratch"));
     cudaError_t e = cub::DeviceSelect::Flagged(tmp, tb, it, is_long, L->long_rows, nsel, m, st);
-    cudaFree(tmp);
+    gpr::dfree(tmp);
     if (e != cudaSuccess) {
       set_error("long-row select: %s", cudaGetErrorString(e));
       return GPR_ECUDA;

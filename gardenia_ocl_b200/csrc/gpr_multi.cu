@@ -77,9 +77,11 @@ struct MultiArgs {
   unsigned *bar;          // [2] arrivals, generation
   int *status;            // [0] error flags, [1] sweeps of the launch, [2] done
   int *wq;                // [2] work-queue heads by parity
+  const int *pk;          // [n_pk + 1] first unit of each work packet
+  int n_hpk, n_pk;        // packets of heavy units; all packets (zero units last)
   float damp;
   double tol;
-  int max_iter, batch, bar_expect;
+  int max_iter, bar_expect;
   long long timeout_ns;
 };
 
@@ -198,6 +200,22 @@ __device__ __forceinline__ double m_zero(const MultiArgs &a, T *cout, int4 md, f
   return err;
 }
 
+// Lane's share of sum(v[b..e)): elements b + lane + 32 j, eight independent
+// accumulators so eight loads are in flight, combined in a fixed order
+// (deterministic for a given range).
+__device__ __forceinline__ double range_sum(const double *v, int b, int e, int lane) {
+  double acc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+  int u = b + lane;
+  for (; u + 32 * 7 < e; u += 32 * 8) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) acc[q] += __ldcg(v + u + 32 * q);
+  }
+#pragma unroll
+  for (int q = 0; q < 8; ++q)
+    if (u + 32 * q < e) acc[q] += __ldcg(v + u + 32 * q);
+  return ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
+}
+
 // `done` units of graph g finished by this warp in sweep it.  The warp that
 // completes the graph's last unit sums the graph's unit residuals in unit
 // order and decides whether the graph keeps updating.
@@ -212,10 +230,8 @@ __device__ __forceinline__ void finish_units(const MultiArgs &a, int g, int done
   last = __shfl_sync(kFull, last, 0);
   if (!last) return;
   __threadfence();
-  double t = 0.0;
-  for (int u = a.hb[g] + lane; u < a.hb[g + 1]; u += 32) t += __ldcg(a.uerr + u);
-  if (it < 2)
-    for (int u = a.zb[g] + lane; u < a.zb[g + 1]; u += 32) t += __ldcg(a.uerr + u);
+  double t = range_sum(a.uerr, a.hb[g], a.hb[g + 1], lane);
+  if (it < 2) t += range_sum(a.uerr, a.zb[g], a.zb[g + 1], lane);
   t = warp_sum(t);
   if (lane == 0) {
     a.gres[g] = t;
@@ -281,13 +297,13 @@ __global__ void __launch_bounds__(kMultiBlock, 1) k_multi(MultiArgs a) {
     const T *cin = static_cast<const T *>((it & 1) ? a.c1 : a.c0);
     T *cout = static_cast<T *>((it & 1) ? a.c0 : a.c1);
     const GlobalGather<T> gat{cin, pol.keep};
-    const int n_units = a.n_heavy + (it < 2 ? a.n_zero : 0);
+    const int n_pk = it < 2 ? a.n_pk : a.n_hpk;
     for (;;) {
-      int u0 = 0;
-      if (lane == 0) u0 = atomicAdd(a.wq + (it & 1), a.batch);
-      u0 = __shfl_sync(kFull, u0, 0);
-      if (u0 >= n_units) break;
-      const int u1 = min(u0 + a.batch, n_units);
+      int p = 0;
+      if (lane == 0) p = atomicAdd(a.wq + (it & 1), 1);
+      p = __shfl_sync(kFull, p, 0);
+      if (p >= n_pk) break;
+      const int u0 = __ldg(a.pk + p), u1 = __ldg(a.pk + p + 1);
       int cur = -1, done = 0;
       bool act = false;
       float base = 0.f;
@@ -508,6 +524,8 @@ struct gpr_multigraph {
   int *n_next = nullptr;
   unsigned *bar = nullptr;
   int *status = nullptr, *wq = nullptr;
+  int *pk = nullptr;             // work packets: first unit of each
+  int n_hpk = 0, n_pk = 0;
   float *scores_tmp = nullptr;
   int grid = 0;
   bool coop_ok = false;
@@ -529,7 +547,7 @@ void destroy_multi(gpr_multigraph *g) {
                   g->hb,    g->zb,     g->cap,     g->stop,    g->gdone,  g->lazy,
                   g->gres,  g->s,      g->c0,      g->c1,      g->h0,     g->h1,
                   g->partial, g->cnt,  g->uerr,    g->n_next,  g->bar,    g->status,
-                  g->wq,    g->scores_tmp};
+                  g->wq,    g->scores_tmp, g->pk};
   for (void *p : ptrs) gpr::dfree(p);
   if (g->e0) cudaEventDestroy(g->e0);
   if (g->e1) cudaEventDestroy(g->e1);
@@ -612,7 +630,7 @@ int build_multi(gpr_multigraph *g, const int *h_voff, const int *d_rowptr, const
     GPR_TRY(gpr::dmalloc(&tmp, tb, "sort scratch"));
     cudaError_t e = cub::DeviceRadixSort::SortPairs(tmp, tb, key, key2, iota, g->perm, M, 0,
                                                     32 + gbits, st);
-    cudaFree(tmp);
+    gpr::dfree(tmp);
     if (e != cudaSuccess) {
       gpr::set_error("vertex sort: %s", cudaGetErrorString(e));
       return GPR_ECUDA;
@@ -706,7 +724,7 @@ int build_multi(gpr_multigraph *g, const int *h_voff, const int *d_rowptr, const
     void *tmp = nullptr;
     GPR_TRY(gpr::dmalloc(&tmp, tb, "scan scratch"));
     cudaError_t e = cub::DeviceScan::ExclusiveSum(tmp, tb, g->uoff, g->uoff, U + 1, st);
-    cudaFree(tmp);
+    gpr::dfree(tmp);
     if (e != cudaSuccess) {
       gpr::set_error("unit offsets: %s", cudaGetErrorString(e));
       return GPR_ECUDA;
@@ -715,6 +733,41 @@ int build_multi(gpr_multigraph *g, const int *h_voff, const int *d_rowptr, const
   GPR_CUDA(cudaMemcpyAsync(&g->edge_slots, g->uoff + U, sizeof(long long), cudaMemcpyDeviceToHost, st));
   GPR_CUDA(cudaStreamSynchronize(st));
   GPR_TRY(gpr::dalloc(&g->ecol, (size_t)g->edge_slots, "unit edges"));
+  // Work packets: consecutive units of about equal cost (edge slots plus a
+  // per-unit overhead; zero units by rows), about 8 grabs per warp per
+  // sweep; heavy and zero units never share a packet.
+  {
+    std::vector<long long> uo((size_t)U + 1);
+    GPR_CUDA(cudaMemcpyAsync(uo.data(), g->uoff, sizeof(long long) * uo.size(),
+                             cudaMemcpyDeviceToHost, st));
+    GPR_CUDA(cudaStreamSynchronize(st));
+    auto cost = [&](int u) -> long long {
+      const int kind = (meta[u].w >> 4) & 15;
+      return kind == kUnitZero ? 4LL * meta[u].z : (uo[u + 1] - uo[u]) + 64;
+    };
+    long long total = 0;
+    for (int u = 0; u < g->n_heavy; ++u) total += cost(u);
+    int sms = 0;
+    GPR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
+    const long long target = std::max<long long>(256, total / ((long long)sms * (kMultiBlock / 32) * 8));
+    std::vector<int> pk;
+    auto cut = [&](int b, int e) {
+      long long c = 0;
+      for (int u = b; u < e; ++u) {
+        if (c == 0) pk.push_back(u);
+        c += cost(u);
+        if (c >= target) c = 0;
+      }
+    };
+    cut(0, g->n_heavy);
+    g->n_hpk = (int)pk.size();
+    cut(g->n_heavy, U);
+    g->n_pk = (int)pk.size();
+    pk.push_back(U);
+    GPR_TRY(gpr::dalloc(&g->pk, pk.size(), "work packets"));
+    GPR_CUDA(cudaMemcpyAsync(g->pk, pk.data(), sizeof(int) * pk.size(), cudaMemcpyHostToDevice, st));
+    GPR_CUDA(cudaStreamSynchronize(st));
+  }
   if (U > 0)
     k_fill_units<<<capped(32LL * U), 256, 0, st>>>(U, M, g->meta, g->uoff, dchunk, g->perm, inv,
                                                    sdeg, d_rowptr, d_col, g->ecol);
@@ -819,7 +872,9 @@ int solve_phase(gpr_multigraph *g, float *d_scores, const gpr_pr_opts &o, bool b
   a.tol = o.tol;
   a.max_iter = max_cap;
   a.bar_expect = g->grid + (o.reserved[0] > 0 ? o.reserved[0] : 0);
-  a.batch = (int)std::max<long long>(1, (long long)g->n_heavy / ((long long)g->grid * (kMultiBlock / 32) * 4));
+  a.pk = g->pk;
+  a.n_hpk = g->n_hpk;
+  a.n_pk = g->n_pk;
   a.timeout_ns = (long long)(o.timeout_s * 1e9);
   int launches = 0;
   GPR_CUDA(cudaEventRecord(g->e0, st));
@@ -1023,9 +1078,9 @@ int gpr_multigraph_create(int n_graphs, const int *h_voff, long long nnz, const 
       rc = build_multi(g, h_voff, (const int *)rp, (const int *)cp, (const int *)dp, h_lopts);
     cudaStreamSynchronize(g->st);
   } while (0);
-  if (orp) cudaFree(rp);
-  if (ocp) cudaFree(cp);
-  if (odp) cudaFree(dp);
+  if (orp) gpr::dfree(rp);
+  if (ocp) gpr::dfree(cp);
+  if (odp) gpr::dfree(dp);
   if (rc != GPR_OK) {
     destroy_multi(g);
     return rc;

@@ -61,6 +61,7 @@ struct PrArgs {
   int hot;                // contributions [0, hot) are staged in shared memory
   int *wq;                // [2] work-queue heads of the hot kernel, by sweep parity
   int batch;              // units per work-queue grab
+  unsigned long long cond;  // graph mode: while-node condition handle (0: none)
 };
 
 using namespace gpr::dev;
@@ -328,12 +329,21 @@ __global__ void __launch_bounds__(1024, MINB) k_pr_hot(PrArgs a) {
 // One sweep per launch (graph mode).  The sweep index and the done flag live
 // in device memory, so a captured sequence of launches needs no host input;
 // launches after convergence return at once.
+// In graph mode the launch is the body of a CUDA-graph while node whose
+// condition starts at 1 and is only ever cleared: by the CTA that closes the
+// sweep when the solve is done, by a launch that finds the solve done, and by
+// CTA 0 of the max_iter-th launch (status[3] counts launches), so the loop
+// ends within max_iter launches whatever the sweeps compute.
 template <int U, int U4, typename T>
 __global__ void __launch_bounds__(gpr::kBlock) k_pr_step(PrArgs a) {
   __shared__ int s_it, s_last;
   if (threadIdx.x == 0) {
     const int done = *(volatile int *)(a.status + 2);
     s_it = done ? -1 : *(volatile int *)(a.status + 1);
+    if (a.cond && blockIdx.x == 0) {
+      const int n = atomicAdd(a.status + 3, 1) + 1;
+      if (done || n >= a.max_iter) cudaGraphSetConditional(a.cond, 0u);
+    }
   }
   __syncthreads();
   const int it = s_it;
@@ -361,8 +371,10 @@ __global__ void __launch_bounds__(gpr::kBlock) k_pr_step(PrArgs a) {
       a.err_hist[it] = t;
       atomicExch(a.bar, 0u);
       a.status[1] = it + 1;
-      if (t < a.tol || it + 1 >= a.max_iter) a.status[2] = 1;
+      const bool done = t < a.tol || it + 1 >= a.max_iter;
+      if (done) a.status[2] = 1;
       __threadfence();
+      if (a.cond && done) cudaGraphSetConditional(a.cond, 0u);
     }
   }
 }
@@ -502,6 +514,7 @@ int hot_entries(const gpr_graph *g, int ki) {
 PrArgs make_args(gpr_graph *g, const gpr_pr_opts &o, int ki) {
   const PrLayout &L = g->L;
   PrArgs a;
+  memset(&a, 0, sizeof(a));  // padding too: cached graphs compare the bytes
   a.m = L.m;
   a.n_long = L.n_long;
   a.n_nz = L.n_nz;
@@ -542,8 +555,11 @@ PrArgs make_args(gpr_graph *g, const gpr_pr_opts &o, int ki) {
   return a;
 }
 
+void drop_loop_graph(gpr_graph *g);
+
 void destroy(gpr_graph *g) {
   if (!g) return;
+  drop_loop_graph(g);
   gpr::free_pr_layout(&g->L);
   gpr::dfree(g->s);
   gpr::dfree(g->c0);
@@ -592,9 +608,9 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
     rc = gpr::build_pr_layout(m, nnz, (const int *)rp, (const int *)cp, (const int *)dp,
                               lane_max, chunk_min, chunk, keep_csr, &g->L, st);
   cudaStreamSynchronize(st);
-  if (orp) cudaFree(rp);
-  if (ocp) cudaFree(cp);
-  if (odp) cudaFree(dp);
+  if (orp) gpr::dfree(rp);
+  if (ocp) gpr::dfree(cp);
+  if (odp) gpr::dfree(dp);
   GPR_TRY(rc);
   const PrLayout &L = g->L;
   GPR_TRY(gpr::dalloc(&g->s, (size_t)m, "scores"));
@@ -647,6 +663,53 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
   return GPR_OK;
 }
 
+// Graph mode: the sweep loop as one CUDA graph -- a while node whose body is
+// one k_pr_step launch; the kernel clears the condition when the solve is
+// done.  The instantiated graph is kept and reused while the kernel and its
+// arguments are unchanged.
+void drop_loop_graph(gpr_graph *g) {
+  if (g->loop_exec) cudaGraphExecDestroy(g->loop_exec);
+  if (g->loop_graph) cudaGraphDestroy(g->loop_graph);
+  g->loop_exec = nullptr;
+  g->loop_graph = nullptr;
+  g->loop_ki = -1;
+}
+
+int graph_loop(gpr_graph *g, const PrArgs &a, int ki, cudaStream_t st) {
+  static_assert(sizeof(PrArgs) <= sizeof(g->loop_args), "loop_args too small");
+  if (!g->loop_exec || g->loop_ki != ki || memcmp(g->loop_args, &a, sizeof(PrArgs)) != 0) {
+    drop_loop_graph(g);
+    cudaGraph_t graph = nullptr;
+    GPR_CUDA(cudaGraphCreate(&graph, 0));
+    g->loop_graph = graph;
+    cudaGraphConditionalHandle h;
+    GPR_CUDA(cudaGraphConditionalHandleCreate(&h, graph, 1u, cudaGraphCondAssignDefault));
+    cudaGraphNodeParams cp = {};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    cudaGraphNode_t cn;
+    GPR_CUDA(cudaGraphAddNode(&cn, graph, nullptr, 0, &cp));
+    PrArgs ac = a;
+    ac.cond = h;
+    void *kargs[] = {&ac};
+    cudaKernelNodeParams kp;
+    memset(&kp, 0, sizeof(kp));
+    kp.func = (void *)kKernels[ki].step;
+    kp.gridDim = dim3(g->grid_step);
+    kp.blockDim = dim3(gpr::kBlock);
+    kp.kernelParams = kargs;
+    cudaGraphNode_t kn;
+    GPR_CUDA(cudaGraphAddKernelNode(&kn, cp.conditional.phGraph_out[0], nullptr, 0, &kp));
+    GPR_CUDA(cudaGraphInstantiate(&g->loop_exec, graph, 0));
+    g->loop_ki = ki;
+    memcpy(g->loop_args, &a, sizeof(PrArgs));
+  }
+  GPR_CUDA(cudaGraphLaunch(g->loop_exec, st));
+  return GPR_OK;
+}
+
 // One solve with sweep kernel ki from the scores in d_scores (device, vertex
 // order); the result is written back to d_scores.
 int solve_impl(gpr_graph *g, float *d_scores, const gpr_pr_opts &o, int ki, gpr_pr_stats *out) {
@@ -666,6 +729,7 @@ int solve_impl(gpr_graph *g, float *d_scores, const gpr_pr_opts &o, int ki, gpr_
   PrArgs a = make_args(g, o, ki);
   if (o.reserved[0] > 0) a.bar_expect += o.reserved[0];  // test hook: a barrier nobody completes
   int launches = 0;
+  bool graph_mode = false;
   GPR_CUDA(cudaEventRecord(g->e0, st));
   if (kKernels[ki].elem == 2)
     k_pr_prologue<bf16><<<grid_for((long long)m + 1), 256, 0, st>>>(
@@ -696,17 +760,8 @@ int solve_impl(gpr_graph *g, float *d_scores, const gpr_pr_opts &o, int ki, gpr_
       }
     }
     if (loop == GPR_LOOP_GRAPH) {
-      const int batch = 8;
-      int done = 0, issued = 0;
-      while (!done && issued < o.max_iter) {
-        for (int q = 0; q < batch && issued < o.max_iter; ++q, ++issued) {
-          kKernels[ki].step<<<g->grid_step, gpr::kBlock, 0, st>>>(a);
-          ++launches;
-        }
-        GPR_CUDA(cudaGetLastError());
-        GPR_CUDA(cudaMemcpyAsync(&done, g->status + 2, sizeof(int), cudaMemcpyDeviceToHost, st));
-        GPR_CUDA(cudaStreamSynchronize(st));
-      }
+      GPR_TRY(graph_loop(g, a, ki, st));
+      graph_mode = true;
     }
   }
   GPR_CUDA(cudaEventRecord(g->e3, st));
@@ -725,7 +780,7 @@ int solve_impl(gpr_graph *g, float *d_scores, const gpr_pr_opts &o, int ki, gpr_
   out->iterations = hs[1];
   g->last_sweeps = hs[1];
   out->solve_ms = ms;
-  out->gpu_launches = launches;
+  out->gpu_launches = launches + (graph_mode ? hs[1] : 0);
   if (hs[1] > 0)
     GPR_CUDA(cudaMemcpy(&out->residual, g->err_hist + hs[1] - 1, sizeof(double),
                         cudaMemcpyDeviceToHost));
@@ -938,7 +993,7 @@ int gpr_pr_residual_f64(gpr_graph *g, const float *any_scores, float damping, do
   if (!g->res_tmp) {
     int rc = gpr::dalloc(&g->res_tmp, 2 * (size_t)m + 2 + L.n_long, "residual scratch");
     if (rc != GPR_OK) {
-      if (owned) cudaFree(dv);
+      if (owned) gpr::dfree(dv);
       return rc;
     }
   }
@@ -958,7 +1013,7 @@ int gpr_pr_residual_f64(gpr_graph *g, const float *any_scores, float damping, do
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(residual, out, sizeof(double), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (owned) cudaFree(dv);
+  if (owned) gpr::dfree(dv);
   if (e != cudaSuccess) {
     gpr::set_error("gpr_pr_residual_f64: %s", cudaGetErrorString(e));
     return GPR_ECUDA;

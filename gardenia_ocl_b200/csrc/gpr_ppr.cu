@@ -489,7 +489,7 @@ int build_chunk_table(gpr_graph *g, int dmax, int chunk, cudaStream_t st) {
   int nlong = 0;
   cudaError_t e = cudaMemcpyAsync(&nlong, cnt, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFree(cnt);
+  gpr::dfree(cnt);
   if (e != cudaSuccess) {
     gpr::set_error("gpr_ppr chunk table: %s", cudaGetErrorString(e));
     return GPR_ECUDA;
@@ -506,7 +506,7 @@ int build_chunk_table(gpr_graph *g, int dmax, int chunk, cudaStream_t st) {
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(&nch, g->b_cbeg + nlong, sizeof(int), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  cudaFree(tmp);
+  gpr::dfree(tmp);
   if (e != cudaSuccess) {
     gpr::set_error("gpr_ppr chunk table: %s", cudaGetErrorString(e));
     return GPR_ECUDA;

@@ -183,9 +183,9 @@ int create_impl(int m, long long nnz, const int *any_Ap, const int *any_Aj, cons
     rc = gpr::build_spmv_layout(m, nnz, (const int *)ap, (const int *)aj, (const float *)ax,
                                 gpr::kSellMaxDefault, gpr::kChunkDefault, &A->L, st);
   cudaStreamSynchronize(st);
-  if (oap) cudaFree(ap);
-  if (oaj) cudaFree(aj);
-  if (oax) cudaFree(ax);
+  if (oap) gpr::dfree(ap);
+  if (oaj) gpr::dfree(aj);
+  if (oax) gpr::dfree(ax);
   GPR_TRY(rc);
   GPR_TRY(gpr::dalloc(&A->partial, (size_t)A->L.n_chunks, "spmv partials"));
   GPR_TRY(gpr::dalloc(&A->cnt, (size_t)A->L.n_long, "spmv counters"));
@@ -304,8 +304,8 @@ int gpr_spmv_solver(int m, int nnz, const int *Ap, const int *Aj, const float *A
       rc = GPR_ECUDA;
     }
   }
-  if (ox) cudaFree(dx);
-  if (oy) cudaFree(dy);
+  if (ox) gpr::dfree(dx);
+  if (oy) gpr::dfree(dy);
   gpr_matrix_destroy(A);
   return rc;
 }

@@ -190,6 +190,43 @@ int gpr_multigraph_pagerank(gpr_multigraph *mg, float *any_scores,
                             const gpr_pr_opts *opts, int *h_iters,
                             double *h_residuals, gpr_pr_stats *stats);
 
+/* ---- autotuner -------------------------------------------------------------
+ * No counterpart in the reference (its launch shape is fixed at compile time,
+ * include/common.h:30, src/pr/Makefile:17-47).  Picks the layout bins
+ * (sell_max = lanes-per-row bound of the SELL width classes, chunk_min /
+ * chunk = chunked-row threshold and chunk size), the shared-memory hot prefix
+ * and the sweep-kernel variant for a graph's in-degree distribution by timing
+ * candidates on the graph (coordinate descent from the defaults, each
+ * candidate the best of 2 solves of exactly `sweeps` sweeps), and caches the
+ * pick per distribution signature in the text file cache_path (NULL: no
+ * cache).  A cached signature returns at once (from_cache = 1). */
+typedef struct {
+  gpr_layout_opts layout;       /* pass to gpr_graph_create_ex */
+  int variant;                  /* pass as gpr_pr_opts.variant */
+  int from_cache;               /* 1: read from the cache, nothing timed */
+  int candidates;               /* configurations timed */
+  double ms_per_sweep;          /* the pick, measured (or as cached) */
+  double default_ms_per_sweep;  /* the defaults, measured (0 when cached) */
+  char signature[48];           /* distribution signature (cache key) */
+} gpr_tune_result;
+int gpr_tune_graph(int m, long long nnz, const int *any_rowptr,
+                   const int *any_col, const int *any_outdeg,
+                   const char *cache_path, int sweeps, gpr_tune_result *out);
+/* Batch: graphs grouped by signature, one group tuned at a time on the whole
+ * batch; h_lopts_out (n_graphs entries) receives each graph's bins for
+ * gpr_multigraph_create; out (may be NULL) describes the largest group. */
+int gpr_tune_multigraph(int n_graphs, const int *h_voff, long long nnz,
+                        const int *any_rowptr, const int *any_col,
+                        const int *any_outdeg, const char *cache_path,
+                        int sweeps, gpr_layout_opts *h_lopts_out,
+                        gpr_tune_result *out);
+/* The signature of a host CSR (batch != 0: the per-graph key of the batch
+ * tuner), and a cache lookup; both host-only. */
+int gpr_tune_signature(int m, long long nnz, const int *h_rowptr, int batch,
+                       char *buf, int len);
+int gpr_tune_cache_lookup(const char *cache_path, const char *signature,
+                          gpr_tune_result *out);
+
 /* ---- PageRank without any allocation ----------------------------------------
  * No counterpart in the reference.  For callers that cannot let a library
  * allocate device memory (their allocator owns the device heap, or the call
@@ -247,6 +284,14 @@ int gpr_gen_stencil27(int n, int **d_Ap, int **d_Aj, float **d_Ax,
 /* Seeded uniform [0,1) floats (24 random bits). */
 int gpr_gen_uniform(long long n, unsigned long long seed, float *d_out);
 int gpr_free(void *d_ptr);
+/* The library keeps device blocks of 1 MiB and more after they are freed
+ * (at most 24 GiB, reused by later requests that fit them within 1/8), so
+ * one-shot calls do not map and unmap gigabytes each time.  Freeing a block
+ * synchronises the device first, as cudaFree does.  gpr_release_cached returns
+ * every cached block to the driver (released_bytes may be NULL);
+ * gpr_cached_bytes reports how much is held. */
+int gpr_release_cached(long long *released_bytes);
+int gpr_cached_bytes(long long *bytes);
 /* Device allocation / copy helpers for callers without a CUDA runtime of
  * their own (copies use cudaMemcpyDefault: any direction). */
 int gpr_malloc(void **d_ptr, size_t bytes);

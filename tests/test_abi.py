@@ -108,3 +108,18 @@ def test_invalid_arguments_rejected_before_device(G):
         G.Graph(np.array([0, 0], np.int32), np.array([], np.int32), np.array([0], np.int32),
                 m=-1)
     assert e.value.status == G.GPR_EINVAL
+
+
+@pytest.mark.gpu
+def test_block_cache_reuses_and_releases(G):
+    G.release_cached()
+    p = C.c_void_p()
+    assert G.lib().gpr_malloc(C.byref(p), 64 << 20) == 0
+    first = p.value
+    assert G.lib().gpr_free(p) == 0
+    assert G.cached_bytes() >= 64 << 20
+    q = C.c_void_p()
+    assert G.lib().gpr_malloc(C.byref(q), (64 << 20) - 4096) == 0  # fits within 1/8
+    assert q.value == first
+    assert G.lib().gpr_free(q) == 0
+    assert G.release_cached() >= 64 << 20 and G.cached_bytes() == 0

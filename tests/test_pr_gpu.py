@@ -197,3 +197,21 @@ def test_bf16_mixed_form_matches_plain_accuracy(G, O, loop):
     assert sm.refine_iterations > 0 and sm.iterations > sm.refine_iterations
     assert sm.residual < 1e-6
     assert l1_m <= 1.1 * l1_p + 1e-8 and mx_m <= 1.1 * mx_p + 1e-9
+
+
+def test_graph_loop_caps_and_reuse(G, O):
+    # The CUDA-graph sweep loop (a while node over the per-sweep kernel) stops
+    # at max_iter and at tol, matches the persistent loop, and is rebuilt when
+    # the options change.
+    rp, col, od = O.rmat_graph(13, 8, seed=11)
+    with G.Graph(rp, col, od) as g:
+        for tol, mi in ((0.0, 7), (1e-6, 60), (0.0, 1), (1e-6, 60), (1e-3, 60)):
+            a, sa = g.pagerank(tol=tol, max_iter=mi, loop=G.LOOP_PERSISTENT)
+            b, sb = g.pagerank(tol=tol, max_iter=mi, loop=G.LOOP_GRAPH)
+            assert sa.iterations == sb.iterations
+            assert np.array_equal(a, b)
+            assert sb.gpu_launches == 2 + sb.iterations
+            if tol == 0.0:
+                assert sb.iterations == mi
+            ref, ref_it, _ = O.pr_plain_f32(rp, col, od, tol=tol, max_iter=mi)
+            assert abs(sb.iterations - ref_it) <= 1
