@@ -139,6 +139,16 @@ def lib():
         "gpr_read_graph": (I, [C.c_char_p, I, I, I, I, I, C.POINTER(I), C.POINTER(I),
                                C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
         "gpr_read_graph_free": (None, [_vp]),
+        "gpr_csr_from_edges": (I, [I, LL, _vp, _vp, _vp, I, I, I, C.POINTER(_vp),
+                                   C.POINTER(_vp), C.POINTER(_vp), C.POINTER(LL)]),
+        "gpr_read_graph_gpu": (I, [C.c_char_p, I, I, I, I, I, C.POINTER(I), C.POINTER(LL),
+                                   C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),
+                                   C.POINTER(_vp)]),
+        "gpr_read_graph_pr": (I, [C.c_char_p, I, C.POINTER(I), C.POINTER(LL), C.POINTER(LL),
+                                  C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp),
+                                  C.POINTER(_vp), C.POINTER(_vp)]),
+        "gpr_parse_edges": (I, [C.c_char_p, I, I, I, C.POINTER(I), C.POINTER(I), C.POINTER(LL),
+                                C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)]),
         "gpr_tune_graph": (I, [I, LL, _vp, _vp, _vp, C.c_char_p, I, C.POINTER(TuneResult)]),
         "gpr_tune_multigraph": (I, [I, _vp, LL, _vp, _vp, _vp, C.c_char_p, I,
                                     C.POINTER(LayoutOptions), C.POINTER(TuneResult)]),
@@ -524,6 +534,27 @@ def read_graph(path, symmetrize=False, transpose=False, sorted=True, remove_self
     return mm, nz, rp, col, deg, wt
 
 
+def parse_edges(path, symmetrize=False, transpose=False, threads=0):
+    """The file's edges as the reference pushes them into per-vertex lists
+    (multithreaded parse, gpr_parse_edges): returns (m, nnz_header, row, col,
+    weight) numpy arrays in push order."""
+    L = lib()
+    m, nnz, n = C.c_int(), C.c_int(), C.c_longlong()
+    p = [C.c_void_p() for _ in range(3)]
+    st = L.gpr_parse_edges(os.fsencode(path), int(symmetrize), int(transpose), int(threads),
+                           C.byref(m), C.byref(nnz), C.byref(n), *[C.byref(q) for q in p])
+    if st != 0:
+        raise GprError(GPR_EINVAL, f"cannot parse {path}")
+    k = n.value
+
+    def take(ptr, ct, dt):
+        a = np.ctypeslib.as_array(C.cast(ptr, C.POINTER(ct)), shape=(max(k, 1),))[:k].astype(dt, copy=True)
+        L.gpr_read_graph_free(ptr)
+        return a
+    return (m.value, nnz.value, take(p[0], C.c_int, np.int32), take(p[1], C.c_int, np.int32),
+            take(p[2], C.c_float, np.float32))
+
+
 class DeviceCSR:
     """CSR arrays in device memory produced by a generator."""
 
@@ -531,11 +562,56 @@ class DeviceCSR:
         self.m, self.nnz = m, nnz
         self.rowptr = DeviceArray(rowptr, m + 1, np.int32)
         self.col = DeviceArray(col, nnz, np.int32)
-        self.third = DeviceArray(third, m if third_dtype == np.int32 else nnz, third_dtype)
+        self.third = DeviceArray(third, m if third_dtype == np.int32 else nnz, third_dtype) \
+            if third else None
 
     def close(self):
         for a in (self.rowptr, self.col, self.third):
-            a.close()
+            if a is not None:
+                a.close()
+
+
+def csr_from_edges(m, row, col, wt=None, sorted=True, remove_selfloops=True,
+                   remove_redundents=True):
+    """fill_data on the GPU over a push list (gpr_csr_from_edges): returns
+    (DeviceCSR with third = weights or None)."""
+    pr, k0 = _ptr(row, np.int32)
+    pc, k1 = _ptr(col, np.int32)
+    pw, k2 = _ptr(wt, np.float32) if wt is not None else (None, None)
+    rp, cp, wp, nnz = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_longlong()
+    _check(lib().gpr_csr_from_edges(int(m), int(len(row)), pr, pc, pw, int(sorted),
+                                    int(remove_selfloops), int(remove_redundents), C.byref(rp),
+                                    C.byref(cp), C.byref(wp) if wt is not None else None,
+                                    C.byref(nnz)))
+    return DeviceCSR(int(m), nnz.value, rp.value, cp.value,
+                     wp.value if wt is not None else None, np.float32)
+
+
+def read_graph_gpu(path, symmetrize=False, transpose=False, sorted=True, remove_selfloops=True,
+                   remove_redundents=True):
+    """read_graph with a multithreaded parse and the CSR built on the GPU:
+    returns (DeviceCSR with third = degree, weights DeviceArray)."""
+    m, nnz = C.c_int(), C.c_longlong()
+    rp, cp, dp, wp = C.c_void_p(), C.c_void_p(), C.c_void_p(), C.c_void_p()
+    _check(lib().gpr_read_graph_gpu(os.fsencode(path), int(symmetrize), int(transpose),
+                                    int(sorted), int(remove_selfloops), int(remove_redundents),
+                                    C.byref(m), C.byref(nnz), C.byref(rp), C.byref(cp),
+                                    C.byref(dp), C.byref(wp)))
+    return (DeviceCSR(m.value, nnz.value, rp.value, cp.value, dp.value, np.int32),
+            DeviceArray(wp.value, nnz.value, np.float32))
+
+
+def read_graph_pr(path, symmetrize=False):
+    """The PR driver's two reads (src/pr/main.cc:23-24) from one parse:
+    returns (out DeviceCSR with third = out-degree, in DeviceCSR with third =
+    out-degree as well -- the PRSolver arguments)."""
+    m, no, ni = C.c_int(), C.c_longlong(), C.c_longlong()
+    p = [C.c_void_p() for _ in range(5)]
+    _check(lib().gpr_read_graph_pr(os.fsencode(path), int(symmetrize), C.byref(m), C.byref(no),
+                                   C.byref(ni), *[C.byref(q) for q in p]))
+    out = DeviceCSR(m.value, no.value, p[0].value, p[1].value, p[2].value, np.int32)
+    inn = DeviceCSR(m.value, ni.value, p[3].value, p[4].value, None, np.int32)
+    return out, inn
 
 
 def gen_rmat(scale, edge_factor=16, seed=1, abc=(0.57, 0.19, 0.19), scramble=True) -> DeviceCSR:

@@ -16,6 +16,7 @@
 
 #include <algorithm>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "gardenia_graph_io.h"
@@ -283,6 +284,330 @@ void read_graph(int argc, char *argv[], int &m, int &n, int &nnz, int *&row_offs
   degree = (int *)malloc((size_t)(m > 0 ? m : 1) * sizeof(int));
   for (int i = 0; i < m; i++) degree[i] = row_offsets[i + 1] - row_offsets[i];
   printf(" Done\n");
+}
+
+namespace {
+
+// ---------------------------------------------------------------------------
+// Parallel parse into the reference's push order.
+//
+// The reference builds vector<vector<Edge>> by pushing, line by line, each
+// edge into the list of one vertex (graph_io.h:133-261).  A push is a pure
+// function of its line: the "symmetrize stops transposing" side effect never
+// changes what is pushed (with symmetrize the reverse edge is pushed before
+// the flag is read, and an .mtx self-loop lands in the same list either way).
+// So the file can be parsed in parallel chunks of whole lines into an array
+// of pushes (row, col, weight) in file order; a stable sort of the pushes by
+// row then reproduces every per-vertex list exactly (gpr_csr_from_edges).
+// Files with a line the reference would read with carried-over values (an
+// .mtx entry line with fewer than two numbers) are parsed sequentially.
+// ---------------------------------------------------------------------------
+struct Pushes {
+  std::vector<int> row, col;
+  std::vector<float> wt;
+  void add(int r, int c, float w) {
+    row.push_back(r);
+    col.push_back(c);
+    wt.push_back(w);
+  }
+};
+
+enum Fmt { kMtx, kGraph, kGr };
+
+// Pushes of one edge src->dst (0-based) under the reference's rules.
+inline void push_edge(Pushes &P, int src, int dst, float wt, bool symmetrize, bool transpose,
+                      bool sym_skips_selfloop) {
+  if (symmetrize) {
+    if (!sym_skips_selfloop || src != dst) P.add(dst, src, wt);
+    P.add(src, dst, wt);
+  } else if (!transpose) {
+    P.add(src, dst, wt);
+  } else {
+    P.add(dst, src, wt);
+  }
+}
+
+struct ChunkResult {
+  Pushes P;
+  int err = 0;          // 1 index out of range, 2 bad arc line, 3 irregular .mtx line
+  long long lines = 0;  // lines parsed
+};
+
+// Parses lines [first_line, limit) of this chunk (global line numbers).
+void parse_chunk(const std::string &buf, size_t cb, size_t ce, long long first_line,
+                 long long limit, Fmt fmt, int m, bool symmetrize, bool transpose,
+                 ChunkResult *out) {
+  size_t pos = cb;
+  long long ln = first_line;
+  while (pos < ce && ln < limit) {
+    const char *nl = (const char *)memchr(buf.data() + pos, '\n', ce - pos);
+    const size_t e = nl ? (size_t)(nl - buf.data()) : ce;
+    const char *p = buf.data() + pos, *pe = buf.data() + e;
+    if (fmt == kMtx) {
+      int src = 0, dst = 0;
+      float wt = 1.0f;
+      int num = 0;
+      if (parse_int(p, pe, &src)) {
+        ++num;
+        if (parse_int(p, pe, &dst)) {
+          ++num;
+          if (parse_float(p, pe, &wt)) ++num;
+        }
+      }
+      if (num < 2) {
+        out->err = 3;
+        return;
+      }
+      if (num == 2) wt = 1;
+      if (wt < 0) wt = -wt;
+      const int s = src - 1, d = dst - 1;
+      if (!in_range(s, m) || !in_range(d, m)) {
+        out->err = 1;
+        return;
+      }
+      push_edge(out->P, s, d, wt, symmetrize, transpose, true);
+    } else if (fmt == kGr) {
+      if (p < pe) ++p;
+      int src = 0, dst = 0;
+      if (!parse_int(p, pe, &src) || !parse_int(p, pe, &dst)) {
+        out->err = 2;
+        return;
+      }
+      --src;
+      --dst;
+      if (!in_range(src, m) || !in_range(dst, m)) {
+        out->err = 1;
+        return;
+      }
+      push_edge(out->P, src, dst, 1.0f, symmetrize, transpose, false);
+    } else {
+      const int src = (int)ln;
+      int dst;
+      while (parse_int(p, pe, &dst)) {
+        --dst;
+        if (!in_range(dst, m)) {
+          out->err = 1;
+          return;
+        }
+        push_edge(out->P, src, dst, 1.0f, symmetrize, transpose, false);
+      }
+    }
+    ++ln;
+    ++out->lines;
+    pos = nl ? e + 1 : ce;
+  }
+}
+
+int io_threads() {
+  const char *env = getenv("GPR_IO_THREADS");
+  int t = env ? atoi(env) : (int)std::thread::hardware_concurrency();
+  return std::max(1, std::min(t, 64));
+}
+
+// Parses `path` into pushes; returns 0, or -1 (cannot open / malformed:
+// message in *why) or -2 (needs the sequential reader).
+int parse_pushes(const char *path, bool symmetrize, bool transpose, int threads, int *m_out,
+                 int *nnz_out, Pushes *out, const char **why) {
+  Fmt fmt;
+  if (strstr(path, ".mtx")) fmt = kMtx;
+  else if (strstr(path, ".graph")) fmt = kGraph;
+  else if (strstr(path, ".gr")) fmt = kGr;
+  else {
+    *why = "unrecognizable input file format";
+    return -1;
+  }
+  Reader R;
+  if (!R.load(path)) {
+    *why = "cannot open";
+    return -1;
+  }
+  size_t b, e;
+  if (!R.line(&b, &e)) {
+    *why = "empty file";
+    return -1;
+  }
+  int m = 0, n = 0, nnz = 0;
+  const char *p, *pe;
+  if (fmt == kMtx) {
+    while (b < e && R.buf[b] == '%')
+      if (!R.line(&b, &e)) {
+        *why = "missing size line";
+        return -1;
+      }
+    p = R.buf.data() + b;
+    pe = R.buf.data() + e;
+    if (!parse_int(p, pe, &m) || !parse_int(p, pe, &n) || !parse_int(p, pe, &nnz)) {
+      *why = "bad size line";
+      return -1;
+    }
+  } else if (fmt == kGr) {
+    while (b < e && R.buf[b] == 'c')
+      if (!R.line(&b, &e)) {
+        *why = "missing problem line";
+        return -1;
+      }
+    p = R.buf.data() + b;
+    pe = R.buf.data() + e;
+    if (p < pe) ++p;
+    while (p < pe && (*p == ' ' || *p == '\t')) ++p;
+    while (p < pe && *p != ' ' && *p != '\t') ++p;
+    if (!parse_int(p, pe, &m) || !parse_int(p, pe, &nnz)) {
+      *why = "bad problem line";
+      return -1;
+    }
+  } else {
+    p = R.buf.data() + b;
+    pe = R.buf.data() + e;
+    if (!parse_int(p, pe, &m) || !parse_int(p, pe, &nnz)) {
+      *why = "bad size line";
+      return -1;
+    }
+  }
+  if (m < 0) {
+    *why = "bad size line";
+    return -1;
+  }
+  const long long limit = fmt == kGraph ? m : nnz;
+  const size_t start = R.pos, size = R.buf.size();
+  const int T = std::max(1, threads);
+  std::vector<size_t> cut(T + 1, size);
+  cut[0] = start;
+  for (int k = 1; k < T; ++k) {
+    size_t q = start + (size - start) / T * k;
+    if (q < cut[k - 1]) q = cut[k - 1];
+    const char *nl = q < size ? (const char *)memchr(R.buf.data() + q, '\n', size - q) : nullptr;
+    cut[k] = nl ? (size_t)(nl - R.buf.data()) + 1 : size;
+  }
+  // Lines per chunk (a final line without a newline counts), then each
+  // chunk's first global line number.
+  std::vector<long long> nlines(T, 0), first(T + 1, 0);
+  {
+    std::vector<std::thread> th;
+    for (int k = 0; k < T; ++k)
+      th.emplace_back([&, k] {
+        long long c = 0;
+        for (size_t i = cut[k]; i < cut[k + 1]; ++i) c += R.buf[i] == '\n';
+        if (cut[k + 1] == size && cut[k] < size && R.buf[size - 1] != '\n') ++c;
+        nlines[k] = c;
+      });
+    for (auto &t : th) t.join();
+  }
+  for (int k = 0; k < T; ++k) first[k + 1] = first[k] + nlines[k];
+  if (fmt != kGraph && first[T] < limit) {
+    *why = fmt == kMtx ? "fewer entries than announced" : "fewer arcs than announced";
+    return -1;
+  }
+  std::vector<ChunkResult> res(T);
+  {
+    std::vector<std::thread> th;
+    for (int k = 0; k < T; ++k)
+      th.emplace_back([&, k] {
+        parse_chunk(R.buf, cut[k], cut[k + 1], first[k], limit, fmt, m, symmetrize, transpose,
+                    &res[k]);
+      });
+    for (auto &t : th) t.join();
+  }
+  for (auto &r : res) {
+    if (r.err == 3) return -2;
+    if (r.err == 1) {
+      *why = "index out of range";
+      return -1;
+    }
+    if (r.err == 2) {
+      *why = "bad arc line";
+      return -1;
+    }
+  }
+  size_t total = 0;
+  for (auto &r : res) total += r.P.row.size();
+  out->row.resize(total);
+  out->col.resize(total);
+  out->wt.resize(total);
+  size_t o = 0;
+  for (auto &r : res) {
+    std::copy(r.P.row.begin(), r.P.row.end(), out->row.begin() + o);
+    std::copy(r.P.col.begin(), r.P.col.end(), out->col.begin() + o);
+    std::copy(r.P.wt.begin(), r.P.wt.end(), out->wt.begin() + o);
+    o += r.P.row.size();
+  }
+  *m_out = m;
+  *nnz_out = nnz;
+  return 0;
+}
+
+// Sequential fallback: the reference-order reader, emitting pushes.
+void parse_pushes_sequential(const char *path, bool symmetrize, bool transpose, int *m_out,
+                             int *nnz_out, Pushes *out) {
+  Reader R;
+  if (!R.load(path)) bad(path, "cannot open");
+  size_t b, e;
+  if (!R.line(&b, &e)) bad(path, "empty file");
+  while (b < e && R.buf[b] == '%')
+    if (!R.line(&b, &e)) bad(path, "missing size line");
+  const char *p = R.buf.data() + b, *pe = R.buf.data() + e;
+  int m = 0, n = 0, nnz = 0;
+  if (!parse_int(p, pe, &m) || !parse_int(p, pe, &n) || !parse_int(p, pe, &nnz))
+    bad(path, "bad size line");
+  int src = 0, dst = 0;
+  WeightT wt = 1.0f;
+  for (int i = 0; i < nnz; i++) {
+    if (!R.line(&b, &e)) bad(path, "fewer entries than announced");
+    p = R.buf.data() + b;
+    pe = R.buf.data() + e;
+    int num = 0;
+    if (parse_int(p, pe, &src)) {
+      ++num;
+      if (parse_int(p, pe, &dst)) {
+        ++num;
+        if (parse_float(p, pe, &wt)) ++num;
+      }
+    }
+    if (num == 2) wt = 1;
+    if (wt < 0) wt = -wt;
+    const int s = src - 1, d = dst - 1;
+    if (!in_range(s, m) || !in_range(d, m)) bad(path, "index out of range");
+    push_edge(*out, s, d, wt, symmetrize, transpose, true);
+  }
+  *m_out = m;
+  *nnz_out = nnz;
+}
+
+}  // namespace
+
+// Pushes of `path` in the reference's order (row, col, weight), malloc'd
+// here and released with gpr_read_graph_free.  threads <= 0: all cores
+// (GPR_IO_THREADS overrides).
+extern "C" int gpr_parse_edges(const char *path, int symmetrize, int transpose, int threads,
+                               int *m_out, int *nnz_header, long long *n_push, int **row,
+                               int **col, float **wt) {
+  if (!path || !m_out || !nnz_header || !n_push || !row || !col || !wt) return 1;
+  Pushes P;
+  const char *why = "";
+  int m = 0, nnz = 0;
+  const int rc = parse_pushes(path, symmetrize != 0, transpose != 0,
+                              threads > 0 ? threads : io_threads(), &m, &nnz, &P, &why);
+  if (rc == -1) {
+    fprintf(stderr, "gpr_parse_edges: %s: %s\n", path, why);
+    return 1;
+  }
+  if (rc == -2) {
+    P = Pushes();
+    parse_pushes_sequential(path, symmetrize != 0, transpose != 0, &m, &nnz, &P);
+  }
+  const size_t k = P.row.size();
+  *row = (int *)malloc(sizeof(int) * (k ? k : 1));
+  *col = (int *)malloc(sizeof(int) * (k ? k : 1));
+  *wt = (float *)malloc(sizeof(float) * (k ? k : 1));
+  if (!*row || !*col || !*wt) return 2;
+  if (k) {
+    memcpy(*row, P.row.data(), sizeof(int) * k);
+    memcpy(*col, P.col.data(), sizeof(int) * k);
+    memcpy(*wt, P.wt.data(), sizeof(float) * k);
+  }
+  *m_out = m;
+  *nnz_header = nnz;
+  *n_push = (long long)k;
+  return 0;
 }
 
 // C entry point for foreign callers (ctypes / cgo): same flags, arrays

@@ -12,7 +12,8 @@
 // Search: coordinate descent from the defaults -- kernel variant, then hot
 // prefix, then lanes-per-row bound, then chunk threshold / size -- each
 // candidate timed as the best of `reps` solves of exactly `sweeps` sweeps
-// (tol 0), device time of the sweep loop (gpr_pr_stats.loop_ms).  The batch
+// (tol 0), device time of the sweep loop (gpr_pr_stats.loop_ms), and taken
+// only when at least 3% faster than the current pick.  The batch
 // tuner groups graphs by signature and tunes one group at a time on the whole
 // batch, the other groups keeping their current picks.
 //
@@ -152,6 +153,10 @@ struct SingleBench {
   }
 };
 
+// A candidate must beat the current pick by this fraction to replace it, so
+// run-to-run timing noise does not move the pick.
+constexpr double kMargin = 0.03;
+
 // Coordinate descent over one knob: keeps the best of `vals` applied to x.
 template <typename F, typename T>
 void descend(Cfg *x, double *best, const std::vector<T> &vals, F apply,
@@ -161,7 +166,7 @@ void descend(Cfg *x, double *best, const std::vector<T> &vals, F apply,
     apply(&y, v);
     if (y == *x) continue;
     const double t = time(y);
-    if (t < *best) {
+    if (t < *best * (1.0 - kMargin)) {
       *best = t;
       *x = y;
     }

@@ -311,6 +311,40 @@ int gpr_read_graph(const char *path, int symmetrize, int transpose, int sorted,
                    float **weight);
 void gpr_read_graph_free(void *p);
 
+/* The file's edges in the order the reference pushes them into its
+ * per-vertex lists (graph_io.h:133-261): entry k appends (col[k], wt[k]) to
+ * the list of vertex row[k]; symmetrize / transpose as in read_graph.
+ * Parsed by `threads` threads (<= 0: all cores, GPR_IO_THREADS overrides);
+ * arrays malloc'd, released with gpr_read_graph_free.  Returns 0, or
+ * non-zero when the file cannot be read. */
+int gpr_parse_edges(const char *path, int symmetrize, int transpose, int threads,
+                    int *m, int *nnz_header, long long *n_push, int **row,
+                    int **col, float **wt);
+/* fill_data (graph_io.h:21-130) on the GPU over such a push list: lists in
+ * push order (stable), optionally sorted by column, self-loops dropped, then
+ * an entry equal to the previous kept one dropped.  Rows and columns match
+ * the reference for every flag; with `sorted` the weights of duplicate
+ * columns may come in another order (std::sort leaves it unspecified).
+ * Outputs are device arrays allocated here (gpr_free); d_wt may be NULL. */
+int gpr_csr_from_edges(int m, long long n, const int *any_row, const int *any_col,
+                       const float *any_wt, int sorted, int remove_selfloops,
+                       int remove_redundents, int **d_rowptr, int **d_col,
+                       float **d_wt, long long *nnz);
+/* read_graph with the parse above and the CSR built on the GPU (device
+ * outputs; d_wt may be NULL). */
+int gpr_read_graph_gpu(const char *path, int symmetrize, int transpose, int sorted,
+                       int remove_selfloops, int remove_redundents, int *m,
+                       long long *nnz, int **d_rowptr, int **d_col, int **d_degree,
+                       float **d_wt);
+/* The PR driver's two reads (src/pr/main.cc:23-24: out-CSR, then the
+ * transposed in-CSR, both unsorted with self-loops and repeats removed) from
+ * one parse: the in-CSR is built from the same pushes with row and column
+ * swapped.  Identical to the reference's two read_graph calls. */
+int gpr_read_graph_pr(const char *path, int symmetrize, int *m,
+                      long long *nnz_out_csr, long long *nnz_in_csr,
+                      int **d_out_rowptr, int **d_out_col, int **d_out_degree,
+                      int **d_in_rowptr, int **d_in_col);
+
 #ifdef __cplusplus
 }
 #endif

@@ -252,6 +252,29 @@ def uniform_int(n, seed, hi):
     return out
 
 
+def csr_from_pushes(m, row, col, wt, sorted=True, remove_selfloops=True, remove_redundents=True):
+    """fill_data of include/graph_io.h:21-130 over a push list (entry k
+    appends (col[k], wt[k]) to the list of vertex row[k], in order): per-row
+    lists in push order, optionally sorted by column (stable), self-loops
+    dropped, then entries equal to the previous kept one dropped.  Returns
+    (rowptr, col, wt)."""
+    row = np.asarray(row, dtype=np.int64)
+    col = np.asarray(col, dtype=np.int64)
+    wt = np.asarray(wt, dtype=np.float32)
+    order = np.lexsort((col, row)) if sorted else np.argsort(row, kind="stable")
+    r, c, w = row[order], col[order], wt[order]
+    if remove_selfloops:
+        keep = c != r
+        r, c, w = r[keep], c[keep], w[keep]
+    if remove_redundents and len(r):
+        keep = np.ones(len(r), dtype=bool)
+        keep[1:] = ~((r[1:] == r[:-1]) & (c[1:] == c[:-1]))
+        r, c, w = r[keep], c[keep], w[keep]
+    rowptr = np.zeros(m + 1, dtype=np.int32)
+    np.cumsum(np.bincount(r, minlength=m), out=rowptr[1:])
+    return rowptr, c.astype(np.int32), w
+
+
 def transpose_csr(m, rowptr, col):
     """Out-CSR of a pull (in-)CSR, columns ascending: used for the push check."""
     rowptr = np.asarray(rowptr, dtype=np.int64)

@@ -163,3 +163,37 @@ def test_multigraph_sizes_log_uniform(O):
     assert sizes.min() >= 1000 and sizes.max() <= 500000
     frac = np.mean(np.log(sizes) < 0.5 * (np.log(1000) + np.log(500000)))
     assert abs(frac - 0.5) < 0.03
+
+
+def same_weights_per_entry(rp, c, w, w_ref):
+    """Equal (row, column, weight) multisets: the weights of equal columns in
+    a row may come in another order."""
+    rows = np.repeat(np.arange(len(rp) - 1), np.diff(rp))
+    a = np.lexsort((w, c, rows))
+    b = np.lexsort((w_ref, c, rows))
+    return np.array_equal(w[a], w_ref[b])
+
+
+@pytest.mark.parametrize("name", ["graph_small", "graph_dups", "graph_simple"])
+@pytest.mark.parametrize("ext", [".mtx", ".gr", ".graph"])
+@pytest.mark.parametrize("threads", [1, 3, 8])
+def test_parallel_parse_reproduces_reference_lists(G, O, loader_gold, name, ext, threads):
+    # Pushes from the multithreaded parser, formed into lists by fill_data's
+    # rules, give the reference loader's CSR under every flag combination.
+    # With `sorted` the reference orders equal columns of a row by std::sort,
+    # whose order among equal keys the C++ standard leaves unspecified; a
+    # stable sort gives the same rows and columns, and the same weights except
+    # that duplicate columns may carry them in another order (and duplicate
+    # removal may then keep another duplicate's weight).
+    path = os.path.join(GOLD, name + ext)
+    for sym, trans in itertools.product([False, True], repeat=2):
+        m, _, row, col, wt = G.parse_edges(path, sym, trans, threads=threads)
+        for srt, sl, rd in itertools.product([False, True], repeat=3):
+            key = name + ext + ":" + "".join(str(int(x)) for x in (sym, trans, srt, sl, rd))
+            rp, c, w = O.csr_from_pushes(m, row, col, wt, srt, sl, rd)
+            assert np.array_equal(rp, loader_gold[key + ":rowptr"]), key
+            assert np.array_equal(c, loader_gold[key + ":col"]), key
+            if not srt:
+                assert np.array_equal(w, loader_gold[key + ":weight"]), key
+            elif not rd:
+                assert same_weights_per_entry(rp, c, w, loader_gold[key + ":weight"]), key

@@ -37,7 +37,7 @@ def test_tune_graph_and_cache(G, O, tmp_path):
     cache = str(tmp_path / "tune.txt")
     r = G.tune_graph(rp, col, od, cache=cache, sweeps=4)
     assert not r["from_cache"] and r["candidates"] >= 10
-    assert r["ms_per_sweep"] <= r["default_ms_per_sweep"]
+    assert r["ms_per_sweep"] <= r["default_ms_per_sweep"]  # a pick only replaces a slower one
     assert os.path.exists(cache)
     r2 = G.tune_graph(rp, col, od, cache=cache, sweeps=4)
     assert r2["from_cache"] and r2["signature"] == r["signature"]
