@@ -105,6 +105,7 @@ def lib():
                               C.POINTER(PrStats)]),
         "gpr_page_rank": (I, [I, I, _vp, _vp, _vp, _vp, C.POINTER(PrOptions),
                               C.POINTER(PrStats)]),
+        "gpr_pagerank_push": (I, [_vp, _vp, C.POINTER(PrOptions), C.POINTER(PrStats)]),
         "gpr_ppr": (I, [_vp, I, _vp, _vp, C.POINTER(PrOptions), _vp, C.POINTER(PrStats)]),
         "gpr_pagerank_noalloc": (I, [I, I, _vp, _vp, _vp, _vp, C.POINTER(PrOptions),
                                      C.POINTER(PrStats), _vp]),
@@ -242,7 +243,7 @@ class Graph:
     the out-degree of every vertex (src/pr/omp_base.cc:9 arguments)."""
 
     def __init__(self, rowptr, col, outdeg, m=None, nnz=None, sell_max=0, chunk=0, chunk_min=0,
-                 hot_entries=0, batched=False):
+                 hot_entries=0, batched=False, push=False):
         L = lib()
         m = int(len(rowptr) - 1) if m is None else int(m)
         nnz = int(len(col)) if nnz is None else int(nnz)
@@ -251,7 +252,7 @@ class Graph:
         pd, k2 = _ptr(outdeg, np.int32)
         h = C.c_void_p()
         lo = LayoutOptions(int(sell_max), int(chunk), int(chunk_min), int(hot_entries),
-                           1 if batched else 0)
+                           (1 if batched else 0) | (2 if push else 0))
         _check(L.gpr_graph_create_ex(m, nnz, pr, pc, pd, C.byref(lo), C.byref(h)))
         self._h, self.m, self.nnz = h, m, nnz
         self.last_stats = None
@@ -268,6 +269,18 @@ class Graph:
         ps, keep = _ptr(scores)
         st = PrStats()
         _check(lib().gpr_pagerank(self._h, ps, C.byref(o), C.byref(st)))
+        self.last_stats = st
+        return scores, st
+
+    def pagerank_push(self, scores=None, opts: PrOptions | None = None, **kw):
+        """Push-style solve (graph created with push=True or batched=True);
+        same arguments and results as ``pagerank``."""
+        o = opts if opts is not None else options(**kw)
+        if scores is None:
+            scores = np.full(self.m, np.float32(1.0) / np.float32(self.m), dtype=np.float32)
+        ps, keep = _ptr(scores)
+        st = PrStats()
+        _check(lib().gpr_pagerank_push(self._h, ps, C.byref(o), C.byref(st)))
         self.last_stats = st
         return scores, st
 

@@ -181,5 +181,63 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+__device__ __forceinline__ double block_sum_double(double v) {
+  __shared__ double red[32];
+  v = warp_sum(v);
+  const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  __syncthreads();
+  if (lane == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int i = 0; i < (int)(blockDim.x >> 5); ++i) t += red[i];
+  return t;
+}
+
+// Bounded grid barrier of a cooperative launch.  bar[0] counts arrivals,
+// bar[1] is the generation.  When cta_part is given, every CTA first stores
+// its value in cta_part[blockIdx.x] and the last CTA to arrive sums them in
+// CTA order (deterministic) into *sum_out before it opens the next
+// generation.  Waits are bounded by timeout_ns of %globaltimer; on expiry
+// status[0] bit 0 is raised and false is returned.  Call from every thread.
+__device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned expect, double *cta_part,
+                                             double cta_value, double *sum_out, int *status,
+                                             long long timeout_ns) {
+  __shared__ int s_state;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (cta_part) cta_part[blockIdx.x] = cta_value;
+    const unsigned gen = ld_acquire(bar + 1);
+    __threadfence();
+    const unsigned arrived = atomicAdd(bar, 1u);
+    s_state = 0;
+    if (arrived == expect - 1u) {
+      __threadfence();
+      if (cta_part) {
+        double t = 0.0;
+        for (unsigned i = 0; i < gridDim.x; ++i) t += __ldcg(cta_part + i);
+        *sum_out = t;
+      }
+      atomicExch(bar, 0u);
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      const long long t0 = global_ns();
+      unsigned spins = 0;
+      while (ld_acquire(bar + 1) == gen) {
+        if ((++spins & 31u) == 0 && global_ns() - t0 > timeout_ns) {
+          atomicOr(status, 1);
+          s_state = 2;
+          break;
+        }
+        __nanosleep(100);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return s_state != 2;
+}
+
 }  // namespace dev
 }  // namespace gpr

@@ -177,6 +177,10 @@ struct gpr_graph {
   // b_chunk-edge chunks), built on first use for a given (b_dmax, b_chunk).
   int *b_cbeg = nullptr, *b_crow = nullptr;
   int b_nlong = -1, b_nchunks = 0, b_dmax = 0, b_chunk = 0;
+  // Push solver: edges sorted by source and the per-vertex accumulators,
+  // built on first use.
+  int *push_src = nullptr, *push_dst = nullptr;
+  float *push_sum = nullptr;
   // Graph mode: the instantiated sweep-loop graph and the kernel and
   // arguments it was built for.
   cudaGraph_t loop_graph = nullptr;

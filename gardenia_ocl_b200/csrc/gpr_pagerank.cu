@@ -577,6 +577,9 @@ void destroy(gpr_graph *g) {
   gpr::dfree(g->wq);
   gpr::dfree(g->b_cbeg);
   gpr::dfree(g->b_crow);
+  gpr::dfree(g->push_src);
+  gpr::dfree(g->push_dst);
+  gpr::dfree(g->push_sum);
   if (g->e0) cudaEventDestroy(g->e0);
   if (g->e1) cudaEventDestroy(g->e1);
   if (g->e2) cudaEventDestroy(g->e2);
@@ -902,7 +905,7 @@ int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr, const int *
     return GPR_ENODEV;
   }
   gpr_graph *g = new gpr_graph();
-  const bool keep_csr = lopts && (lopts->flags & GPR_LAYOUT_BATCHED);
+  const bool keep_csr = lopts && (lopts->flags & (GPR_LAYOUT_BATCHED | GPR_LAYOUT_PUSH));
   int rc = create_impl(m, nnz, any_rowptr, any_col, any_outdeg, lane_max, chunk_min, chunk,
                        hot_max, keep_csr, g);
   if (rc != GPR_OK) {

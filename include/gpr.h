@@ -92,7 +92,10 @@ int gpr_graph_create(int m, long long nnz, const int *any_rowptr,
                      const int *any_col, const int *any_outdeg,
                      gpr_graph **out);
 /* Layout knobs (the autotuner's search space); zero fields take defaults. */
-enum { GPR_LAYOUT_BATCHED = 1 /* also keep a relabelled CSR: needed by gpr_ppr */ };
+enum {
+  GPR_LAYOUT_BATCHED = 1, /* also keep a relabelled CSR: needed by gpr_ppr */
+  GPR_LAYOUT_PUSH = 2     /* also keep it for gpr_pagerank_push */
+};
 typedef struct {
   int sell_max;   /* max edges per lane in a SELL slice: rows of in-degree <= sell_max get
                      one lane, wider rows 2..32 lanes (default 64) */
@@ -155,6 +158,17 @@ int gpr_page_rank(int m, int nnz, const int *row_offsets,
  * GPR_LAYOUT_BATCHED. */
 int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
             const gpr_pr_opts *opts, int *h_iters, gpr_pr_stats *stats);
+
+/* ---- push-style PageRank --------------------------------------------------
+ * The reference's push variants (src/pr/scatter.cu:16-41, lb.cu:20-82)
+ * scatter each source's contribution to its out-neighbours with atomic adds.
+ * Same recurrence and stop rule as gpr_pagerank (so the two directions solve
+ * the same problem); edges sorted by source, hot destinations accumulated in
+ * shared memory, one persistent launch.  Atomic adds make the last bits of
+ * the result vary from run to run.  The graph must be created with
+ * GPR_LAYOUT_PUSH (or GPR_LAYOUT_BATCHED); FP32 only. */
+int gpr_pagerank_push(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts,
+                      gpr_pr_stats *stats);
 
 /* ---- uneven multi-graph batch ------------------------------------------------
  * No counterpart in the reference (each reference run solves one graph read
