@@ -106,6 +106,10 @@ def lib():
         "gpr_page_rank": (I, [I, I, _vp, _vp, _vp, _vp, C.POINTER(PrOptions),
                               C.POINTER(PrStats)]),
         "gpr_pagerank_push": (I, [_vp, _vp, C.POINTER(PrOptions), C.POINTER(PrStats)]),
+        "gpr_symgs_create": (I, [I, LL, _vp, _vp, _vp, _vp, _vp, I, C.POINTER(_vp)]),
+        "gpr_symgs_destroy": (I, [_vp]),
+        "gpr_symgs_apply": (I, [_vp, _vp, _vp, I, C.POINTER(D)]),
+        "gpr_symgs_solver": (I, [I, I, _vp, _vp, _vp, _vp, _vp, _vp, _vp, I]),
         "gpr_ppr": (I, [_vp, I, _vp, _vp, C.POINTER(PrOptions), _vp, C.POINTER(PrStats)]),
         "gpr_pagerank_noalloc": (I, [I, I, _vp, _vp, _vp, _vp, C.POINTER(PrOptions),
                                      C.POINTER(PrStats), _vp]),
@@ -510,6 +514,61 @@ class Matrix:
             self.close()
         except Exception:
             pass
+
+
+class SymGS:
+    """Multicolour symmetric Gauss-Seidel smoother (src/symgs): the matrix
+    laid out per colour on the device; ``apply`` runs sweeps in place."""
+
+    def __init__(self, Ap, Aj, Ax, indices, color_offsets, m=None, nnz=None):
+        m = int(len(Ap) - 1) if m is None else int(m)
+        nnz = int(len(Aj)) if nnz is None else int(nnz)
+        co = np.ascontiguousarray(color_offsets, dtype=np.int32)
+        args = [_ptr(Ap, np.int32), _ptr(Aj, np.int32), _ptr(Ax, np.float32),
+                _ptr(indices, np.int32)]
+        h = C.c_void_p()
+        _check(lib().gpr_symgs_create(m, nnz, *[p for p, _ in args], C.c_void_p(co.ctypes.data),
+                                      len(co) - 1, C.byref(h)))
+        self._h, self.m = h, m
+
+    def apply(self, x, b, sweeps=1):
+        """x (float32 host array or device memory) updated in place; returns
+        the device time of the launch in ms."""
+        px, k0 = _ptr(x)
+        pb, k1 = _ptr(b, np.float32)
+        ms = C.c_double()
+        _check(lib().gpr_symgs_apply(self._h, px, pb, int(sweeps), C.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gpr_symgs_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def SymGSSolver(m, nnz, Ap, Aj, indices, Ax, x, b, color_offsets):
+    """src/symgs/symgs.h:28: one sweep, ``x`` (float32 numpy) updated in place."""
+    if not (isinstance(x, np.ndarray) and x.dtype == np.float32 and x.flags.c_contiguous):
+        raise TypeError("x must be a contiguous float32 numpy array")
+    co = np.ascontiguousarray(color_offsets, dtype=np.int32)
+    args = [_ptr(Ap, np.int32), _ptr(Aj, np.int32), _ptr(indices, np.int32),
+            _ptr(Ax, np.float32)]
+    pb, kb = _ptr(b, np.float32)
+    _check(lib().gpr_symgs_solver(int(m), int(nnz), *[p for p, _ in args],
+                                  C.c_void_p(x.ctypes.data), pb, C.c_void_p(co.ctypes.data),
+                                  len(co) - 1))
 
 
 def SpmvSolver(m, nnz, Ap, Aj, Ax, x, y):

@@ -1,5 +1,5 @@
 // C++ drop-ins with the reference's symbols (src/pr/pr.h:23-24,
-// src/spmv/spmv.h:29-30) over the C ABI of gpr.h.  Output lines and the
+// src/spmv/spmv.h:29-30, src/symgs/symgs.h:28-29) over the C ABI of gpr.h.  Output lines and the
 // print-and-exit error convention follow the reference drivers.
 #include <cuda_runtime.h>
 #include <float.h>
@@ -11,6 +11,7 @@
 
 #include "gardenia_pr.h"
 #include "gardenia_spmv.h"
+#include "gardenia_symgs.h"
 #include "gardenia_timer.h"
 #include "gpr.h"
 
@@ -163,4 +164,69 @@ void SpmvVerifier(int m, int nnz, int *Ap, int *Aj, ValueType *Ax, ValueType *x,
   printf("\t[max error %9f]\n", max_error);
   if (max_error > 5 * sqrtf(FLT_EPSILON)) printf("POSSIBLE FAILURE\n");
   else printf("Correct\n");
+}
+
+// ---- SymGS ---------------------------------------------------------------
+
+void SymGSSolver(int m, int nnz, int *Ap, int *Aj, int *indices, ValueType *Ax, ValueType *x,
+                 ValueType *b, std::vector<int> color_offsets) {
+  printf("Launching B200 SymGS solver (gpr, sm_100a, %d colours) ...\n",
+         (int)color_offsets.size() - 1);
+  gpr_symgs *h = nullptr;
+  if (gpr_symgs_create(m, nnz, Ap, Aj, Ax, indices, color_offsets.data(),
+                       (int)color_offsets.size() - 1, &h) != GPR_OK)
+    die("SymGSSolver");
+  double ms = 0.0;
+  if (gpr_symgs_apply(h, x, b, 1, &ms) != GPR_OK) die("SymGSSolver");
+  gpr_symgs_destroy(h);
+  printf("\truntime [%s] = %f ms.\n", "gpr_b200", ms);
+}
+
+namespace {
+
+// One row sweep of src/symgs/verifier.cc:56-70 (gs_serial).
+void gs_rows(const int *Ap, const int *Aj, const int *indices, const ValueType *Ax, ValueType *x,
+             const ValueType *b, int begin, int end) {
+  for (int i = begin; i != end; ++i) {
+    const int r = indices[i];
+    ValueType rsum = 0, diag = 0;
+    for (int jj = Ap[r]; jj < Ap[r + 1]; ++jj) {
+      const int j = Aj[jj];
+      if (j == r) diag = Ax[jj];
+      else rsum += x[j] * Ax[jj];
+    }
+    if (diag != 0) x[r] = (b[r] - rsum) / diag;
+  }
+}
+
+}  // namespace
+
+void SymGSVerifier(int num_rows, int *Ap, int *Aj, int *indices, ValueType *Ax,
+                   ValueType *test_x, ValueType *x_host, ValueType *b,
+                   std::vector<int> color_offsets) {
+  printf("Verifying...\n");
+  std::vector<ValueType> x(x_host, x_host + num_rows);
+  Timer t;
+  t.Start();
+  const int nc = (int)color_offsets.size() - 1;
+  for (int c = 0; c < nc; ++c)
+    gs_rows(Ap, Aj, indices, Ax, x.data(), b, color_offsets[c], color_offsets[c + 1]);
+  for (int c = nc; c > 0; --c)
+    gs_rows(Ap, Aj, indices, Ax, x.data(), b, color_offsets[c - 1], color_offsets[c]);
+  t.Stop();
+  printf("\truntime [verify] = %f ms.\n", t.Millisecs());
+  const ValueType eps = sqrtf(FLT_EPSILON);
+  ValueType max_error = 0;
+  bool ok = true;
+  for (int i = 0; i < num_rows; ++i) {
+    const ValueType a = test_x[i], r = x[i];
+    const ValueType err = fabsf(a - r);
+    if (err != 0) max_error = fmaxf(max_error, err / (fabsf(a) + fabsf(r) + eps));
+    if (ok && fabs((double)(a - r)) > 1e-4 * (fabs((double)a) + fabs((double)r)) + 1e-4) {
+      ok = false;
+      printf("x_test[%d] (%f) != x[%d] (%f)\n", i, a, i, r);
+    }
+  }
+  printf("\t[max error %9f]\n", max_error);
+  printf(ok ? "Correct\n" : "POSSIBLE FAILURE\n");
 }

@@ -274,6 +274,29 @@ int gpr_spmv(gpr_matrix *A, const float *d_x, float *d_y, void *stream);
 int gpr_spmv_solver(int m, int nnz, const int *Ap, const int *Aj,
                     const float *Ax, const float *x, float *y);
 
+/* ---- symmetric Gauss-Seidel (multicolour) ----------------------------------
+ * src/symgs: one sweep = the colours of a vertex colouring forward, then
+ * backward; rows of one colour are updated together; each row sums
+ * x[j]*Ax[jj] over its off-diagonal entries in CSR order and, when its last
+ * diagonal entry d != 0, sets x = (b - sum) / d (src/symgs/omp_base.cc:8-45).
+ * indices: the rows colour by colour; color_offsets: n_colors + 1 boundaries.
+ * Results are bit-identical to the reference's.  The colouring must be valid
+ * (no entry joins two rows of one colour; GPR_EINVAL otherwise).  Matrix
+ * arrays may be host or device memory; the layout is built on the host. */
+typedef struct gpr_symgs gpr_symgs;
+int gpr_symgs_create(int m, long long nnz, const int *any_Ap, const int *any_Aj,
+                     const float *any_Ax, const int *any_indices,
+                     const int *any_color_offsets, int n_colors, gpr_symgs **out);
+int gpr_symgs_destroy(gpr_symgs *h);
+/* `sweeps` sweeps in one persistent launch; x (in/out) and b host or device;
+ * loop_ms (may be NULL) receives the device time of the launch. */
+int gpr_symgs_apply(gpr_symgs *h, float *any_x, const float *any_b, int sweeps,
+                    double *loop_ms);
+/* SymGSSolver, src/symgs/symgs.h:28: one sweep, x updated in place. */
+int gpr_symgs_solver(int m, int nnz, const int *Ap, const int *Aj,
+                     const int *indices, const float *Ax, float *x,
+                     const float *b, const int *color_offsets, int n_colors);
+
 /* ---- graph construction on the GPU (inputs for the solvers) ------------- */
 /* Seeded RMAT pull graph (self-loops and duplicates removed, columns
  * ascending): fills device arrays allocated by the library; release with

@@ -81,6 +81,11 @@ def lib():
         L.orc_uniform_int.restype = None
         L.orc_uniform_int.argtypes = [C.c_longlong, C.c_ulonglong, C.c_int, _i32p]
         L.orc_num_threads.restype = C.c_int
+        L.orc_symgs_f32.restype = None
+        L.orc_symgs_f32.argtypes = [C.c_int, _i32p, _i32p, _f32p, _i32p, _i32p, C.c_int, _f32p,
+                                    _f32p]
+        L.orc_greedy_coloring.restype = C.c_int
+        L.orc_greedy_coloring.argtypes = [C.c_int, _i32p, _i32p, _i32p]
         L.orc_multigraph_size.restype = C.c_int
         L.orc_multigraph_size.argtypes = [C.c_int, C.c_int, C.c_int, C.c_ulonglong]
         L.orc_chung_lu_prefix.restype = None
@@ -275,6 +280,29 @@ def csr_from_pushes(m, row, col, wt, sorted=True, remove_selfloops=True, remove_
     return rowptr, c.astype(np.int32), w
 
 
+def greedy_coloring(rowptr, col):
+    """First-fit colouring in vertex order; returns (indices, color_offsets):
+    vertices sorted by colour (ties by id) and the colour boundaries, as the
+    reference's SymGS driver builds them (src/symgs/main.cc:36-46)."""
+    m = len(rowptr) - 1
+    colors = np.empty(m, dtype=np.int32)
+    nc = lib().orc_greedy_coloring(m, _c(rowptr), _c(col), colors)
+    indices = np.argsort(colors, kind="stable").astype(np.int32)
+    offsets = np.zeros(nc + 1, dtype=np.int32)
+    np.cumsum(np.bincount(colors, minlength=nc), out=offsets[1:])
+    return indices, offsets
+
+
+def symgs_f32(rowptr, col, vals, indices, color_offsets, x, b):
+    """One multicolour symmetric Gauss-Seidel sweep (src/symgs/verifier.cc
+    gs_serial order); returns the new x."""
+    m = len(rowptr) - 1
+    xo = np.ascontiguousarray(x, dtype=np.float32).copy()
+    lib().orc_symgs_f32(m, _c(rowptr), _c(col), _cf(vals), _c(indices), _c(color_offsets),
+                        len(color_offsets) - 1, xo, _cf(b))
+    return xo
+
+
 def transpose_csr(m, rowptr, col):
     """Out-CSR of a pull (in-)CSR, columns ascending: used for the push check."""
     rowptr = np.asarray(rowptr, dtype=np.int64)
@@ -313,6 +341,8 @@ def ref():
                                      C.POINTER(C.POINTER(C.c_int)), C.POINTER(C.POINTER(C.c_int)),
                                      C.POINTER(C.POINTER(C.c_int)), C.POINTER(C.POINTER(C.c_float))]
         R.ref_free.argtypes = [C.c_void_p]
+        R.ref_symgs_solver.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _i32p, _f32p, _f32p, _f32p,
+                                       _i32p, C.c_int]
         _REF = R
     return _REF
 
@@ -371,6 +401,18 @@ def ref_spmv_solver(Ap, Aj, Ax, x, y):
     with _CaptureStdout() as cap:
         ref().ref_spmv_solver(len(Ap) - 1, len(Aj), _c(Ap), _c(Aj), _cf(Ax), _cf(x), out)
     return out, cap.text
+
+
+def ref_symgs_solver(rowptr, col, vals, indices, color_offsets, x, b):
+    """The reference's OpenMP SymGSSolver (src/symgs/omp_base.cc); returns
+    (x, stdout)."""
+    R = ref()
+    xo = np.ascontiguousarray(x, dtype=np.float32).copy()
+    co = _c(color_offsets)
+    with _CaptureStdout() as cap:
+        R.ref_symgs_solver(len(rowptr) - 1, len(col), _c(rowptr), _c(col), _c(indices),
+                           _cf(vals), xo, _cf(b), co, len(co))
+    return xo, cap.text
 
 
 def ref_read_graph(path, symmetrize=False, transpose=False, sorted=True,

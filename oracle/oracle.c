@@ -538,3 +538,67 @@ void orc_multigraph_edges(int g, int m_g, int deg, unsigned long long seed,
         }
     }
 }
+
+/* ------------------------------------------------------------------------ */
+/* Symmetric Gauss-Seidel smoother, multicolour order (src/symgs/verifier.cc */
+/* :56-79 gs_serial and SymGSVerifier; src/symgs/omp_base.cc:8-45): colours  */
+/* 0..n-1 forward, then n-1..0 backward, rows of a colour in `indices`       */
+/* order; each row sums x[j]*Ax[jj] over its off-diagonal entries in CSR     */
+/* order (one rounded multiply and one rounded add per entry), takes the     */
+/* last diagonal entry as diag, and if diag != 0 sets                        */
+/* x[row] = (b[row] - rsum) / diag.                                          */
+/* ------------------------------------------------------------------------ */
+static void orc_gs_rows(const int *Ap, const int *Aj, const float *Ax, const int *indices,
+                        int begin, int end, float *x, const float *b)
+{
+    int i;
+    for (i = begin; i < end; i++) {
+        const int r = indices[i];
+        float rsum = 0.0f, diag = 0.0f;
+        int jj;
+        for (jj = Ap[r]; jj < Ap[r + 1]; jj++) {
+            const int j = Aj[jj];
+            if (j == r) diag = Ax[jj];
+            else {
+                const float p = x[j] * Ax[jj];
+                rsum = rsum + p;
+            }
+        }
+        if (diag != 0.0f) x[r] = (b[r] - rsum) / diag;
+    }
+}
+
+void orc_symgs_f32(int m, const int *Ap, const int *Aj, const float *Ax, const int *indices,
+                   const int *color_offsets, int ncolors, float *x, const float *b)
+{
+    int c;
+    (void)m;
+    for (c = 0; c < ncolors; c++)
+        orc_gs_rows(Ap, Aj, Ax, indices, color_offsets[c], color_offsets[c + 1], x, b);
+    for (c = ncolors; c > 0; c--)
+        orc_gs_rows(Ap, Aj, Ax, indices, color_offsets[c - 1], color_offsets[c], x, b);
+}
+
+/* First-fit greedy colouring in vertex order over the off-diagonal entries
+ * (a valid colouring of a structurally symmetric matrix's graph; the
+ * reference takes its colouring from its vertex-colouring kernel, src/vc).
+ * Returns the number of colours. */
+int orc_greedy_coloring(int m, const int *Ap, const int *Aj, int *colors)
+{
+    int v, nc = 0;
+    int *mark = (int *)malloc(sizeof(int) * ((size_t)m + 1));
+    for (v = 0; v < m; v++) colors[v] = -1;
+    for (v = 0; v <= m; v++) mark[v] = -1;
+    for (v = 0; v < m; v++) {
+        int jj, c = 0;
+        for (jj = Ap[v]; jj < Ap[v + 1]; jj++) {
+            const int u = Aj[jj];
+            if (u != v && colors[u] >= 0) mark[colors[u]] = v;
+        }
+        while (mark[c] == v) c++;
+        colors[v] = c;
+        if (c + 1 > nc) nc = c + 1;
+    }
+    free(mark);
+    return nc;
+}

@@ -9,10 +9,13 @@
  *   PRVerifier    src/pr/pr.h:24,      defined in src/pr/verifier.cc:10
  *   SpmvSolver    src/spmv/spmv.h:29,  defined in src/spmv/omp_base.cc:8
  *   SpmvVerifier  src/spmv/spmv.h:30,  defined in src/spmv/verifier.cc:24
+ *   SymGSSolver   src/symgs/symgs.h:28, defined in src/symgs/omp_base.cc:28
  *   read_graph    include/graph_io.h:280
  */
 #include "common.h"
 #include "graph_io.h"
+
+#include <vector>
 
 double gpr_ref_epsilon = 0.001;  // src/pr/pr.h:4
 int gpr_ref_max_iter = 30;       // src/pr/pr.h:5
@@ -26,6 +29,8 @@ void PRVerifier(int m, int *in_row_offsets, int *in_column_indices,
 void SpmvSolver(int m, int nnz, int *Ap, int *Aj, float *Ax, float *x, float *y);
 void SpmvVerifier(int m, int nnz, int *Ap, int *Aj, float *Ax, float *x,
                   float *y, float *test_y);
+void SymGSSolver(int m, int nnz, int *Ap, int *Aj, int *indices, ValueType *Ax, ValueType *x,
+                 ValueType *b, std::vector<int> color_offsets);
 
 extern "C" {
 
@@ -54,6 +59,15 @@ void ref_spmv_solver(int m, int nnz, int *Ap, int *Aj, float *Ax, float *x, floa
 void ref_spmv_verifier(int m, int nnz, int *Ap, int *Aj, float *Ax, float *x,
                        float *y, float *test_y) {
   SpmvVerifier(m, nnz, Ap, Aj, Ax, x, y, test_y);
+  fflush(stdout);
+}
+
+/* SymGSSolver (src/symgs/symgs.h:28, omp_base.cc:28-45) with the colour
+ * boundaries passed as an array of n_offsets ints. */
+void ref_symgs_solver(int m, int nnz, int *Ap, int *Aj, int *indices, float *Ax, float *x,
+                      float *b, int *color_offsets, int n_offsets) {
+  std::vector<int> co(color_offsets, color_offsets + n_offsets);
+  SymGSSolver(m, nnz, Ap, Aj, indices, Ax, x, b, co);
   fflush(stdout);
 }
 

@@ -18,7 +18,13 @@ Outputs (committed, so machines without the reference tree keep the pin):
   printed sweep counts on those graphs and on a seeded RMAT scale-10 graph,
   at its compiled-in constants (1e-3 / 30) and at 1e-4 / 100;
 * spmv.npz -- the reference's OpenMP SpmvSolver (src/spmv/omp_base.cc) on the
-  same CSRs with seeded x and y.
+  same CSRs with seeded x and y;
+* symgs.npz -- the reference's OpenMP SymGSSolver (src/symgs/omp_base.cc), one
+  multicolour sweep with a first-fit colouring, on the synthetic .mtx files
+  read as its driver reads them (src/symgs/main.cc:17: symmetrized, sorted,
+  self-loops kept, repeats removed) and on a 27-point stencil, seeded x and b.
+
+`python tests/golden/make_golden.py symgs` regenerates symgs.npz alone.
 """
 import itertools
 import os
@@ -79,7 +85,33 @@ def synthetic():
     return out
 
 
+def symgs_golden():
+    out = {}
+    cases = {}
+    for name in ("graph_small.mtx", "graph_dups.mtx", "graph_simple.mtx"):
+        rp, col, _, wt, _ = O.ref_read_graph(os.path.join(HERE, name), True, False, True, False,
+                                             True)
+        cases[name] = (rp, col, wt)
+    cases["stencil27_n9"] = O.stencil27(9)
+    for name, (rp, col, wt) in cases.items():
+        m = len(rp) - 1
+        idx, co = O.greedy_coloring(rp, col)
+        x = O.uniform_f32(m, 13)
+        b = O.uniform_f32(m, 14)
+        xr, _ = O.ref_symgs_solver(rp, col, wt, idx, co, x, b)
+        for k, v in (("Ap", rp), ("Aj", col), ("Ax", wt), ("indices", idx),
+                     ("color_offsets", co), ("x0", x), ("b", b), ("x", xr)):
+            out[f"{name}:{k}"] = v
+    np.savez_compressed(os.path.join(HERE, "symgs.npz"), **out)
+    print(f"wrote {len(out)} symgs arrays")
+
+
 def main():
+    if not O.ref_available():
+        sys.exit("oracle/_ref is not built (needs the reference tree)")
+    if sys.argv[1:] == ["symgs"]:
+        symgs_golden()
+        return
     if not O.ref_available():
         sys.exit("oracle/_ref is not built (needs the reference tree)")
     loader, pr, spmv = {}, {}, {}
@@ -130,6 +162,7 @@ def main():
     np.savez_compressed(os.path.join(HERE, "pr.npz"), **pr)
     np.savez_compressed(os.path.join(HERE, "spmv.npz"), **spmv)
     print(f"wrote {len(loader)} loader, {len(pr)} pr, {len(spmv)} spmv arrays")
+    symgs_golden()
 
 
 if __name__ == "__main__":

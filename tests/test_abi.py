@@ -10,7 +10,7 @@ import pytest
 
 from conftest import ROOT, has_gpu
 
-HEADERS = ["gpr.h", "gardenia_pr.h", "gardenia_spmv.h", "gardenia_graph_io.h"]
+HEADERS = ["gpr.h", "gardenia_pr.h", "gardenia_spmv.h", "gardenia_symgs.h", "gardenia_graph_io.h"]
 
 
 def declared_c_functions():
@@ -35,11 +35,13 @@ def test_every_declared_c_symbol_is_exported(G):
 
 def test_cpp_dropins_exported_with_reference_mangling(G):
     # The reference's own symbols (C++ linkage, src/pr/pr.h:23-24,
-    # src/spmv/spmv.h:29-30, include/graph_io.h:280).
+    # src/spmv/spmv.h:29-30, src/symgs/symgs.h:28-29, include/graph_io.h:280).
     syms = exported(G.LIB_PATH)
     for s in ["_Z8PRSolveriiPiS_S_S_S_Pf", "_Z10PRVerifieriPiS_S_S_S_Pfd",
               "_Z8PageRankiiPiS_S_Pf", "_Z10SpmvSolveriiPiS_PfS0_S0_",
-              "_Z12SpmvVerifieriiPiS_PfS0_S0_S0_", "_Z10read_graphiPPcRiS1_S1_RPiS3_S3_RPfbbbbb"]:
+              "_Z12SpmvVerifieriiPiS_PfS0_S0_S0_", "_Z10read_graphiPPcRiS1_S1_RPiS3_S3_RPfbbbbb",
+              "_Z11SymGSSolveriiPiS_S_PfS0_S0_St6vectorIiSaIiEE",
+              "_Z13SymGSVerifieriPiS_S_PfS0_S0_S0_St6vectorIiSaIiEE"]:
         assert s in syms, s
 
 

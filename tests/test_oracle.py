@@ -197,3 +197,15 @@ def test_parallel_parse_reproduces_reference_lists(G, O, loader_gold, name, ext,
                 assert np.array_equal(w, loader_gold[key + ":weight"]), key
             elif not rd:
                 assert same_weights_per_entry(rp, c, w, loader_gold[key + ":weight"]), key
+
+
+def test_symgs_restatement_bit_identical_to_reference(O):
+    # src/symgs/omp_base.cc SymGSSolver, one sweep, fixtures made by the reference
+    gold = np.load(os.path.join(GOLD, "symgs.npz"))
+    for g in graphs(gold):
+        a = {k: gold[f"{g}:{k}"] for k in ("Ap", "Aj", "Ax", "indices", "color_offsets", "x0",
+                                           "b", "x")}
+        idx, co = O.greedy_coloring(a["Ap"], a["Aj"])
+        assert np.array_equal(idx, a["indices"]) and np.array_equal(co, a["color_offsets"]), g
+        x = O.symgs_f32(a["Ap"], a["Aj"], a["Ax"], a["indices"], a["color_offsets"], a["x0"], a["b"])
+        assert np.array_equal(x, a["x"]), g
