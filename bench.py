@@ -125,6 +125,39 @@ def dist_setup():
     return world, rank, local
 
 
+def init_dist(world, local, use_cuda=True, timeout_s=120):
+    """One process per GPU (replicas): NCCL on GPUs, gloo on CPU; the group
+    carries only barriers and the max-over-ranks timings.  None at N = 1."""
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+    if use_cuda:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=timeout_s),
+                                device_id=torch.device("cuda", local))
+    else:
+        dist.init_process_group("gloo", timeout=datetime.timedelta(seconds=timeout_s))
+    return dist
+
+
+def max_over_ranks(x, dist, device=None):
+    """The largest x over all ranks (the timing of a multi-rank step)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_rate(world, units_per_rank, seconds):
+    """Whole-job rate of `world` replicas that each processed units_per_rank
+    in (at most) `seconds`."""
+    return world * units_per_rank / seconds
+
+
 def cpu_reference_sample(rp, col, od, sweeps, budget_s, min_calls=1):
     """Time the reference's OpenMP PRSolver (oracle/_ref) or, without it, the
     oracle port, on the full graph, `sweeps` sweeps per call."""
@@ -207,13 +240,7 @@ def run_ours(args):
     world, rank, local = dist_setup()
     torch.cuda.set_device(local)
     G.set_device(local)
-    dist = None
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+    dist = init_dist(world, local)
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
     t0 = time.time()
@@ -266,14 +293,10 @@ def run_ours(args):
     if dist:
         dist.barrier()
     clocks = sampler.stop()
-    ms = ev0.elapsed_time(ev1)
-    if dist:
-        t = torch.tensor([ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(ev0.elapsed_time(ev1), dist, dev)
     sweeps = sum(s.iterations for s in stats)
     launches = sum(s.gpu_launches for s in stats)
-    gteps = world * nnz * sweeps / (ms / 1e3) / 1e9
+    gteps = replica_rate(world, nnz * sweeps, ms / 1e3) / 1e9
     loop_ms = sum(s.loop_ms for s in stats) / len(stats)
     sweeps_per_solve = sweeps / len(stats)
     per_sweep = pr_bytes_per_sweep(m, nnz)
@@ -326,11 +349,8 @@ def run_ours(args):
             if i > 0:
                 e_sweeps += st.iterations
                 e_time += dt
-        if dist:
-            t = torch.tensor([e_time], device=dev, dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            e_time = float(t.item())
-        line["e2e"] = {"value": world * nnz * e_sweeps / e_time / 1e9, "unit": "GTEPS",
+        e_time = max_over_ranks(e_time, dist, dev)
+        line["e2e"] = {"value": replica_rate(world, nnz * e_sweeps, e_time) / 1e9, "unit": "GTEPS",
                        "h2d_bytes_per_step": 4 * (m + 1) + 4 * nnz + 4 * m + 4 * m,
                        "d2h_bytes_per_step": 4 * m, "ms_per_step": 1e3 * e_time / e2e_steps,
                        "call": "PageRank(m, nnz, row_offsets, column_indices, degree, scores) "
