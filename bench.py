@@ -362,6 +362,8 @@ def run_ours(args):
             (ms / args.steps) / line["forms"]["pr_bf16_refined"]["loop_ms"])
     if not args.no_multigraph:
         line["multigraph"] = multigraph_leg(G, torch, dev, stream, gteps / world, args)
+    if not args.no_forms:
+        line["ppr"] = ppr_leg(G, torch, dev, stream, args)
 
     if not args.no_spmv:
         line["spmv"] = spmv_leg(G, torch, dev, stream, args)
@@ -443,6 +445,52 @@ def forms_leg(G, torch, dev, g, m, nnz, plain_gteps, args):
                      "useful_edge_vector_gteps": nnz * float(it.sum()) / (st.loop_ms / 1e3) / 1e9,
                      "vs_plain_fp32": rate / plain_gteps, "max_final_residual": st.residual}
         del buf
+    return out
+
+
+PPR_SCALE, PPR_KS = 22, (8, 32, 128)
+
+
+def ppr_leg(G, torch, dev, stream, args):
+    """Batched personalized PageRank on its own configuration: RMAT scale 22,
+    edge factor 16 (same RMAT parameters), k = 8, 32 and 128 seed vectors,
+    each seed drawn uniformly (seeded), teleport mass on the seed, tol 1e-6
+    per vector, one persistent launch, FP32 and BF16 + FP32 refinement.
+    Rate: nnz x k x sweeps per second of the sweep loop (edge-vector pairs);
+    the plain FP32 single-vector GTEPS on the same graph is the comparison."""
+    csr = G.gen_rmat(PPR_SCALE, EDGE_FACTOR, seed=SEED, abc=ABC)
+    m, nnz = csr.m, csr.nnz
+    g = G.Graph(csr.rowptr, csr.col, csr.third, m=m, nnz=nnz, batched=True)
+    g.set_stream(stream.cuda_stream)
+    scores = torch.empty(m, dtype=torch.float32, device=dev)
+    best = None
+    for _ in range(4):
+        scores.fill_(float(np.float32(1.0) / np.float32(m)))
+        _, st = g.pagerank(scores, G.options(tol=TOL, max_iter=MAX_ITER, damping=DAMPING))
+        if best is None or st.loop_ms < best.loop_ms:
+            best = st
+    plain = nnz * best.iterations / (best.loop_ms / 1e3) / 1e9
+    out = {"workload": f"ppr_rmat{PPR_SCALE}_ef{EDGE_FACTOR}_tol1e-6", "m": m, "nnz": nnz,
+           "plain_fp32": {"sweeps": best.iterations, "loop_ms": best.loop_ms, "gteps": plain}}
+    rng = np.random.default_rng(22)
+    for k in PPR_KS:
+        seeds = rng.integers(0, m, k).astype(np.int32)
+        buf = torch.empty(m * k, dtype=torch.float32, device=dev)
+        for prec, tag in ((G.PREC_FP32, "fp32"), (G.PREC_BF16, "bf16_refined")):
+            bst = None
+            for _ in range(2):
+                _, it, st = g.ppr(seeds, out=buf, tol=TOL, max_iter=MAX_ITER, precision=prec)
+                if bst is None or st.loop_ms < bst[0].loop_ms:
+                    bst = (st, it)
+            st, it = bst
+            rate = nnz * k * st.iterations / (st.loop_ms / 1e3) / 1e9
+            out[f"k{k}_{tag}"] = {"sweeps": st.iterations, "refine_sweeps": st.refine_iterations,
+                                  "vector_sweeps_min": int(it.min()), "loop_ms": st.loop_ms,
+                                  "edge_vector_gteps": rate, "vs_plain_fp32": rate / plain,
+                                  "max_final_residual": st.residual}
+        del buf
+    g.close()
+    csr.close()
     return out
 
 
@@ -661,6 +709,24 @@ def profile_multigraph(args):
     return 0
 
 
+def profile_ppr(args):
+    """One batched PPR solve of --profile-ppr vectors, exactly --profile-solve
+    sweeps (tol 0) on the RMAT graph of --scale (for ncu)."""
+    import torch
+
+    import gardenia_ocl_b200 as G
+    csr = G.gen_rmat(args.scale, EDGE_FACTOR, seed=SEED, abc=ABC)
+    g = G.Graph(csr.rowptr, csr.col, csr.third, m=csr.m, nnz=csr.nnz, batched=True)
+    k = args.profile_ppr
+    seeds = np.random.default_rng(22).integers(0, csr.m, k).astype(np.int32)
+    buf = torch.empty(csr.m * k, dtype=torch.float32, device="cuda")
+    _, it, st = g.ppr(seeds, out=buf, tol=0.0, max_iter=args.profile_solve or 3)
+    log(json.dumps({"m": csr.m, "nnz": csr.nnz, "k": k, **st.as_dict()}))
+    g.close()
+    csr.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -687,9 +753,14 @@ def main():
     ap.add_argument("--profile-multigraph", type=int, default=0, metavar="GRAPHS",
                     help="build the first GRAPHS graphs of the multi-graph batch and run one "
                          "solve of --profile-solve sweeps (the case profiled with ncu)")
+    ap.add_argument("--profile-ppr", type=int, default=0, metavar="K",
+                    help="one batched PPR solve with K seed vectors and --profile-solve sweeps "
+                         "on the RMAT graph of --scale (the case profiled with ncu)")
     args = ap.parse_args()
     if args.profile_multigraph:
         return profile_multigraph(args)
+    if args.profile_ppr:
+        return profile_ppr(args)
     if args.profile_solve:
         return profile_solve(args)
     if args.warmup < 3:

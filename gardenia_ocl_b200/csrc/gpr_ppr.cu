@@ -54,7 +54,7 @@ struct PprArgs {
   int *iters;            // [K]
   unsigned *bar;         // [2] arrivals, generation
   int *status;           // [0] error flags, [1] sweeps, [2] any active
-  int *wq;               // [2] work-queue heads by parity
+  int *wq;               // [4] work-queue heads by parity: rows [0..1], chunks [2..3]
   float damp;
   double tol;
   int max_iter, batch, bar_expect;
@@ -201,7 +201,6 @@ __global__ void __launch_bounds__(kPprBlock) k_ppr(PprArgs a) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int g = lane / L, lq = lane % L;
   const int G = gridDim.x;
-  const int n_units = a.n_chunks + a.n_row_units;
   int it = 0;
   while (it < a.max_iter) {
     const T *cin = reinterpret_cast<const T *>((it & 1) ? a.c1 : a.c0);
@@ -216,13 +215,33 @@ __global__ void __launch_bounds__(kPprBlock) k_ppr(PprArgs a) {
     double err[C], dng[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) err[c] = dng[c] = 0.0;
+    // Chunks of long rows are taken one per grab (each is a long run of
+    // dependent gathers for a wide vector block), then rows in batches.
+    int chunk_next = 0, row_u0 = 0, row_u1 = 0;
     for (;;) {
-      int u0 = 0;
-      if (lane == 0) u0 = atomicAdd(a.wq + (it & 1), a.batch);
-      u0 = __shfl_sync(kFull, u0, 0);
-      if (u0 >= n_units) break;
-      const int u1 = min(u0 + a.batch, n_units);
-      for (int u = u0; u < u1; ++u) {
+      int u;
+      if (chunk_next >= 0) {
+        int c = 0;
+        if (lane == 0) c = atomicAdd(a.wq + 2 + (it & 1), 1);
+        c = __shfl_sync(kFull, c, 0);
+        if (c < a.n_chunks) {
+          u = c;
+        } else {
+          chunk_next = -1;
+          continue;
+        }
+      } else {
+        if (row_u0 >= row_u1) {
+          int u0 = 0;
+          if (lane == 0) u0 = atomicAdd(a.wq + (it & 1), a.batch);
+          u0 = __shfl_sync(kFull, u0, 0);
+          if (u0 >= a.n_row_units) break;
+          row_u0 = u0;
+          row_u1 = min(u0 + a.batch, a.n_row_units);
+        }
+        u = a.n_chunks + row_u0++;
+      }
+      {
         float acc[C];
 #pragma unroll
         for (int c = 0; c < C; ++c) acc[c] = 0.f;
@@ -360,6 +379,7 @@ __global__ void __launch_bounds__(kPprBlock) k_ppr(PprArgs a) {
         }
         a.status[2] = any != 0;
         atomicExch(a.wq + (it & 1), 0);
+        atomicExch(a.wq + 2 + (it & 1), 0);
         atomicExch(a.bar, 0u);
         __threadfence();
         atomicAdd(a.bar + 1, 1u);
@@ -618,9 +638,11 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
   const size_t smem = sizeof(double) * 2 * (kPprBlock / 32) * K;
   const int Lb = K <= 32 ? 8 : K / 4;
   const int R = 32 / Lb;
-  // Rows above 8 rounds of one sub-group are cut into 1024-edge chunks that
-  // the whole warp works on, so no unit runs far longer than another.
-  const int b_dmax = 8 * Lb, b_chunk = 1024;
+  // Rows above 8 rounds of one sub-group are cut into chunks that the whole
+  // warp works on, 8192 / L edges each (1024 for K <= 32, 256 for K = 128),
+  // so a chunk costs about the same number of dependent gather rounds for
+  // every K.
+  const int b_dmax = 8 * Lb, b_chunk = 8192 / Lb;
   GPR_TRY(build_chunk_table(g, b_dmax, b_chunk, st));
   const int n_row_units = (int)gpr::ceil_div((long long)L.n_nz - g->b_nlong, R);
   const long long units = (long long)g->b_nchunks + n_row_units;
@@ -663,7 +685,7 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
   GPR_TRY(B.get(&seeds_old, (size_t)k, "ppr seeds (input)"));
   GPR_TRY(B.get(&iters, (size_t)K, "ppr iterations"));
   GPR_TRY(B.get(&status, 4, "ppr status"));
-  GPR_TRY(B.get(&wq, 2, "ppr queue"));
+  GPR_TRY(B.get(&wq, 4, "ppr queues"));
   GPR_TRY(B.get(&cta_red, (size_t)2 * Gmax * K, "ppr cta sums"));
   GPR_TRY(B.get(&seed_red, (size_t)2 * K, "ppr seed sums"));
   GPR_TRY(B.get(&res_hist, (size_t)std::max(1, max_iter) * K, "ppr residuals"));
@@ -714,10 +736,10 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
   auto phase = [&](const PprKernels &kk, int G, double tol, int *sweeps,
                    std::vector<int> *it_out) -> int {
     a.tol = tol;
-    a.batch = (int)std::max<long long>(1, units / ((long long)G * (kPprBlock / 32) * 4));
+    a.batch = (int)std::max<long long>(1, n_row_units / ((long long)G * (kPprBlock / 32) * 4));
     a.bar_expect = G + (o.reserved[0] > 0 ? o.reserved[0] : 0);
     GPR_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 4, st));
-    GPR_CUDA(cudaMemsetAsync(wq, 0, sizeof(int) * 2, st));
+    GPR_CUDA(cudaMemsetAsync(wq, 0, sizeof(int) * 4, st));
     if (max_iter > 0) {
       void *args[] = {&a};
       GPR_CUDA(cudaLaunchCooperativeKernel(kk.solve, dim3(G), dim3(kPprBlock), args, smem, st));
