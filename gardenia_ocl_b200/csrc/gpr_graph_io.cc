@@ -192,9 +192,12 @@ void mtx2csr(const char *path, int &m, int &n, int &nnz, int *&rowptr, int *&col
     }
     if (num == 2) wt = 1;
     if (wt < 0) wt = -wt;
-    int s = src - 1, d = dst - 1;
-    if (!in_range(s, m) || !in_range(d, m)) bad(path, "index out of range");
-    add_edge(v, s, d, wt, symmetrize, transpose, true);
+    // decremented in place, as the reference does: a line that sets neither
+    // number repeats the previous edge decremented once more
+    --src;
+    --dst;
+    if (!in_range(src, m) || !in_range(dst, m)) bad(path, "index out of range");
+    add_edge(v, src, dst, wt, symmetrize, transpose, true);
   }
   fill_data(m, nnz, rowptr, col, w, v, symmetrize, sorted, rm_self, rm_dup);
 }
@@ -239,14 +242,14 @@ void gr2csr(const char *path, int &m, int &nnz, int *&rowptr, int *&col, WeightT
   while (p < pe && *p != ' ' && *p != '\t') ++p;
   if (!parse_int(p, pe, &m) || !parse_int(p, pe, &nnz)) bad(path, "bad problem line");
   std::vector<std::vector<Edge>> v((size_t)m);
+  int src = 0, dst = 0;  // kept across lines: a missing number keeps its last value
   for (int i = 0; i < nnz; i++) {
     if (!R.line(&b, &e)) bad(path, "fewer arcs than announced");
     p = R.buf.data() + b;
     pe = R.buf.data() + e;
     if (p < pe && *p != 'a') printf("line %d\n", __LINE__);
     if (p < pe) ++p;
-    int src = 0, dst = 0;
-    if (!parse_int(p, pe, &src) || !parse_int(p, pe, &dst)) bad(path, "bad arc line");
+    if (parse_int(p, pe, &src)) parse_int(p, pe, &dst);
     --src;
     --dst;
     if (!in_range(src, m) || !in_range(dst, m)) bad(path, "index out of range");
@@ -329,7 +332,7 @@ inline void push_edge(Pushes &P, int src, int dst, float wt, bool symmetrize, bo
 
 struct ChunkResult {
   Pushes P;
-  int err = 0;          // 1 index out of range, 2 bad arc line, 3 irregular .mtx line
+  int err = 0;          // 1 index out of range, 3 a line the sequential reader must take
   long long lines = 0;  // lines parsed
 };
 
@@ -370,7 +373,7 @@ void parse_chunk(const std::string &buf, size_t cb, size_t ce, long long first_l
       if (p < pe) ++p;
       int src = 0, dst = 0;
       if (!parse_int(p, pe, &src) || !parse_int(p, pe, &dst)) {
-        out->err = 2;
+        out->err = 3;  // carries values over from the previous line: sequential reader
         return;
       }
       --src;
@@ -513,10 +516,6 @@ int parse_pushes(const char *path, bool symmetrize, bool transpose, int threads,
       *why = "index out of range";
       return -1;
     }
-    if (r.err == 2) {
-      *why = "bad arc line";
-      return -1;
-    }
   }
   size_t total = 0;
   for (auto &r : res) total += r.P.row.size();
@@ -535,38 +534,54 @@ int parse_pushes(const char *path, bool symmetrize, bool transpose, int threads,
   return 0;
 }
 
-// Sequential fallback: the reference-order reader, emitting pushes.
+// Sequential fallback for files with lines the reference reads with values
+// carried over from the previous line (.mtx and .gr): the numbers live across
+// lines and are decremented in place, as in graph_io.h:155-158 and :238-245.
 void parse_pushes_sequential(const char *path, bool symmetrize, bool transpose, int *m_out,
                              int *nnz_out, Pushes *out) {
+  const bool gr = strstr(path, ".mtx") == nullptr;
   Reader R;
   if (!R.load(path)) bad(path, "cannot open");
   size_t b, e;
   if (!R.line(&b, &e)) bad(path, "empty file");
-  while (b < e && R.buf[b] == '%')
+  while (b < e && R.buf[b] == (gr ? 'c' : '%'))
     if (!R.line(&b, &e)) bad(path, "missing size line");
   const char *p = R.buf.data() + b, *pe = R.buf.data() + e;
   int m = 0, n = 0, nnz = 0;
-  if (!parse_int(p, pe, &m) || !parse_int(p, pe, &n) || !parse_int(p, pe, &nnz))
+  if (gr) {
+    if (p < pe) ++p;
+    while (p < pe && (*p == ' ' || *p == '\t')) ++p;
+    while (p < pe && *p != ' ' && *p != '\t') ++p;
+    if (!parse_int(p, pe, &m) || !parse_int(p, pe, &nnz)) bad(path, "bad problem line");
+  } else if (!parse_int(p, pe, &m) || !parse_int(p, pe, &n) || !parse_int(p, pe, &nnz)) {
     bad(path, "bad size line");
+  }
   int src = 0, dst = 0;
   WeightT wt = 1.0f;
   for (int i = 0; i < nnz; i++) {
     if (!R.line(&b, &e)) bad(path, "fewer entries than announced");
     p = R.buf.data() + b;
     pe = R.buf.data() + e;
-    int num = 0;
-    if (parse_int(p, pe, &src)) {
-      ++num;
-      if (parse_int(p, pe, &dst)) {
+    if (gr) {
+      if (p < pe) ++p;
+      if (parse_int(p, pe, &src)) parse_int(p, pe, &dst);
+      wt = 1.0f;
+    } else {
+      int num = 0;
+      if (parse_int(p, pe, &src)) {
         ++num;
-        if (parse_float(p, pe, &wt)) ++num;
+        if (parse_int(p, pe, &dst)) {
+          ++num;
+          if (parse_float(p, pe, &wt)) ++num;
+        }
       }
+      if (num == 2) wt = 1;
+      if (wt < 0) wt = -wt;
     }
-    if (num == 2) wt = 1;
-    if (wt < 0) wt = -wt;
-    const int s = src - 1, d = dst - 1;
-    if (!in_range(s, m) || !in_range(d, m)) bad(path, "index out of range");
-    push_edge(*out, s, d, wt, symmetrize, transpose, true);
+    --src;
+    --dst;
+    if (!in_range(src, m) || !in_range(dst, m)) bad(path, "index out of range");
+    push_edge(*out, src, dst, wt, symmetrize, transpose, !gr);
   }
   *m_out = m;
   *nnz_out = nnz;

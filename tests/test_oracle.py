@@ -209,3 +209,30 @@ def test_symgs_restatement_bit_identical_to_reference(O):
         assert np.array_equal(idx, a["indices"]) and np.array_equal(co, a["color_offsets"]), g
         x = O.symgs_f32(a["Ap"], a["Aj"], a["Ax"], a["indices"], a["color_offsets"], a["x0"], a["b"])
         assert np.array_equal(x, a["x"]), g
+
+
+@pytest.mark.parametrize("ext", [".mtx", ".gr"])
+def test_parse_falls_back_on_irregular_lines(G, O, tmp_path, ext):
+    # An entry line with missing numbers makes the reference reuse the values
+    # left by the previous line -- already decremented in place, so they are
+    # decremented once more (graph_io.h:155-158, :238-245).  The parallel
+    # parser hands such files to the sequential reader, which reproduces it.
+    p = tmp_path / ("irregular" + ext)
+    if ext == ".mtx":
+        p.write_text("%%MatrixMarket matrix coordinate real general\n5 5 6\n1 2 0.5\n3 4\n"
+                     "\n4 5 -2\n5 1 1.5\n3 3 1\n")
+    else:
+        p.write_text("p sp 5 6\na 1 2 1\na 3 4 1\na\na 4 5 1\na 5 1 1\na 3 3 1\n")
+    m, nnz, row, col, wt = G.parse_edges(str(p), threads=4)
+    assert (m, nnz) == (5, 6) and len(row) == 6
+    # the line without numbers repeats the previous edge decremented again
+    assert list(zip(row, col)) == [(0, 1), (2, 3), (1, 2), (3, 4), (4, 0), (2, 2)]
+    if ext == ".mtx":
+        assert list(wt) == [0.5, 1.0, 1.0, 2.0, 1.5, 1.0]
+    for fl in itertools.product([False, True], repeat=3):
+        mm, nz, rp_ref, col_ref, deg, w_ref = G.read_graph(str(p), False, False, *fl)
+        rp, c, w = O.csr_from_pushes(m, row, col, wt, *fl)
+        assert np.array_equal(rp, rp_ref) and np.array_equal(c, col_ref)
+        if O.ref_available():  # the reference's own loader on the same file
+            rr, cr, _, wr, _ = O.ref_read_graph(str(p), False, False, *fl)
+            assert np.array_equal(rp, rr) and np.array_equal(c, cr)
