@@ -37,6 +37,19 @@ _f64p = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 KDAMP = np.float32(0.85)  # include/common.h:18
 
 
+def reference_root() -> str:
+    """The reference tree the recipe in oracle/Makefile compiles from: its
+    REF_ROOT (environment first, then the Makefile's default)."""
+    env = os.environ.get("REF_ROOT")
+    if env:
+        return env
+    with open(os.path.join(_HERE, "Makefile")) as f:
+        for line in f:
+            if line.startswith("REF_ROOT ?="):
+                return line.split("?=", 1)[1].strip()
+    return ""
+
+
 def build() -> None:
     """Compile liboracle.so (and _ref when the reference tree is present)."""
     subprocess.run(["make", "-s", "-C", _HERE], check=True)

@@ -212,7 +212,8 @@ float orc_max_rel_err_f32(const float *a, const float *b, long long n)
 }
 
 /* ------------------------------------------------------------------------ */
-/* Batched personalized PageRank (north-star extension; no reference file). */
+/* Batched personalized PageRank (no reference file: the reference computes
+ * one global PageRank). */
 /* For each vector q with seed s_q:                                          */
 /*   x_new[v] = d * sum_{u in in(v)} x[u]/outdeg[u]                          */
 /*            + [v == s_q] * ((1 - d) + d * dangling_q)                      */

@@ -37,7 +37,7 @@ ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 import oracle as O  # noqa: E402
 
-REF_DATA = "/root/reference/datasets"
+REF_DATA = os.path.join(O.reference_root(), "datasets")
 FLAGS = list(itertools.product([False, True], repeat=5))  # sym, trans, sorted, selfloops, dups
 
 

@@ -14,8 +14,10 @@ import pytest
 
 from conftest import ROOT
 
+import oracle  # noqa: E402  (on sys.path through conftest)
+
 GOLD = os.path.join(ROOT, "tests", "golden")
-REF_DATA = "/root/reference/datasets"
+REF_DATA = os.path.join(oracle.reference_root(), "datasets")
 
 
 @pytest.fixture(scope="module")
