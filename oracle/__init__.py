@@ -428,6 +428,57 @@ def ref_symgs_solver(rowptr, col, vals, indices, color_offsets, x, b):
     return xo, cap.text
 
 
+_REF_GPU = {}
+
+
+def ref_gpu_available(name="gather") -> bool:
+    """The reference's own CUDA solver `name` (gather, gather_warp, spmv_base),
+    recompiled for sm_100a into oracle/_ref."""
+    return os.path.exists(os.path.join(_HERE, "_ref", f"libgardenia_ref_{name}.so"))
+
+
+def _ref_gpu(name):
+    if name not in _REF_GPU:
+        R = C.CDLL(os.path.join(_HERE, "_ref", f"libgardenia_ref_{name}.so"))
+        R.ref_set_constants.argtypes = [C.c_double, C.c_int]
+        if name.startswith("gather"):
+            R.ref_gpu_pr_solver.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _i32p, _f32p]
+        else:
+            R.ref_gpu_spmv_solver.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f32p, _f32p, _f32p]
+        _REF_GPU[name] = R
+    return _REF_GPU[name]
+
+
+def _runtime_ms(text):
+    import re
+    mt = re.search(r"runtime \[[^\]]*\] = ([0-9.]+) ms", text)
+    return float(mt.group(1)) if mt else float("nan")
+
+
+def ref_gpu_pr_solver(name, rowptr, col, outdeg, scores=None, tol=1e-3, max_iter=30):
+    """The reference's CUDA PRSolver (src/pr/gather.cu or gather_warp.cu) on the
+    GPU: returns (scores, sweeps, runtime_ms of its own Timer, stdout)."""
+    import re
+    R = _ref_gpu(name)
+    m = len(rowptr) - 1
+    s = (np.full(m, np.float32(1.0) / np.float32(m), dtype=np.float32) if scores is None
+         else np.ascontiguousarray(scores, dtype=np.float32).copy())
+    R.ref_set_constants(float(tol), int(max_iter))
+    with _CaptureStdout() as cap:
+        R.ref_gpu_pr_solver(m, len(col), _c(rowptr), _c(col), _c(outdeg), s)
+    it = re.search(r"iterations = (\d+)\.", cap.text)
+    return s, int(it.group(1)) if it else -1, _runtime_ms(cap.text), cap.text
+
+
+def ref_gpu_spmv_solver(Ap, Aj, Ax, x, y):
+    """The reference's CUDA SpmvSolver (src/spmv/base.cu): returns (y, runtime_ms)."""
+    R = _ref_gpu("spmv_base")
+    yo = np.ascontiguousarray(y, dtype=np.float32).copy()
+    with _CaptureStdout() as cap:
+        R.ref_gpu_spmv_solver(len(Ap) - 1, len(Aj), _c(Ap), _c(Aj), _cf(Ax), _cf(x), yo)
+    return yo, _runtime_ms(cap.text)
+
+
 def ref_read_graph(path, symmetrize=False, transpose=False, sorted=True,
                    remove_selfloops=True, remove_redundents=True):
     """The reference loader (include/graph_io.h:280).  Returns
