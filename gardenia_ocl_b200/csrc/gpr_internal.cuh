@@ -177,6 +177,13 @@ struct gpr_graph {
   // b_chunk-edge chunks), built on first use for a given (b_dmax, b_chunk).
   int *b_cbeg = nullptr, *b_crow = nullptr;
   int b_nlong = -1, b_nchunks = 0, b_dmax = 0, b_chunk = 0;
+  // Chunk descriptors (int4 per chunk) and the packet table (first unit of
+  // each of b_npk packets), rebuilt with the chunk table or for another
+  // packet count b_pk_want.
+  void *b_cdesc = nullptr;
+  int *b_pk = nullptr;
+  int b_npk = -1;
+  long long b_pk_want = 0;
   // Push solver: edges sorted by source and the per-vertex accumulators,
   // built on first use.
   int *push_src = nullptr, *push_dst = nullptr;

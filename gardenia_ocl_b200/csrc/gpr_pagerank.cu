@@ -577,6 +577,8 @@ void destroy(gpr_graph *g) {
   gpr::dfree(g->wq);
   gpr::dfree(g->b_cbeg);
   gpr::dfree(g->b_crow);
+  gpr::dfree(g->b_cdesc);
+  gpr::dfree(g->b_pk);
   gpr::dfree(g->push_src);
   gpr::dfree(g->push_dst);
   gpr::dfree(g->push_sum);

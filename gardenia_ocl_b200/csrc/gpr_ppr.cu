@@ -14,9 +14,9 @@
 // row m is a zero sentinel), K = the vector count rounded up to 8..128.  One
 // gather of an in-neighbour's row serves all K vectors, so the 4-byte index
 // stream and the per-request cost are shared by K edge-vector pairs.
-//   lanes per row L = 8 (K <= 32) or K / 4, rows per warp R = 32 / L,
-//   components per lane C = K / L <= 4 (contiguous, one vector load per
-//   gather).
+//   lanes per row L = K / 4, rows per warp R = 32 / L, components per lane
+//   C = 4 (contiguous, one vector load per gather), so one warp-wide load
+//   instruction serves R rows and 8 gathers per lane are in flight.
 // Rows with in-degree 0 hold x = 0 except at seeds, so only rows with
 // in-edges and the k seed rows are updated.  Rows above chunk_min in-edges
 // are cut into chunks whose K-wide partial sums the last arriving warp adds
@@ -39,8 +39,10 @@ constexpr unsigned kFull = 0xffffffffu;
 constexpr int kPprBlock = 256;
 
 struct PprArgs {
-  int m, n_long, n_nz, n_chunks, chunk, k, n_row_units;
-  const int *csr_ptr, *csr_col, *row_cbeg, *chunk_row, *outdeg;
+  int m, n_long, n_nz, n_chunks, k, n_pk;
+  const int *csr_ptr, *csr_col, *row_cbeg, *outdeg;
+  const int4 *cdesc;     // [n_chunks] {row, first edge, end edge, first chunk of the row or -1}
+  const int *pk;         // [n_pk + 1] first unit of each packet
   float *x;              // [m][K]
   void *c0, *c1;         // [m+1][K] of T
   float *partial;        // [n_chunks][K]
@@ -54,21 +56,31 @@ struct PprArgs {
   int *iters;            // [K]
   unsigned *bar;         // [2] arrivals, generation
   int *status;           // [0] error flags, [1] sweeps, [2] any active
-  int *wq;               // [4] work-queue heads by parity: rows [0..1], chunks [2..3]
+  int *wq;               // [2] packet-queue heads by sweep parity
   float damp;
   double tol;
-  int max_iter, batch, bar_expect;
+  int max_iter, bar_expect;
   long long timeout_ns;
 };
 
-// Lanes per row L, rows per warp R, components per lane C (<= 4, so one
-// gather is at most a 16-byte load): K=8 -> 8x4x1, 16 -> 8x4x2, 32 -> 8x4x4,
-// 64 -> 16x2x4, 128 -> 32x1x4.
+// Lanes per row L = K / 4, rows per warp R = 32 / L, components per lane
+// C = 4 (one 16-byte FP32 or 8-byte BF16 load per gather): K=8 -> 2x16,
+// 16 -> 4x8, 32 -> 8x4, 64 -> 16x2, 128 -> 32x1.  Each lane loads P column
+// indices per round, so a sub-group covers E = L * P >= 8 edges per round and
+// every lane has 8 gathers in flight: P = 4, 2, 1, 1, 1.
 template <int K>
 struct Shape {
-  static constexpr int L = K <= 32 ? 8 : K / 4;
+  static constexpr int L = K / 4;
   static constexpr int R = 32 / L;
-  static constexpr int C = K / L;
+  static constexpr int C = 4;
+  static constexpr int P = L >= 8 ? 1 : 8 / L;
+  static constexpr int E = L * P;
+  // Early fetch: each row's scores and out-degree (and the next row group's
+  // offsets) are loaded before its gathers.  It pays where a warp updates
+  // several rows at once (K <= 32: 4-16 rows per warp; measured on RMAT s22
+  // +15% at K = 8, +8% at K = 32); at K >= 64 the extra registers cost more
+  // occupancy than the overlap gains (-28% at K = 128).
+  static constexpr bool early = K <= 32;
 };
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
@@ -131,33 +143,60 @@ __device__ __forceinline__ bool is_active(const unsigned (&act)[4], int q) {
 }
 
 // Sums in-neighbour rows over `niter` rounds; niter is warp-uniform.  In
-// round j this lane's sub-group covers edges [first + j*stride, +L) clipped
-// to `end`: each lane loads one index, the sub-group broadcasts them, and
-// every lane gathers its C components of each row.  Lanes past their
-// sub-group's end (or with no live component) gather the zero sentinel row,
-// so every shuffle runs on the full warp.
+// round j this lane's sub-group covers edges [first + j*stride, +E) clipped
+// to `end`: lane lq holds the indices of edges lq + p*L (p < P), the
+// sub-group broadcasts them, and every lane gathers its C components of each
+// row.  Edges past the sub-group's end (or lanes with no live component)
+// gather the zero sentinel row, so every shuffle runs on the full warp.
 template <int K, typename T>
 __device__ __forceinline__ void gather_edges(const PprArgs &a, const T *cin, long long first,
                                              long long end, long long stride, int niter, int lq,
                                              bool live, float (&acc)[Shape<K>::C]) {
-  constexpr int L = Shape<K>::L, C = Shape<K>::C;
-  int nxt = (niter > 0 && first + lq < end) ? ld_idx(a.csr_col + first + lq) : a.m;
+  constexpr int L = Shape<K>::L, C = Shape<K>::C, P = Shape<K>::P, E = Shape<K>::E;
+  constexpr int UB = 8;  // gathers in flight per lane
+  int nxt[P];
+#pragma unroll
+  for (int p = 0; p < P; ++p)
+    nxt[p] = (niter > 0 && first + lq + p * L < end) ? ld_idx(a.csr_col + first + lq + p * L) : a.m;
   for (int j = 0; j < niter; ++j) {
     const long long eb = first + (long long)j * stride;
-    const int my = nxt;
-    // next round's indices are in flight while this round gathers
-    nxt = (j + 1 < niter && eb + stride + lq < end) ? ld_idx(a.csr_col + eb + stride + lq) : a.m;
-    const int ng = (int)max(0LL, min((long long)L, end - eb));
+    int my[P];
+#pragma unroll
+    for (int p = 0; p < P; ++p) {
+      my[p] = nxt[p];
+      // next round's indices are in flight while this round gathers
+      const long long en = eb + stride + lq + p * L;
+      nxt[p] = (j + 1 < niter && en < end) ? ld_idx(a.csr_col + en) : a.m;
+    }
+    const int ng = (int)max(0LL, min((long long)E, end - eb));
     const int nmax = (int)__reduce_max_sync(kFull, (unsigned)ng);
-    // UB = 8 gathers in flight per lane (up to 32 floats of row data).
-    constexpr int UB = 8;
-    for (int t0 = 0; t0 < nmax; t0 += UB) {
+    if constexpr (P == 1) {
+      for (int t0 = 0; t0 < nmax; t0 += UB) {
+        float v[UB][C];
+#pragma unroll
+        for (int t = 0; t < UB; ++t) {
+          const int u = __shfl_sync(kFull, my[0], (t0 + t) & (L - 1), L);
+          const int uu = (t0 + t < ng && live) ? u : a.m;
+          load_row<C>(cin + (size_t)uu * K + lq * C, v[t]);
+        }
+#pragma unroll
+        for (int t = 0; t < UB; ++t)
+#pragma unroll
+          for (int c = 0; c < C; ++c) acc[c] += v[t][c];
+      }
+    } else {
+      static_assert(E == UB, "one block of gathers per round");
       float v[UB][C];
 #pragma unroll
       for (int t = 0; t < UB; ++t) {
-        const int u = __shfl_sync(kFull, my, (t0 + t) & (L - 1), L);
-        const int uu = (t0 + t < ng && live) ? u : a.m;
-        load_row<C>(cin + (size_t)uu * K + lq * C, v[t]);
+        const int u = __shfl_sync(kFull, my[t / L], t % L, L);
+        const int uu = (t < ng && live) ? u : a.m;
+        if (t < nmax) {
+          load_row<C>(cin + (size_t)uu * K + lq * C, v[t]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < C; ++c) v[t][c] = 0.f;
+        }
       }
 #pragma unroll
       for (int t = 0; t < UB; ++t)
@@ -167,25 +206,38 @@ __device__ __forceinline__ void gather_edges(const PprArgs &a, const T *cin, lon
   }
 }
 
-// Update of row v from its pulled sums (acc) for this lane's components.
+// Out-degree and current scores (this lane's C components) of row v, issued
+// before the row's gathers so that they are in flight together.
+template <int K>
+__device__ __forceinline__ void row_fetch(const PprArgs &a, int v, int lq, int &od,
+                                          float (&xo)[Shape<K>::C]) {
+  static_assert(Shape<K>::C == 4, "one 16-byte load of x");
+  asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(od) : "l"(a.outdeg + v));
+  asm volatile("ld.global.v4.f32 {%0,%1,%2,%3}, [%4];"
+               : "=f"(xo[0]), "=f"(xo[1]), "=f"(xo[2]), "=f"(xo[3])
+               : "l"(a.x + (size_t)v * K + lq * 4));
+}
+
+// Update of row v from its pulled sums (acc) for this lane's components;
+// od and xo from row_fetch, sd the lane's seed vertices.
 template <int K, typename T>
 __device__ __forceinline__ void row_update(const PprArgs &a, T *cout, int v, int lq,
                                            const unsigned (&act)[4], const double *dang_cur,
-                                           const float (&acc)[Shape<K>::C],
+                                           const int (&sd)[Shape<K>::C],
+                                           const float (&acc)[Shape<K>::C], int od,
+                                           const float (&xo)[Shape<K>::C],
                                            double (&err)[Shape<K>::C], double (&dng)[Shape<K>::C]) {
   constexpr int C = Shape<K>::C;
-  const int od = a.outdeg[v];
   const float inv = od > 0 ? 1.0f / (float)od : 0.f;
 #pragma unroll
   for (int c = 0; c < C; ++c) {
     const int q = lq * C + c;
     if (!is_active(act, q)) continue;
     float xn = a.damp * acc[c];
-    if (a.seed[q] == v) xn += (float)((1.0 - (double)a.damp) + (double)a.damp * dang_cur[q]);
+    if (sd[c] == v) xn += (float)((1.0 - (double)a.damp) + (double)a.damp * dang_cur[q]);
     const size_t o = (size_t)v * K + q;
-    const float xo = a.x[o];
     a.x[o] = xn;
-    err[c] += fabs((double)xn - (double)xo);
+    err[c] += fabs((double)xn - (double)xo[c]);
     store_c(cout + o, od > 0 ? xn * inv : 0.f);
     if (od == 0) dng[c] += (double)xn;
   }
@@ -193,7 +245,7 @@ __device__ __forceinline__ void row_update(const PprArgs &a, T *cout, int v, int
 
 template <int K, typename T>
 __global__ void __launch_bounds__(kPprBlock) k_ppr(PprArgs a) {
-  constexpr int L = Shape<K>::L, R = Shape<K>::R, C = Shape<K>::C;
+  constexpr int L = Shape<K>::L, R = Shape<K>::R, C = Shape<K>::C, E = Shape<K>::E;
   extern __shared__ double s_red[];  // [2][warps][K]
   __shared__ unsigned s_act[4];
   __shared__ int s_state;
@@ -201,6 +253,9 @@ __global__ void __launch_bounds__(kPprBlock) k_ppr(PprArgs a) {
   const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
   const int g = lane / L, lq = lane % L;
   const int G = gridDim.x;
+  int sd[C];  // seed vertices of this lane's components (-1: padding)
+#pragma unroll
+  for (int c = 0; c < C; ++c) sd[c] = a.seed[lq * C + c];
   int it = 0;
   while (it < a.max_iter) {
     const T *cin = reinterpret_cast<const T *>((it & 1) ? a.c1 : a.c0);
@@ -215,89 +270,96 @@ __global__ void __launch_bounds__(kPprBlock) k_ppr(PprArgs a) {
     double err[C], dng[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) err[c] = dng[c] = 0.0;
-    // Chunks of long rows are taken one per grab (each is a long run of
-    // dependent gathers for a wide vector block), then rows in batches.
-    int chunk_next = 0, row_u0 = 0, row_u1 = 0;
+    // Warps take packets (runs of units of about equal cost) from one queue;
+    // units [0, n_chunks) are chunks of long rows, the rest groups of R rows.
     for (;;) {
-      int u;
-      if (chunk_next >= 0) {
-        int c = 0;
-        if (lane == 0) c = atomicAdd(a.wq + 2 + (it & 1), 1);
-        c = __shfl_sync(kFull, c, 0);
-        if (c < a.n_chunks) {
-          u = c;
-        } else {
-          chunk_next = -1;
-          continue;
-        }
-      } else {
-        if (row_u0 >= row_u1) {
-          int u0 = 0;
-          if (lane == 0) u0 = atomicAdd(a.wq + (it & 1), a.batch);
-          u0 = __shfl_sync(kFull, u0, 0);
-          if (u0 >= a.n_row_units) break;
-          row_u0 = u0;
-          row_u1 = min(u0 + a.batch, a.n_row_units);
-        }
-        u = a.n_chunks + row_u0++;
-      }
-      {
-        float acc[C];
+      int p = 0;
+      if (lane == 0) p = atomicAdd(a.wq + (it & 1), 1);
+      p = __shfl_sync(kFull, p, 0);
+      if (p >= a.n_pk) break;
+      const int u1 = __ldg(a.pk + p + 1);
+      int u = __ldg(a.pk + p);
+      for (; u < u1 && u < a.n_chunks; ++u) {
+        float acc[C], xo[C];
+        int od = 0;
 #pragma unroll
         for (int c = 0; c < C; ++c) acc[c] = 0.f;
-        if (u < a.n_chunks) {
-          const int r = a.chunk_row[u];
-          const int cb = a.row_cbeg[r], nc = a.row_cbeg[r + 1] - cb;
-          const long long b = a.csr_ptr[r] + (long long)(u - cb) * a.chunk;
-          const long long e = min(b + (long long)a.chunk, (long long)a.csr_ptr[r + 1]);
-          const int niter = (int)gpr::ceil_div(e - b, (long long)R * L);
-          gather_edges<K, T>(a, cin, b + (long long)g * L, e, (long long)R * L, niter, lq, live,
-                             acc);
+        const int4 d = __ldg(a.cdesc + u);
+        const int r = d.x, cb = d.w;
+        const long long b = d.y, e = d.z;
+        if (Shape<K>::early && cb < 0) row_fetch<K>(a, r, lq, od, xo);  // the row's only chunk
+        const int niter = (int)gpr::ceil_div(e - b, (long long)R * E);
+        gather_edges<K, T>(a, cin, b + (long long)g * E, e, (long long)R * E, niter, lq, live,
+                           acc);
 #pragma unroll
-          for (int o = L; o < 32; o <<= 1)
+        for (int o = L; o < 32; o <<= 1)
 #pragma unroll
-            for (int c = 0; c < C; ++c) acc[c] += __shfl_xor_sync(kFull, acc[c], o);
-          if (nc == 1) {
-            if (g == 0) row_update<K, T>(a, cout, r, lq, act, dang_cur, acc, err, dng);
-            continue;
-          }
-          if (g == 0)
+          for (int c = 0; c < C; ++c) acc[c] += __shfl_xor_sync(kFull, acc[c], o);
+        if (cb < 0) {
+          if (!Shape<K>::early) row_fetch<K>(a, r, lq, od, xo);
+          if (g == 0) row_update<K, T>(a, cout, r, lq, act, dang_cur, sd, acc, od, xo, err, dng);
+          continue;
+        }
+        if (g == 0)
 #pragma unroll
-            for (int c = 0; c < C; ++c) a.partial[(size_t)u * K + lq * C + c] = acc[c];
-          __threadfence();
-          __syncwarp();
-          int last = 0;
-          if (lane == 0) last = atomicAdd(a.cnt + r, 1) == nc - 1;
-          last = __shfl_sync(kFull, last, 0);
-          if (!last) continue;
-          __threadfence();
-          // Sum the row's chunk partials in chunk order (sub-group 0).
+          for (int c = 0; c < C; ++c) a.partial[(size_t)u * K + lq * C + c] = acc[c];
+        __threadfence();
+        __syncwarp();
+        const int nc = __ldg(a.row_cbeg + r + 1) - cb;
+        int last = 0;
+        if (lane == 0) last = atomicAdd(a.cnt + r, 1) == nc - 1;
+        last = __shfl_sync(kFull, last, 0);
+        if (!last) continue;
+        __threadfence();
+        // Sum the row's chunk partials in chunk order (sub-group 0).
+        row_fetch<K>(a, r, lq, od, xo);
 #pragma unroll
-          for (int c = 0; c < C; ++c) acc[c] = 0.f;
-          for (int q = 0; q < nc; ++q)
+        for (int c = 0; c < C; ++c) acc[c] = 0.f;
+        for (int q = 0; q < nc; ++q)
 #pragma unroll
-            for (int c = 0; c < C; ++c) acc[c] += __ldcg(a.partial + (size_t)(cb + q) * K + lq * C + c);
-          if (lane == 0) atomicExch(a.cnt + r, 0);
-          if (g == 0) row_update<K, T>(a, cout, r, lq, act, dang_cur, acc, err, dng);
-        } else {
-          const int v = a.n_long + (u - a.n_chunks) * R + g;
-          long long e0 = 0, e1 = 0;
-          if (v < a.n_nz) {
-            e0 = a.csr_ptr[v];
-            e1 = a.csr_ptr[v + 1];
-          }
-          // Rows of one warp have nearly equal degrees (degree order); the
-          // sub-groups loop to the warp's longest row.
-          long long span = e1 - e0;
-#pragma unroll
-          for (int o = L; o < 32; o <<= 1) span = max(span, __shfl_xor_sync(kFull, span, o));
-          gather_edges<K, T>(a, cin, e0, e1, (long long)L, (int)gpr::ceil_div(span, L), lq,
-                             live && v < a.n_nz, acc);
-          if (v < a.n_nz) {
-            // edges past this row's end gathered the sentinel row (zeros)
-            row_update<K, T>(a, cout, v, lq, act, dang_cur, acc, err, dng);
+          for (int c = 0; c < C; ++c) acc[c] += __ldcg(a.partial + (size_t)(cb + q) * K + lq * C + c);
+        if (lane == 0) atomicExch(a.cnt + r, 0);
+        if (g == 0) row_update<K, T>(a, cout, r, lq, act, dang_cur, sd, acc, od, xo, err, dng);
+      }
+      if (u >= u1) continue;
+      // Row groups; with the early fetch, the next group's row offsets are
+      // in flight while this group gathers.
+      int v = a.n_long + (u - a.n_chunks) * R + g;
+      int p0 = 0, p1 = 0;
+      if (Shape<K>::early && v < a.n_nz) {
+        p0 = a.csr_ptr[v];
+        p1 = a.csr_ptr[v + 1];
+      }
+      for (; u < u1; ++u, v += R) {
+        const bool has = v < a.n_nz;
+        if (!Shape<K>::early) {
+          p0 = has ? a.csr_ptr[v] : 0;
+          p1 = has ? a.csr_ptr[v + 1] : 0;
+        }
+        const long long e0 = p0, e1 = p1;
+        if (Shape<K>::early) {
+          if (u + 1 < u1 && v + R < a.n_nz) {
+            asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(p0) : "l"(a.csr_ptr + v + R));
+            asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(p1) : "l"(a.csr_ptr + v + R + 1));
+          } else {
+            p0 = p1 = 0;
           }
         }
+        float acc[C], xo[C];
+        int od = 0;
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[c] = 0.f;
+        if (Shape<K>::early && has) row_fetch<K>(a, v, lq, od, xo);
+        // Rows of one warp have nearly equal degrees (degree order); the
+        // sub-groups loop to the warp's longest row.
+        long long span = e1 - e0;
+#pragma unroll
+        for (int o = L; o < 32; o <<= 1) span = max(span, __shfl_xor_sync(kFull, span, o));
+        gather_edges<K, T>(a, cin, e0, e1, (long long)E, (int)gpr::ceil_div(span, E), lq,
+                           live && has, acc);
+        // edges past this row's end gathered the sentinel row (zeros)
+        if (!Shape<K>::early && has) row_fetch<K>(a, v, lq, od, xo);
+        if (has) row_update<K, T>(a, cout, v, lq, act, dang_cur, sd, acc, od, xo, err, dng);
       }
     }
     // Seed rows without in-edges: only their teleport term changes.
@@ -379,7 +441,6 @@ __global__ void __launch_bounds__(kPprBlock) k_ppr(PprArgs a) {
         }
         a.status[2] = any != 0;
         atomicExch(a.wq + (it & 1), 0);
-        atomicExch(a.wq + 2 + (it & 1), 0);
         atomicExch(a.bar, 0u);
         __threadfence();
         atomicAdd(a.bar + 1, 1u);
@@ -494,12 +555,27 @@ __global__ void k_b_fill(int n, const int *__restrict__ cbeg, int *crow) {
     for (int c = cbeg[r] + lane; c < cbeg[r + 1]; c += 32) crow[c] = (int)r;
 }
 
+// Chunk descriptors {row, first edge, end edge, first chunk of the row, or
+// -1 when the row has one chunk}.
+__global__ void k_b_desc(int nch, int chunk, const int *__restrict__ ptr,
+                         const int *__restrict__ cbeg, const int *__restrict__ crow, int4 *desc) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nch) return;
+  const int r = crow[c], cb = cbeg[r], nc = cbeg[r + 1] - cb;
+  const int b = ptr[r] + (c - cb) * chunk;
+  desc[c] = make_int4(r, b, min(b + chunk, ptr[r + 1]), nc == 1 ? -1 : cb);
+}
+
 int build_chunk_table(gpr_graph *g, int dmax, int chunk, cudaStream_t st) {
   if (g->b_nlong >= 0 && g->b_dmax == dmax && g->b_chunk == chunk) return GPR_OK;
   gpr::dfree(g->b_cbeg);
   gpr::dfree(g->b_crow);
-  g->b_cbeg = g->b_crow = nullptr;
+  gpr::dfree(g->b_cdesc);
+  gpr::dfree(g->b_pk);
+  g->b_cbeg = g->b_crow = g->b_pk = nullptr;
+  g->b_cdesc = nullptr;
   g->b_nlong = -1;
+  g->b_npk = -1;
   const gpr::PrLayout &L = g->L;
   int *cnt = nullptr;
   GPR_TRY(gpr::dalloc(&cnt, 1, "chunk count"));
@@ -537,6 +613,11 @@ int build_chunk_table(gpr_graph *g, int dmax, int chunk, cudaStream_t st) {
     if (gr > 148u * 32u) gr = 148u * 32u;
     k_b_fill<<<gr, 256, 0, st>>>(nlong, g->b_cbeg, g->b_crow);
   }
+  GPR_TRY(gpr::dalloc(reinterpret_cast<int **>(&g->b_cdesc), (size_t)std::max(1, nch) * 4,
+                      "batched chunk descriptors"));
+  if (nch > 0)
+    k_b_desc<<<(unsigned)gpr::ceil_div(nch, 256), 256, 0, st>>>(
+        nch, chunk, L.csr_ptr, g->b_cbeg, g->b_crow, reinterpret_cast<int4 *>(g->b_cdesc));
   GPR_CUDA(cudaGetLastError());
   GPR_CUDA(cudaStreamSynchronize(st));
   g->b_nlong = nlong;
@@ -544,6 +625,115 @@ int build_chunk_table(gpr_graph *g, int dmax, int chunk, cudaStream_t st) {
   g->b_dmax = dmax;
   g->b_chunk = chunk;
   return GPR_OK;
+}
+
+// ---- packets: runs of consecutive units of about equal cost -----------------
+// Cost of a unit in edge slots: a chunk's edges, or R times the first (widest)
+// row of a row group, plus kUnitCost for the per-unit latency (descriptor,
+// row offsets, score update).
+constexpr long long kUnitCost = 64;
+
+__global__ void k_pk_cost(int n_chunks, int n_units, int R, int n_long, int n_nz,
+                          const int4 *__restrict__ desc, const int *__restrict__ ptr,
+                          long long *cost) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u >= n_units) return;
+  long long c;
+  if (u < n_chunks) {
+    const int4 d = desc[u];
+    c = d.z - d.y;
+  } else {
+    const int v = n_long + (u - n_chunks) * R;
+    c = (long long)R * (ptr[v + 1] - ptr[v]);
+  }
+  cost[u] = c + kUnitCost;
+}
+
+__global__ void k_pk_flag(int n, const long long *__restrict__ excl, long long target, int *flag) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < n) flag[u] = (u == 0 || excl[u] / target != excl[u - 1] / target) ? 1 : 0;
+}
+
+__global__ void k_pk_emit(int n, const int *__restrict__ flag, const int *__restrict__ pos,
+                          int *pk) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < n && flag[u]) pk[pos[u]] = u;
+  if (u == n - 1) pk[pos[u] + flag[u]] = n;
+}
+
+// Cuts the units (chunks, then row groups of R rows) into about `want`
+// packets of equal cost; a unit above the target cost is a packet alone.
+// Cached per chunk table and `want`.
+int build_packets(gpr_graph *g, int R, long long want, cudaStream_t st) {
+  if (g->b_npk >= 0 && g->b_pk_want == want) return GPR_OK;
+  gpr::dfree(g->b_pk);
+  g->b_pk = nullptr;
+  g->b_npk = -1;
+  const gpr::PrLayout &L = g->L;
+  const int n_units = g->b_nchunks + (int)gpr::ceil_div((long long)L.n_nz - g->b_nlong, R);
+  if (n_units == 0) {
+    GPR_TRY(gpr::dalloc(&g->b_pk, 1, "ppr packets"));
+    GPR_CUDA(cudaMemsetAsync(g->b_pk, 0, sizeof(int), st));
+    g->b_npk = 0;
+    g->b_pk_want = want;
+    return GPR_OK;
+  }
+  long long *cost = nullptr, *excl = nullptr;
+  int *flag = nullptr, *pos = nullptr;
+  void *tmp = nullptr;
+  size_t tb1 = 0, tb2 = 0;
+  int rc = GPR_OK;
+  long long tail[2] = {0, 0};
+  int ftail[2] = {0, 0};
+  const unsigned nb = (unsigned)gpr::ceil_div(n_units, 256);
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, tb1, cost, excl, n_units, st);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb2, flag, pos, n_units, st);
+  if (e != cudaSuccess) goto cuda_fail;
+  if ((rc = gpr::dalloc(&cost, n_units, "packet costs")) != GPR_OK ||
+      (rc = gpr::dalloc(&excl, n_units, "packet prefix")) != GPR_OK ||
+      (rc = gpr::dalloc(&flag, n_units, "packet flags")) != GPR_OK ||
+      (rc = gpr::dalloc(&pos, n_units, "packet positions")) != GPR_OK ||
+      (rc = gpr::dmalloc(&tmp, std::max(tb1, tb2), "scan scratch")) != GPR_OK)
+    goto done;
+  k_pk_cost<<<nb, 256, 0, st>>>(g->b_nchunks, n_units, R, g->b_nlong, L.n_nz,
+                                reinterpret_cast<const int4 *>(g->b_cdesc), L.csr_ptr, cost);
+  e = cub::DeviceScan::ExclusiveSum(tmp, tb1, cost, excl, n_units, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&tail[0], excl + n_units - 1, sizeof(long long), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&tail[1], cost + n_units - 1, sizeof(long long), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) goto cuda_fail;
+  {
+    const long long target = std::max(1LL, gpr::ceil_div(tail[0] + tail[1], std::max(1LL, want)));
+    k_pk_flag<<<nb, 256, 0, st>>>(n_units, excl, target, flag);
+    e = cub::DeviceScan::ExclusiveSum(tmp, tb2, flag, pos, n_units, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&ftail[0], pos + n_units - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&ftail[1], flag + n_units - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) goto cuda_fail;
+    const int npk = ftail[0] + ftail[1];
+    if ((rc = gpr::dalloc(&g->b_pk, (size_t)npk + 1, "ppr packets")) != GPR_OK) goto done;
+    k_pk_emit<<<nb, 256, 0, st>>>(n_units, flag, pos, g->b_pk);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) goto cuda_fail;
+    g->b_npk = npk;
+    g->b_pk_want = want;
+  }
+  goto done;
+cuda_fail:
+  gpr::set_error("gpr_ppr packets: %s", cudaGetErrorString(e));
+  rc = GPR_ECUDA;
+done:
+  gpr::dfree(cost);
+  gpr::dfree(excl);
+  gpr::dfree(flag);
+  gpr::dfree(pos);
+  gpr::dfree(tmp);
+  return rc;
 }
 
 struct PprKernels {
@@ -636,16 +826,16 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
   int sms = 0;
   GPR_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device));
   const size_t smem = sizeof(double) * 2 * (kPprBlock / 32) * K;
-  const int Lb = K <= 32 ? 8 : K / 4;
-  const int R = 32 / Lb;
+  // The kernel's shape for this K (Shape<K>): L lanes per row, R rows per
+  // warp, E edges per sub-group round.
+  const int Lb = K / 4, R = 32 / Lb, Eb = Lb >= 8 ? Lb : 8;
   // Rows above 8 rounds of one sub-group are cut into chunks that the whole
-  // warp works on, 8192 / L edges each (1024 for K <= 32, 256 for K = 128),
-  // so a chunk costs about the same number of dependent gather rounds for
-  // every K.
-  const int b_dmax = 8 * Lb, b_chunk = 8192 / Lb;
+  // warp works on, 8192 / L edges each (4096 for K = 8, 256 for K = 128), so
+  // a chunk costs every lane about 256 gathers for every K.
+  const int b_dmax = 8 * Eb, b_chunk = 8192 / Lb;
   GPR_TRY(build_chunk_table(g, b_dmax, b_chunk, st));
-  const int n_row_units = (int)gpr::ceil_div((long long)L.n_nz - g->b_nlong, R);
-  const long long units = (long long)g->b_nchunks + n_row_units;
+  const long long units =
+      (long long)g->b_nchunks + gpr::ceil_div((long long)L.n_nz - g->b_nlong, R);
   auto grid_of = [&](const PprKernels &kk, int *grid) -> int {
     int per_sm = 0;
     GPR_CUDA(cudaFuncSetAttribute(kk.solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
@@ -662,6 +852,10 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
   GPR_TRY(grid_of(k32, &G32));
   if (bf16) GPR_TRY(grid_of(k16, &G16));
   const int Gmax = std::max(G32, G16);
+  // About 32 packets per warp of the larger grid: fine enough that the end
+  // of a sweep is not held by one warp's last packet (measured on RMAT s22:
+  // 4 per warp loses 20-30% against 16-32; 64 and more cost queue traffic).
+  GPR_TRY(build_packets(g, R, (long long)Gmax * (kPprBlock / 32) * 32, st));
   Bufs B;
   float *x = nullptr, *partial = nullptr, *xout = nullptr;
   void *c0 = nullptr, *c1 = nullptr, *h0 = nullptr, *h1 = nullptr;
@@ -707,13 +901,13 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
   a.n_long = g->b_nlong;
   a.n_nz = L.n_nz;
   a.n_chunks = g->b_nchunks;
-  a.chunk = b_chunk;
   a.k = k;
-  a.n_row_units = n_row_units;
   a.csr_ptr = L.csr_ptr;
   a.csr_col = L.csr_col;
   a.row_cbeg = g->b_cbeg;
-  a.chunk_row = g->b_crow;
+  a.cdesc = reinterpret_cast<const int4 *>(g->b_cdesc);
+  a.pk = g->b_pk;
+  a.n_pk = g->b_npk;
   a.outdeg = L.outdeg;
   a.x = x;
   a.partial = partial;
@@ -736,7 +930,6 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
   auto phase = [&](const PprKernels &kk, int G, double tol, int *sweeps,
                    std::vector<int> *it_out) -> int {
     a.tol = tol;
-    a.batch = (int)std::max<long long>(1, n_row_units / ((long long)G * (kPprBlock / 32) * 4));
     a.bar_expect = G + (o.reserved[0] > 0 ? o.reserved[0] : 0);
     GPR_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 4, st));
     GPR_CUDA(cudaMemsetAsync(wq, 0, sizeof(int) * 4, st));
