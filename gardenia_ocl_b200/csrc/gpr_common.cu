@@ -1,7 +1,9 @@
 // Error slot, allocation helpers and small C-ABI entry points.
+#include <cub/cub.cuh>
 #include <stdarg.h>
 #include <string.h>
 
+#include <algorithm>
 #include <mutex>
 #include <unordered_map>
 #include <vector>
@@ -147,6 +149,86 @@ void dfree(void *p) {
 size_t cached_bytes() {
   std::lock_guard<std::mutex> lk(g_mu);
   return g_free_bytes;
+}
+
+namespace {
+__global__ void k_pk_flag(int n, const long long *__restrict__ excl, long long target, int *flag) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < n) flag[u] = (u == 0 || excl[u] / target != excl[u - 1] / target) ? 1 : 0;
+}
+
+__global__ void k_pk_emit(int n, const int *__restrict__ flag, const int *__restrict__ pos,
+                          int *pk) {
+  const int u = blockIdx.x * blockDim.x + threadIdx.x;
+  if (u < n && flag[u]) pk[pos[u]] = u;
+  if (u == n - 1) pk[pos[u] + flag[u]] = n;
+}
+}  // namespace
+
+int make_packets(long long *cost, int n_units, long long want, int **pk_out, int *npk_out,
+                 cudaStream_t st) {
+  *pk_out = nullptr;
+  *npk_out = 0;
+  if (n_units <= 0) {
+    GPR_TRY(dalloc(pk_out, 1, "packets"));
+    GPR_CUDA(cudaMemsetAsync(*pk_out, 0, sizeof(int), st));
+    return GPR_OK;
+  }
+  long long *excl = nullptr;
+  int *flag = nullptr, *pos = nullptr;
+  void *tmp = nullptr;
+  size_t tb1 = 0, tb2 = 0;
+  int rc = GPR_OK;
+  long long tail[2] = {0, 0};
+  int ftail[2] = {0, 0};
+  const unsigned nb = (unsigned)ceil_div(n_units, 256);
+  cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, tb1, cost, excl, n_units, st);
+  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb2, flag, pos, n_units, st);
+  if (e != cudaSuccess) goto cuda_fail;
+  if ((rc = dalloc(&excl, n_units, "packet prefix")) != GPR_OK ||
+      (rc = dalloc(&flag, n_units, "packet flags")) != GPR_OK ||
+      (rc = dalloc(&pos, n_units, "packet positions")) != GPR_OK ||
+      (rc = dmalloc(&tmp, std::max(tb1, tb2), "scan scratch")) != GPR_OK)
+    goto done;
+  e = cub::DeviceScan::ExclusiveSum(tmp, tb1, cost, excl, n_units, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&tail[0], excl + n_units - 1, sizeof(long long), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(&tail[1], cost + n_units - 1, sizeof(long long), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) goto cuda_fail;
+  {
+    const long long target = std::max(1LL, ceil_div(tail[0] + tail[1], std::max(1LL, want)));
+    k_pk_flag<<<nb, 256, 0, st>>>(n_units, excl, target, flag);
+    e = cub::DeviceScan::ExclusiveSum(tmp, tb2, flag, pos, n_units, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&ftail[0], pos + n_units - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(&ftail[1], flag + n_units - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) goto cuda_fail;
+    const int npk = ftail[0] + ftail[1];
+    if ((rc = dalloc(pk_out, (size_t)npk + 1, "packets")) != GPR_OK) goto done;
+    k_pk_emit<<<nb, 256, 0, st>>>(n_units, flag, pos, *pk_out);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) goto cuda_fail;
+    *npk_out = npk;
+  }
+  goto done;
+cuda_fail:
+  set_error("packet table: %s", cudaGetErrorString(e));
+  rc = GPR_ECUDA;
+done:
+  if (rc != GPR_OK) {
+    dfree(*pk_out);
+    *pk_out = nullptr;
+  }
+  dfree(excl);
+  dfree(flag);
+  dfree(pos);
+  dfree(tmp);
+  return rc;
 }
 
 bool is_device_ptr(const void *p) {

@@ -87,6 +87,14 @@ __host__ __device__ inline int slice_class(const PrClasses &c, int s) {
   return k;
 }
 
+// Work packets: cuts units 0..n_units-1 (device costs `cost`, which the scan
+// leaves unchanged) into runs of consecutive units of about equal total cost,
+// about `want` of them; a unit costlier than the target is a packet alone.
+// *pk_out (device, npk + 1 entries) receives the first unit of each packet and
+// n_units last.  Synchronizes `st`.
+int make_packets(long long *cost, int n_units, long long want, int **pk_out, int *npk_out,
+                 cudaStream_t st);
+
 int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
                     const int *d_outdeg, int lane_max, int chunk_min, int chunk,
                     bool keep_csr, PrLayout *L, cudaStream_t st);

@@ -649,18 +649,6 @@ __global__ void k_pk_cost(int n_chunks, int n_units, int R, int n_long, int n_nz
   cost[u] = c + kUnitCost;
 }
 
-__global__ void k_pk_flag(int n, const long long *__restrict__ excl, long long target, int *flag) {
-  const int u = blockIdx.x * blockDim.x + threadIdx.x;
-  if (u < n) flag[u] = (u == 0 || excl[u] / target != excl[u - 1] / target) ? 1 : 0;
-}
-
-__global__ void k_pk_emit(int n, const int *__restrict__ flag, const int *__restrict__ pos,
-                          int *pk) {
-  const int u = blockIdx.x * blockDim.x + threadIdx.x;
-  if (u < n && flag[u]) pk[pos[u]] = u;
-  if (u == n - 1) pk[pos[u] + flag[u]] = n;
-}
-
 // Cuts the units (chunks, then row groups of R rows) into about `want`
 // packets of equal cost; a unit above the target cost is a packet alone.
 // Cached per chunk table and `want`.
@@ -671,69 +659,19 @@ int build_packets(gpr_graph *g, int R, long long want, cudaStream_t st) {
   g->b_npk = -1;
   const gpr::PrLayout &L = g->L;
   const int n_units = g->b_nchunks + (int)gpr::ceil_div((long long)L.n_nz - g->b_nlong, R);
-  if (n_units == 0) {
-    GPR_TRY(gpr::dalloc(&g->b_pk, 1, "ppr packets"));
-    GPR_CUDA(cudaMemsetAsync(g->b_pk, 0, sizeof(int), st));
-    g->b_npk = 0;
-    g->b_pk_want = want;
-    return GPR_OK;
-  }
-  long long *cost = nullptr, *excl = nullptr;
-  int *flag = nullptr, *pos = nullptr;
-  void *tmp = nullptr;
-  size_t tb1 = 0, tb2 = 0;
-  int rc = GPR_OK;
-  long long tail[2] = {0, 0};
-  int ftail[2] = {0, 0};
-  const unsigned nb = (unsigned)gpr::ceil_div(n_units, 256);
-  cudaError_t e = cub::DeviceScan::ExclusiveSum(nullptr, tb1, cost, excl, n_units, st);
-  if (e == cudaSuccess) e = cub::DeviceScan::ExclusiveSum(nullptr, tb2, flag, pos, n_units, st);
-  if (e != cudaSuccess) goto cuda_fail;
-  if ((rc = gpr::dalloc(&cost, n_units, "packet costs")) != GPR_OK ||
-      (rc = gpr::dalloc(&excl, n_units, "packet prefix")) != GPR_OK ||
-      (rc = gpr::dalloc(&flag, n_units, "packet flags")) != GPR_OK ||
-      (rc = gpr::dalloc(&pos, n_units, "packet positions")) != GPR_OK ||
-      (rc = gpr::dmalloc(&tmp, std::max(tb1, tb2), "scan scratch")) != GPR_OK)
-    goto done;
-  k_pk_cost<<<nb, 256, 0, st>>>(g->b_nchunks, n_units, R, g->b_nlong, L.n_nz,
-                                reinterpret_cast<const int4 *>(g->b_cdesc), L.csr_ptr, cost);
-  e = cub::DeviceScan::ExclusiveSum(tmp, tb1, cost, excl, n_units, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(&tail[0], excl + n_units - 1, sizeof(long long), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess)
-    e = cudaMemcpyAsync(&tail[1], cost + n_units - 1, sizeof(long long), cudaMemcpyDeviceToHost, st);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-  if (e != cudaSuccess) goto cuda_fail;
-  {
-    const long long target = std::max(1LL, gpr::ceil_div(tail[0] + tail[1], std::max(1LL, want)));
-    k_pk_flag<<<nb, 256, 0, st>>>(n_units, excl, target, flag);
-    e = cub::DeviceScan::ExclusiveSum(tmp, tb2, flag, pos, n_units, st);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(&ftail[0], pos + n_units - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess)
-      e = cudaMemcpyAsync(&ftail[1], flag + n_units - 1, sizeof(int), cudaMemcpyDeviceToHost, st);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) goto cuda_fail;
-    const int npk = ftail[0] + ftail[1];
-    if ((rc = gpr::dalloc(&g->b_pk, (size_t)npk + 1, "ppr packets")) != GPR_OK) goto done;
-    k_pk_emit<<<nb, 256, 0, st>>>(n_units, flag, pos, g->b_pk);
-    e = cudaGetLastError();
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-    if (e != cudaSuccess) goto cuda_fail;
-    g->b_npk = npk;
-    g->b_pk_want = want;
-  }
-  goto done;
-cuda_fail:
-  gpr::set_error("gpr_ppr packets: %s", cudaGetErrorString(e));
-  rc = GPR_ECUDA;
-done:
+  long long *cost = nullptr;
+  GPR_TRY(gpr::dalloc(&cost, (size_t)std::max(1, n_units), "packet costs"));
+  if (n_units > 0)
+    k_pk_cost<<<(unsigned)gpr::ceil_div(n_units, 256), 256, 0, st>>>(
+        g->b_nchunks, n_units, R, g->b_nlong, L.n_nz, reinterpret_cast<const int4 *>(g->b_cdesc),
+        L.csr_ptr, cost);
+  int npk = 0;
+  const int rc = gpr::make_packets(cost, n_units, want, &g->b_pk, &npk, st);
   gpr::dfree(cost);
-  gpr::dfree(excl);
-  gpr::dfree(flag);
-  gpr::dfree(pos);
-  gpr::dfree(tmp);
-  return rc;
+  GPR_TRY(rc);
+  g->b_npk = npk;
+  g->b_pk_want = want;
+  return GPR_OK;
 }
 
 struct PprKernels {
