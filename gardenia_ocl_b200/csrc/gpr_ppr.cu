@@ -81,6 +81,11 @@ struct Shape {
   // +15% at K = 8, +8% at K = 32); at K >= 64 the extra registers cost more
   // occupancy than the overlap gains (-28% at K = 128).
   static constexpr bool early = K <= 32;
+  // Co-resident 256-thread CTAs per SM the register budget is held to:
+  // K <= 16 trades a few spills for 24 warps instead of 16 (+8% at K = 8,
+  // 4 CTAs lost 3%); K = 32 and 64 fit 2 without spills (3 gained nothing);
+  // K = 128 fits 4.
+  static constexpr int min_ctas = K <= 16 ? 3 : K <= 64 ? 2 : 4;
 };
 
 __device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
@@ -244,7 +249,7 @@ __device__ __forceinline__ void row_update(const PprArgs &a, T *cout, int v, int
 }
 
 template <int K, typename T>
-__global__ void __launch_bounds__(kPprBlock) k_ppr(PprArgs a) {
+__global__ void __launch_bounds__(kPprBlock, Shape<K>::min_ctas) k_ppr(PprArgs a) {
   constexpr int L = Shape<K>::L, R = Shape<K>::R, C = Shape<K>::C, E = Shape<K>::E;
   extern __shared__ double s_red[];  // [2][warps][K]
   __shared__ unsigned s_act[4];
