@@ -552,16 +552,10 @@ def multigraph_leg(G, torch, dev, stream, plain_gteps, args):
     return out
 
 
-def symgs_leg(G, torch, dev, args):
-    """Multicolour symmetric Gauss-Seidel (src/symgs) on the 27-point 128^3
-    stencil with the 8-colour parity colouring (colour = x%2 + 2(y%2) +
-    4(z%2): every neighbour differs by one in some coordinate), x and b
-    seeded uniform.  One sweep = 8 colour passes forward + 8 backward.
-    Bytes per sweep: 2 x (8 bytes per off-diagonal entry + 24 per row:
-    diagonal, row id, length, b, x read and write)."""
-    n = 128
+def symgs_stencil(G, torch, dev, n=128):
+    """The 27-point n^3 stencil, its 8-colour parity colouring and a SymGS
+    handle, with x and b seeded uniform on the device."""
     A = G.gen_stencil27(n)
-    Ap, Aj, Ax = A.rowptr.to_numpy(), A.col.to_numpy(), A.third.to_numpy()
     m = A.m
     v = np.arange(m, dtype=np.int64)
     color = (v % n % 2) + 2 * ((v // n) % n % 2) + 4 * ((v // (n * n)) % 2)
@@ -573,6 +567,18 @@ def symgs_leg(G, torch, dev, args):
     b = torch.empty(m, dtype=torch.float32, device=dev)
     G.gen_uniform(m, 31, x)
     G.gen_uniform(m, 32, b)
+    return A, S, x, b
+
+
+def symgs_leg(G, torch, dev, args):
+    """Multicolour symmetric Gauss-Seidel (src/symgs) on the 27-point 128^3
+    stencil with the 8-colour parity colouring (colour = x%2 + 2(y%2) +
+    4(z%2): every neighbour differs by one in some coordinate), x and b
+    seeded uniform.  One sweep = 8 colour passes forward + 8 backward.
+    Bytes per sweep: 2 x (8 bytes per off-diagonal entry + 24 per row:
+    diagonal, row id, length, b, x read and write)."""
+    A, S, x, b = symgs_stencil(G, torch, dev)
+    m = A.m
     for _ in range(3):
         S.apply(x, b, sweeps=1)
     sweeps = 10
@@ -582,7 +588,7 @@ def symgs_leg(G, torch, dev, args):
     peak, kind = load_peaks()
     S.close()
     A.close()
-    return {"workload": "symgs_stencil27_128^3_8colours", "m": m, "nnz": int(len(Aj)),
+    return {"workload": "symgs_stencil27_128^3_8colours", "m": m, "nnz": int(A.nnz),
             "ms_per_sweep": ms, "achieved_gbs": byts / (ms / 1e3) / 1e9,
             "frac": byts / (ms / 1e3) / 1e9 / peak, "peak_kind": kind,
             "bytes_formula": "2*(8*offdiag_nnz + 24*m)"}
@@ -727,6 +733,20 @@ def profile_ppr(args):
     return 0
 
 
+def profile_symgs(args):
+    """One SymGS apply of exactly --profile-symgs sweeps on the 27-point 128^3
+    stencil with the 8-colour parity colouring (for ncu)."""
+    import torch
+
+    import gardenia_ocl_b200 as G
+    A, S, x, b = symgs_stencil(G, torch, torch.device("cuda"))
+    ms = S.apply(x, b, sweeps=args.profile_symgs)
+    log(json.dumps({"m": A.m, "nnz": A.nnz, "sweeps": args.profile_symgs, "ms": ms}))
+    S.close()
+    A.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -756,7 +776,12 @@ def main():
     ap.add_argument("--profile-ppr", type=int, default=0, metavar="K",
                     help="one batched PPR solve with K seed vectors and --profile-solve sweeps "
                          "on the RMAT graph of --scale (the case profiled with ncu)")
+    ap.add_argument("--profile-symgs", type=int, default=0, metavar="SWEEPS",
+                    help="one SymGS apply of SWEEPS sweeps on the 128^3 stencil "
+                         "(the case profiled with ncu)")
     args = ap.parse_args()
+    if args.profile_symgs:
+        return profile_symgs(args)
     if args.profile_multigraph:
         return profile_multigraph(args)
     if args.profile_ppr:
