@@ -455,7 +455,8 @@ def ppr_leg(G, torch, dev, stream, args):
     """Batched personalized PageRank on its own configuration: RMAT scale 22,
     edge factor 16 (same RMAT parameters), k = 8, 32 and 128 seed vectors,
     each seed drawn uniformly (seeded), teleport mass on the seed, tol 1e-6
-    per vector, one persistent launch, FP32 and BF16 + FP32 refinement.
+    per vector, one persistent launch, FP32 and BF16 + FP32 refinement, and
+    the FP32 solve again as a CUDA-graph loop of one launch per sweep.
     Rate: nnz x k x sweeps per second of the sweep loop (edge-vector pairs);
     the plain FP32 single-vector GTEPS on the same graph is the comparison."""
     csr = G.gen_rmat(PPR_SCALE, EDGE_FACTOR, seed=SEED, abc=ABC)
@@ -488,6 +489,16 @@ def ppr_leg(G, torch, dev, stream, args):
                                   "vector_sweeps_min": int(it.min()), "loop_ms": st.loop_ms,
                                   "edge_vector_gteps": rate, "vs_plain_fp32": rate / plain,
                                   "max_final_residual": st.residual}
+        # the same FP32 solve as a CUDA-graph loop (one launch per sweep)
+        bst = None
+        for _ in range(2):
+            _, it, st = g.ppr(seeds, out=buf, tol=TOL, max_iter=MAX_ITER, loop=G.LOOP_GRAPH)
+            if bst is None or st.loop_ms < bst.loop_ms:
+                bst = st
+        rate = nnz * k * bst.iterations / (bst.loop_ms / 1e3) / 1e9
+        out[f"k{k}_fp32_graph_loop"] = {"sweeps": bst.iterations, "loop_ms": bst.loop_ms,
+                                        "gpu_launches": bst.gpu_launches,
+                                        "edge_vector_gteps": rate, "vs_plain_fp32": rate / plain}
         del buf
     g.close()
     csr.close()

@@ -61,6 +61,7 @@ struct PprArgs {
   double tol;
   int max_iter, bar_expect;
   long long timeout_ns;
+  unsigned long long cond;  // graph mode: while-node condition handle (0: none)
 };
 
 // Lanes per row L = K / 4, rows per warp R = 32 / L, components per lane
@@ -248,170 +249,239 @@ __device__ __forceinline__ void row_update(const PprArgs &a, T *cout, int v, int
   }
 }
 
+// One sweep of this CTA's share: packets of units, the seed rows without
+// in-edges, and the CTA's residual and dangling sums (per vector, warps in
+// order) into cta_red.  Ends with the CTA synchronised.
+template <int K, typename T>
+__device__ __forceinline__ void ppr_sweep(const PprArgs &a, int it, const int (&sd)[Shape<K>::C],
+                                          double *s_red) {
+  constexpr int L = Shape<K>::L, R = Shape<K>::R, C = Shape<K>::C, E = Shape<K>::E;
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+  const int g = lane / L, lq = lane % L;
+  const int G = gridDim.x;
+  const T *cin = reinterpret_cast<const T *>((it & 1) ? a.c1 : a.c0);
+  T *cout = reinterpret_cast<T *>((it & 1) ? a.c0 : a.c1);
+  const double *dang_cur = a.dang + (it & 1) * K;
+  unsigned act[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) act[i] = __ldcg(a.active + (it & 1) * 4 + i);
+  bool live = false;
+#pragma unroll
+  for (int c = 0; c < C; ++c) live |= is_active(act, lq * C + c);
+  double err[C], dng[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) err[c] = dng[c] = 0.0;
+  // Warps take packets (runs of units of about equal cost) from one queue;
+  // units [0, n_chunks) are chunks of long rows, the rest groups of R rows.
+  for (;;) {
+    int p = 0;
+    if (lane == 0) p = atomicAdd(a.wq + (it & 1), 1);
+    p = __shfl_sync(kFull, p, 0);
+    if (p >= a.n_pk) break;
+    const int u1 = __ldg(a.pk + p + 1);
+    int u = __ldg(a.pk + p);
+    for (; u < u1 && u < a.n_chunks; ++u) {
+      float acc[C], xo[C];
+      int od = 0;
+#pragma unroll
+      for (int c = 0; c < C; ++c) acc[c] = 0.f;
+      const int4 d = __ldg(a.cdesc + u);
+      const int r = d.x, cb = d.w;
+      const long long b = d.y, e = d.z;
+      if (Shape<K>::early && cb < 0) row_fetch<K>(a, r, lq, od, xo);  // the row's only chunk
+      const int niter = (int)gpr::ceil_div(e - b, (long long)R * E);
+      gather_edges<K, T>(a, cin, b + (long long)g * E, e, (long long)R * E, niter, lq, live,
+                         acc);
+#pragma unroll
+      for (int o = L; o < 32; o <<= 1)
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[c] += __shfl_xor_sync(kFull, acc[c], o);
+      if (cb < 0) {
+        if (!Shape<K>::early) row_fetch<K>(a, r, lq, od, xo);
+        if (g == 0) row_update<K, T>(a, cout, r, lq, act, dang_cur, sd, acc, od, xo, err, dng);
+        continue;
+      }
+      if (g == 0)
+#pragma unroll
+        for (int c = 0; c < C; ++c) a.partial[(size_t)u * K + lq * C + c] = acc[c];
+      __threadfence();
+      __syncwarp();
+      const int nc = __ldg(a.row_cbeg + r + 1) - cb;
+      int last = 0;
+      if (lane == 0) last = atomicAdd(a.cnt + r, 1) == nc - 1;
+      last = __shfl_sync(kFull, last, 0);
+      if (!last) continue;
+      __threadfence();
+      // Sum the row's chunk partials in chunk order (sub-group 0).
+      row_fetch<K>(a, r, lq, od, xo);
+#pragma unroll
+      for (int c = 0; c < C; ++c) acc[c] = 0.f;
+      for (int q = 0; q < nc; ++q)
+#pragma unroll
+        for (int c = 0; c < C; ++c) acc[c] += __ldcg(a.partial + (size_t)(cb + q) * K + lq * C + c);
+      if (lane == 0) atomicExch(a.cnt + r, 0);
+      if (g == 0) row_update<K, T>(a, cout, r, lq, act, dang_cur, sd, acc, od, xo, err, dng);
+    }
+    if (u >= u1) continue;
+    // Row groups; with the early fetch, the next group's row offsets are
+    // in flight while this group gathers.
+    int v = a.n_long + (u - a.n_chunks) * R + g;
+    int p0 = 0, p1 = 0;
+    if (Shape<K>::early && v < a.n_nz) {
+      p0 = a.csr_ptr[v];
+      p1 = a.csr_ptr[v + 1];
+    }
+    for (; u < u1; ++u, v += R) {
+      const bool has = v < a.n_nz;
+      if (!Shape<K>::early) {
+        p0 = has ? a.csr_ptr[v] : 0;
+        p1 = has ? a.csr_ptr[v + 1] : 0;
+      }
+      const long long e0 = p0, e1 = p1;
+      if (Shape<K>::early) {
+        if (u + 1 < u1 && v + R < a.n_nz) {
+          asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(p0) : "l"(a.csr_ptr + v + R));
+          asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(p1) : "l"(a.csr_ptr + v + R + 1));
+        } else {
+          p0 = p1 = 0;
+        }
+      }
+      float acc[C], xo[C];
+      int od = 0;
+#pragma unroll
+      for (int c = 0; c < C; ++c) acc[c] = 0.f;
+      if (Shape<K>::early && has) row_fetch<K>(a, v, lq, od, xo);
+      // Rows of one warp have nearly equal degrees (degree order); the
+      // sub-groups loop to the warp's longest row.
+      long long span = e1 - e0;
+#pragma unroll
+      for (int o = L; o < 32; o <<= 1) span = max(span, __shfl_xor_sync(kFull, span, o));
+      gather_edges<K, T>(a, cin, e0, e1, (long long)E, (int)gpr::ceil_div(span, E), lq,
+                         live && has, acc);
+      // edges past this row's end gathered the sentinel row (zeros)
+      if (!Shape<K>::early && has) row_fetch<K>(a, v, lq, od, xo);
+      if (has) row_update<K, T>(a, cout, v, lq, act, dang_cur, sd, acc, od, xo, err, dng);
+    }
+  }
+  // Seed rows without in-edges: only their teleport term changes.
+  const int gt = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gt < a.k) {
+    const int q = gt, v = a.seed[q];
+    double se = 0.0, sd = 0.0;
+    if (v >= a.n_nz && is_active(act, q)) {
+      const float xn = (float)((1.0 - (double)a.damp) + (double)a.damp * dang_cur[q]);
+      const size_t o = (size_t)v * K + q;
+      const float xo = a.x[o];
+      const int od = a.outdeg[v];
+      a.x[o] = xn;
+      store_c(cout + o, od > 0 ? xn * (1.0f / (float)od) : 0.f);
+      se = fabs((double)xn - (double)xo);
+      if (od == 0) sd = (double)xn;
+    }
+    a.seed_red[q] = se;
+    a.seed_red[K + q] = sd;
+  }
+  // CTA reduction: sub-groups, then warps in order.
+#pragma unroll
+  for (int o = L; o < 32; o <<= 1)
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      err[c] += __shfl_xor_sync(kFull, err[c], o);
+      dng[c] += __shfl_xor_sync(kFull, dng[c], o);
+    }
+  if (g == 0)
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+      s_red[(size_t)wid * K + lq * C + c] = err[c];
+      s_red[(size_t)(nwarps + wid) * K + lq * C + c] = dng[c];
+    }
+  __syncthreads();
+  for (int q = threadIdx.x; q < K; q += blockDim.x) {
+    double te = 0.0, td = 0.0;
+    for (int w = 0; w < nwarps; ++w) {
+      te += s_red[(size_t)w * K + q];
+      td += s_red[(size_t)(nwarps + w) * K + q];
+    }
+    a.cta_red[(size_t)blockIdx.x * K + q] = te;
+    a.cta_red[(size_t)(G + blockIdx.x) * K + q] = td;
+  }
+  __syncthreads();
+}
+
+// Closes sweep it; run by all threads of the last CTA to finish the sweep,
+// after every CTA's cta_red and seed_red are visible.  Sums each vector's
+// residual and dangling mass over CTAs in CTA order (deterministic), records
+// the residual and sweep count of the vectors that updated, freezes those
+// below tol, publishes the next sweep's masks and dangling mass, sets
+// status[2] to whether any vector keeps updating and resets the queue head
+// that sweep it + 2 reuses.
+template <int K>
+__device__ __forceinline__ void ppr_close(const PprArgs &a, int it, unsigned *s_act) {
+  const int G = gridDim.x;
+  const double *dang_cur = a.dang + (it & 1) * K;
+  unsigned act[4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i) act[i] = __ldcg(a.active + (it & 1) * 4 + i);
+  if (threadIdx.x < 4) s_act[threadIdx.x] = act[threadIdx.x];
+  __syncthreads();
+  for (int q = threadIdx.x; q < K; q += blockDim.x) {
+    double te = __ldcg(a.seed_red + q), td = __ldcg(a.seed_red + K + q);
+    for (int c = 0; c < G; ++c) {
+      te += __ldcg(a.cta_red + (size_t)c * K + q);
+      td += __ldcg(a.cta_red + (size_t)(G + c) * K + q);
+    }
+    a.res_hist[(size_t)it * K + q] = te;
+    const bool was = is_active(act, q);
+    a.dang[((it + 1) & 1) * K + q] = was ? td : dang_cur[q];
+    if (was) {
+      a.iters[q] = it + 1;
+      if (te < a.tol) atomicAnd(&s_act[q >> 5], ~(1u << (q & 31)));
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    unsigned any = 0;
+    for (int i = 0; i < 4; ++i) {
+      a.active[((it + 1) & 1) * 4 + i] = s_act[i];
+      any |= s_act[i];
+    }
+    a.status[2] = any != 0;
+    atomicExch(a.wq + (it & 1), 0);
+  }
+  __syncthreads();
+}
+
+// The close as a call: for K <= 16, where the sweep runs at the register
+// limit, keeping it out of the sweep kernel's body leaves the sweep fewer
+// spills (+4% at K = 8); for wider vectors inlining is faster (-18% at
+// K = 128 as a call).
+template <int K>
+__device__ __noinline__ void ppr_close_call(const PprArgs &a, int it, unsigned *s_act) {
+  ppr_close<K>(a, it, s_act);
+}
+
+template <int K>
+__device__ __forceinline__ void close_sweep(const PprArgs &a, int it, unsigned *s_act) {
+  if constexpr (K <= 16) ppr_close_call<K>(a, it, s_act);
+  else ppr_close<K>(a, it, s_act);
+}
+
+// All sweeps in one cooperative launch, a bounded grid barrier between them.
 template <int K, typename T>
 __global__ void __launch_bounds__(kPprBlock, Shape<K>::min_ctas) k_ppr(PprArgs a) {
-  constexpr int L = Shape<K>::L, R = Shape<K>::R, C = Shape<K>::C, E = Shape<K>::E;
+  constexpr int L = Shape<K>::L, C = Shape<K>::C;
   extern __shared__ double s_red[];  // [2][warps][K]
   __shared__ unsigned s_act[4];
   __shared__ int s_state;
   __shared__ unsigned s_gen;
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-  const int g = lane / L, lq = lane % L;
-  const int G = gridDim.x;
+  const int lq = (threadIdx.x & 31) % L;
   int sd[C];  // seed vertices of this lane's components (-1: padding)
 #pragma unroll
   for (int c = 0; c < C; ++c) sd[c] = a.seed[lq * C + c];
   int it = 0;
   while (it < a.max_iter) {
-    const T *cin = reinterpret_cast<const T *>((it & 1) ? a.c1 : a.c0);
-    T *cout = reinterpret_cast<T *>((it & 1) ? a.c0 : a.c1);
-    const double *dang_cur = a.dang + (it & 1) * K;
-    unsigned act[4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i) act[i] = __ldcg(a.active + (it & 1) * 4 + i);
-    bool live = false;
-#pragma unroll
-    for (int c = 0; c < C; ++c) live |= is_active(act, lq * C + c);
-    double err[C], dng[C];
-#pragma unroll
-    for (int c = 0; c < C; ++c) err[c] = dng[c] = 0.0;
-    // Warps take packets (runs of units of about equal cost) from one queue;
-    // units [0, n_chunks) are chunks of long rows, the rest groups of R rows.
-    for (;;) {
-      int p = 0;
-      if (lane == 0) p = atomicAdd(a.wq + (it & 1), 1);
-      p = __shfl_sync(kFull, p, 0);
-      if (p >= a.n_pk) break;
-      const int u1 = __ldg(a.pk + p + 1);
-      int u = __ldg(a.pk + p);
-      for (; u < u1 && u < a.n_chunks; ++u) {
-        float acc[C], xo[C];
-        int od = 0;
-#pragma unroll
-        for (int c = 0; c < C; ++c) acc[c] = 0.f;
-        const int4 d = __ldg(a.cdesc + u);
-        const int r = d.x, cb = d.w;
-        const long long b = d.y, e = d.z;
-        if (Shape<K>::early && cb < 0) row_fetch<K>(a, r, lq, od, xo);  // the row's only chunk
-        const int niter = (int)gpr::ceil_div(e - b, (long long)R * E);
-        gather_edges<K, T>(a, cin, b + (long long)g * E, e, (long long)R * E, niter, lq, live,
-                           acc);
-#pragma unroll
-        for (int o = L; o < 32; o <<= 1)
-#pragma unroll
-          for (int c = 0; c < C; ++c) acc[c] += __shfl_xor_sync(kFull, acc[c], o);
-        if (cb < 0) {
-          if (!Shape<K>::early) row_fetch<K>(a, r, lq, od, xo);
-          if (g == 0) row_update<K, T>(a, cout, r, lq, act, dang_cur, sd, acc, od, xo, err, dng);
-          continue;
-        }
-        if (g == 0)
-#pragma unroll
-          for (int c = 0; c < C; ++c) a.partial[(size_t)u * K + lq * C + c] = acc[c];
-        __threadfence();
-        __syncwarp();
-        const int nc = __ldg(a.row_cbeg + r + 1) - cb;
-        int last = 0;
-        if (lane == 0) last = atomicAdd(a.cnt + r, 1) == nc - 1;
-        last = __shfl_sync(kFull, last, 0);
-        if (!last) continue;
-        __threadfence();
-        // Sum the row's chunk partials in chunk order (sub-group 0).
-        row_fetch<K>(a, r, lq, od, xo);
-#pragma unroll
-        for (int c = 0; c < C; ++c) acc[c] = 0.f;
-        for (int q = 0; q < nc; ++q)
-#pragma unroll
-          for (int c = 0; c < C; ++c) acc[c] += __ldcg(a.partial + (size_t)(cb + q) * K + lq * C + c);
-        if (lane == 0) atomicExch(a.cnt + r, 0);
-        if (g == 0) row_update<K, T>(a, cout, r, lq, act, dang_cur, sd, acc, od, xo, err, dng);
-      }
-      if (u >= u1) continue;
-      // Row groups; with the early fetch, the next group's row offsets are
-      // in flight while this group gathers.
-      int v = a.n_long + (u - a.n_chunks) * R + g;
-      int p0 = 0, p1 = 0;
-      if (Shape<K>::early && v < a.n_nz) {
-        p0 = a.csr_ptr[v];
-        p1 = a.csr_ptr[v + 1];
-      }
-      for (; u < u1; ++u, v += R) {
-        const bool has = v < a.n_nz;
-        if (!Shape<K>::early) {
-          p0 = has ? a.csr_ptr[v] : 0;
-          p1 = has ? a.csr_ptr[v + 1] : 0;
-        }
-        const long long e0 = p0, e1 = p1;
-        if (Shape<K>::early) {
-          if (u + 1 < u1 && v + R < a.n_nz) {
-            asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(p0) : "l"(a.csr_ptr + v + R));
-            asm volatile("ld.global.nc.s32 %0, [%1];" : "=r"(p1) : "l"(a.csr_ptr + v + R + 1));
-          } else {
-            p0 = p1 = 0;
-          }
-        }
-        float acc[C], xo[C];
-        int od = 0;
-#pragma unroll
-        for (int c = 0; c < C; ++c) acc[c] = 0.f;
-        if (Shape<K>::early && has) row_fetch<K>(a, v, lq, od, xo);
-        // Rows of one warp have nearly equal degrees (degree order); the
-        // sub-groups loop to the warp's longest row.
-        long long span = e1 - e0;
-#pragma unroll
-        for (int o = L; o < 32; o <<= 1) span = max(span, __shfl_xor_sync(kFull, span, o));
-        gather_edges<K, T>(a, cin, e0, e1, (long long)E, (int)gpr::ceil_div(span, E), lq,
-                           live && has, acc);
-        // edges past this row's end gathered the sentinel row (zeros)
-        if (!Shape<K>::early && has) row_fetch<K>(a, v, lq, od, xo);
-        if (has) row_update<K, T>(a, cout, v, lq, act, dang_cur, sd, acc, od, xo, err, dng);
-      }
-    }
-    // Seed rows without in-edges: only their teleport term changes.
-    const int gt = blockIdx.x * blockDim.x + threadIdx.x;
-    if (gt < a.k) {
-      const int q = gt, v = a.seed[q];
-      double se = 0.0, sd = 0.0;
-      if (v >= a.n_nz && is_active(act, q)) {
-        const float xn = (float)((1.0 - (double)a.damp) + (double)a.damp * dang_cur[q]);
-        const size_t o = (size_t)v * K + q;
-        const float xo = a.x[o];
-        const int od = a.outdeg[v];
-        a.x[o] = xn;
-        store_c(cout + o, od > 0 ? xn * (1.0f / (float)od) : 0.f);
-        se = fabs((double)xn - (double)xo);
-        if (od == 0) sd = (double)xn;
-      }
-      a.seed_red[q] = se;
-      a.seed_red[K + q] = sd;
-    }
-    // CTA reduction: sub-groups, then warps in order.
-#pragma unroll
-    for (int o = L; o < 32; o <<= 1)
-#pragma unroll
-      for (int c = 0; c < C; ++c) {
-        err[c] += __shfl_xor_sync(kFull, err[c], o);
-        dng[c] += __shfl_xor_sync(kFull, dng[c], o);
-      }
-    if (g == 0)
-#pragma unroll
-      for (int c = 0; c < C; ++c) {
-        s_red[(size_t)wid * K + lq * C + c] = err[c];
-        s_red[(size_t)(nwarps + wid) * K + lq * C + c] = dng[c];
-      }
-    __syncthreads();
-    for (int q = threadIdx.x; q < K; q += blockDim.x) {
-      double te = 0.0, td = 0.0;
-      for (int w = 0; w < nwarps; ++w) {
-        te += s_red[(size_t)w * K + q];
-        td += s_red[(size_t)(nwarps + w) * K + q];
-      }
-      a.cta_red[(size_t)blockIdx.x * K + q] = te;
-      a.cta_red[(size_t)(G + blockIdx.x) * K + q] = td;
-    }
-    __syncthreads();
-    // Grid barrier; the last CTA reduces over CTAs and decides which
-    // vectors keep updating.
+    ppr_sweep<K, T>(a, it, sd, s_red);
+    // Grid barrier; the last CTA closes the sweep.
     if (threadIdx.x == 0) {
       s_gen = ld_acquire(a.bar + 1);
       __threadfence();
@@ -421,31 +491,8 @@ __global__ void __launch_bounds__(kPprBlock, Shape<K>::min_ctas) k_ppr(PprArgs a
     __syncthreads();
     if (s_state == 1) {
       __threadfence();
-      if (threadIdx.x < 4) s_act[threadIdx.x] = act[threadIdx.x];
-      __syncthreads();
-      for (int q = threadIdx.x; q < K; q += blockDim.x) {
-        double te = __ldcg(a.seed_red + q), td = __ldcg(a.seed_red + K + q);
-        for (int c = 0; c < G; ++c) {
-          te += __ldcg(a.cta_red + (size_t)c * K + q);
-          td += __ldcg(a.cta_red + (size_t)(G + c) * K + q);
-        }
-        a.res_hist[(size_t)it * K + q] = te;
-        const bool was = is_active(act, q);
-        a.dang[((it + 1) & 1) * K + q] = was ? td : dang_cur[q];
-        if (was) {
-          a.iters[q] = it + 1;
-          if (te < a.tol) atomicAnd(&s_act[q >> 5], ~(1u << (q & 31)));
-        }
-      }
-      __syncthreads();
+      close_sweep<K>(a, it, s_act);
       if (threadIdx.x == 0) {
-        unsigned any = 0;
-        for (int i = 0; i < 4; ++i) {
-          a.active[((it + 1) & 1) * 4 + i] = s_act[i];
-          any |= s_act[i];
-        }
-        a.status[2] = any != 0;
-        atomicExch(a.wq + (it & 1), 0);
         atomicExch(a.bar, 0u);
         __threadfence();
         atomicAdd(a.bar + 1, 1u);
@@ -469,6 +516,52 @@ __global__ void __launch_bounds__(kPprBlock, Shape<K>::min_ctas) k_ppr(PprArgs a
     if (!__ldcg(a.status + 2)) break;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) a.status[1] = it;
+}
+
+// One sweep per launch (graph mode): the body of a CUDA-graph while node.
+// The sweep index (status[1]) and the any-vector-active flag (status[2]) live
+// in device memory, so the captured launch needs no host input.  The last
+// CTA to finish a sweep closes it; no CTA waits for another, so the grid need
+// not be co-resident.  The node's condition starts at 1 and is only cleared:
+// by the CTA that closes the last sweep, by a launch that finds the solve
+// done, and by CTA 0 of the max_iter-th launch (status[3] counts launches).
+template <int K, typename T>
+__global__ void __launch_bounds__(kPprBlock, Shape<K>::min_ctas) k_ppr_step(PprArgs a) {
+  constexpr int L = Shape<K>::L, C = Shape<K>::C;
+  extern __shared__ double s_red[];  // [2][warps][K]
+  __shared__ unsigned s_act[4];
+  __shared__ int s_it, s_last;
+  if (threadIdx.x == 0) {
+    const int n_done = *(volatile int *)(a.status + 1);
+    const bool live = n_done == 0 || *(volatile int *)(a.status + 2) != 0;
+    s_it = live && n_done < a.max_iter ? n_done : -1;
+    if (a.cond && blockIdx.x == 0) {
+      const int n = atomicAdd(a.status + 3, 1) + 1;
+      if (s_it < 0 || n >= a.max_iter) cudaGraphSetConditional(a.cond, 0u);
+    }
+  }
+  __syncthreads();
+  const int it = s_it;
+  if (it < 0) return;
+  const int lq = (threadIdx.x & 31) % L;
+  int sd[C];
+#pragma unroll
+  for (int c = 0; c < C; ++c) sd[c] = a.seed[lq * C + c];
+  ppr_sweep<K, T>(a, it, sd, s_red);
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(a.bar, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  close_sweep<K>(a, it, s_act);
+  if (threadIdx.x == 0) {
+    atomicExch(a.bar, 0u);
+    a.status[1] = it + 1;
+    __threadfence();
+    if (a.cond && (!a.status[2] || it + 1 >= a.max_iter)) cudaGraphSetConditional(a.cond, 0u);
+  }
 }
 
 // x = e_seed, contributions of the seeds, initial dangling mass and masks.
@@ -680,7 +773,8 @@ int build_packets(gpr_graph *g, int R, long long want, cudaStream_t st) {
 }
 
 struct PprKernels {
-  const void *solve;
+  const void *solve;  // persistent: all sweeps in one cooperative launch
+  const void *step;   // one sweep per launch (graph mode)
   void (*init)(PprArgs);
   void (*scatter)(int, int, const int *, const float *, float *);
   void (*refine_init)(PprArgs, const double *);
@@ -688,7 +782,8 @@ struct PprKernels {
 
 template <int K, typename T>
 PprKernels kernels_for() {
-  return {(const void *)k_ppr<K, T>, k_ppr_init<K, T>, k_ppr_scatter<K>, k_ppr_refine_init<K>};
+  return {(const void *)k_ppr<K, T>, (const void *)k_ppr_step<K, T>, k_ppr_init<K, T>,
+          k_ppr_scatter<K>, k_ppr_refine_init<K>};
 }
 
 int pick_k(int k) {
@@ -840,6 +935,7 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
   k_invert_for_seeds<<<(unsigned)gpr::ceil_div(m, 256), 256, 0, st>>>(m, L.perm, k, seeds_old,
                                                                        seed);
   PprArgs a;
+  memset(&a, 0, sizeof(a));
   a.m = m;
   a.n_long = g->b_nlong;
   a.n_nz = L.n_nz;
@@ -869,24 +965,82 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
   a.max_iter = max_iter;
   a.timeout_ns = (long long)(o.timeout_s * 1e9);
   int launches = 0;
-  // One phase: sweeps until every vector's change is below `tol`.
-  auto phase = [&](const PprKernels &kk, int G, double tol, int *sweeps,
+  // Graph mode: the sweep loop as one CUDA graph, a while node whose body is
+  // one k_ppr_step launch (the kernel clears the condition when the phase is
+  // done).  Built, run and released per phase; `mark` records the loop's
+  // start event after the graph is built, right before its launch.
+  auto step_loop = [&](const PprKernels &kk, int G, bool mark) -> int {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaGraphConditionalHandle h = 0;
+    cudaGraphNodeParams cp = {};
+    cudaGraphNode_t cn = nullptr, kn = nullptr;
+    cudaError_t e = cudaGraphCreate(&graph, 0);
+    if (e == cudaSuccess)
+      e = cudaGraphConditionalHandleCreate(&h, graph, 1u, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      e = cudaGraphAddNode(&cn, graph, nullptr, 0, &cp);
+    }
+    PprArgs ac = a;
+    ac.cond = h;
+    void *kargs[] = {&ac};
+    cudaKernelNodeParams kp;
+    memset(&kp, 0, sizeof(kp));
+    kp.func = const_cast<void *>(kk.step);
+    kp.gridDim = dim3(G);
+    kp.blockDim = dim3(kPprBlock);
+    kp.sharedMemBytes = (unsigned)smem;
+    kp.kernelParams = kargs;
+    if (e == cudaSuccess) e = cudaGraphAddKernelNode(&kn, cp.conditional.phGraph_out[0], nullptr, 0, &kp);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e == cudaSuccess && mark) e = cudaEventRecord(g->e2, st);
+    if (e == cudaSuccess) e = cudaGraphLaunch(exec, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      gpr::set_error("gpr_ppr graph loop: %s", cudaGetErrorString(e));
+      return GPR_ECUDA;
+    }
+    return GPR_OK;
+  };
+  // One phase: sweeps until every vector's change is below `tol`, in one
+  // cooperative launch, or (GPR_LOOP_GRAPH, or when the grid cannot be
+  // co-resident) in the graph loop.  The first phase (`mark`) records the
+  // start event of the sweep loop right before its launch.
+  auto phase = [&](const PprKernels &kk, int G, double tol, bool mark, int *sweeps,
                    std::vector<int> *it_out) -> int {
     a.tol = tol;
     a.bar_expect = G + (o.reserved[0] > 0 ? o.reserved[0] : 0);
     GPR_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 4, st));
     GPR_CUDA(cudaMemsetAsync(wq, 0, sizeof(int) * 4, st));
-    if (max_iter > 0) {
+    bool graph_mode = o.loop == GPR_LOOP_GRAPH;
+    if (mark && (max_iter <= 0 || !graph_mode)) GPR_CUDA(cudaEventRecord(g->e2, st));
+    if (max_iter > 0 && !graph_mode) {
       void *args[] = {&a};
-      GPR_CUDA(cudaLaunchCooperativeKernel(kk.solve, dim3(G), dim3(kPprBlock), args, smem, st));
-      ++launches;
+      cudaError_t e = cudaLaunchCooperativeKernel(kk.solve, dim3(G), dim3(kPprBlock), args, smem, st);
+      if (e == cudaErrorCooperativeLaunchTooLarge) {
+        cudaGetLastError();
+        graph_mode = true;
+      } else if (e != cudaSuccess) {
+        gpr::set_error("gpr_ppr: %s", cudaGetErrorString(e));
+        return GPR_ECUDA;
+      } else {
+        ++launches;
+      }
     }
+    if (max_iter > 0 && graph_mode) GPR_TRY(step_loop(kk, G, mark && o.loop == GPR_LOOP_GRAPH));
     int hs[4];
     GPR_CUDA(cudaMemcpyAsync(hs, status, sizeof(hs), cudaMemcpyDeviceToHost, st));
     it_out->assign(K, 0);
     GPR_CUDA(cudaMemcpyAsync(it_out->data(), iters, sizeof(int) * K, cudaMemcpyDeviceToHost, st));
     GPR_CUDA(cudaStreamSynchronize(st));
     *sweeps = hs[1];
+    if (max_iter > 0 && graph_mode) launches += hs[3];
     if (hs[0] & 1) {
       gpr::set_error("gpr_ppr: grid barrier wait exceeded %.3f s", o.timeout_s);
       return GPR_ETIMEOUT;
@@ -901,8 +1055,7 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
     a.c1 = h1;
     k16.init<<<1, 128, 0, st>>>(a);
     ++launches;
-    GPR_CUDA(cudaEventRecord(g->e2, st));
-    GPR_TRY(phase(k16, G16, tol_lo, &s1, &it1));
+    GPR_TRY(phase(k16, G16, tol_lo, true, &s1, &it1));
     a.c0 = c0;
     a.c1 = c1;
     k32.refine_init<<<(unsigned)gpr::ceil_div((long long)m * K, 256), 256, 0, st>>>(
@@ -913,9 +1066,8 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
     a.c1 = c1;
     k32.init<<<1, 128, 0, st>>>(a);
     ++launches;
-    GPR_CUDA(cudaEventRecord(g->e2, st));
   }
-  GPR_TRY(phase(k32, G32, o.tol, &s2, &it2));
+  GPR_TRY(phase(k32, G32, o.tol, !bf16, &s2, &it2));
   GPR_CUDA(cudaEventRecord(g->e3, st));
   const bool host_out = !gpr::is_device_ptr(any_x);
   float *dout = any_x;

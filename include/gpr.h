@@ -154,7 +154,11 @@ int gpr_page_rank(int m, int nnz, const int *row_offsets,
  * is below opts->tol.  opts->precision: GPR_PREC_FP32 or GPR_PREC_BF16
  * (contributions stored in BF16, FP32 accumulation).  any_x receives x as an
  * m x k row-major array (vertex-major, host or device); h_iters (k ints, may
- * be NULL) the sweeps of each vector.  The graph must be created with
+ * be NULL) the sweeps of each vector.  opts->loop: GPR_LOOP_AUTO /
+ * GPR_LOOP_PERSISTENT run all sweeps in one cooperative launch (grid barrier
+ * bounded by opts->timeout_s); GPR_LOOP_GRAPH runs one launch per sweep in a
+ * CUDA-graph while loop (also used when the grid cannot be co-resident);
+ * both give bit-identical results.  The graph must be created with
  * GPR_LAYOUT_BATCHED. */
 int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
             const gpr_pr_opts *opts, int *h_iters, gpr_pr_stats *stats);

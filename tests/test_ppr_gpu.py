@@ -65,3 +65,39 @@ def test_ppr_requires_batched_layout(G, O):
         with pytest.raises(G.GprError) as e:
             g.ppr(np.array([0], np.int32))
     assert e.value.status == G.GPR_EINVAL
+
+
+@pytest.mark.parametrize("k,prec", [(8, "fp32"), (32, "fp32"), (128, "fp32"), (32, "bf16")])
+def test_ppr_graph_loop_matches_persistent(G, O, k, prec):
+    """GPR_LOOP_GRAPH runs one sweep per launch inside a CUDA-graph while
+    loop (the last CTA to finish a sweep closes it).  The sweep code and the
+    CTA-order reductions are the persistent kernel's, so scores and sweep
+    counts are bit-identical."""
+    rp, col, od = O.rmat_graph(12, 8, seed=33)
+    seeds = O.uniform_int(k, 79, len(rp) - 1)
+    p = G.PREC_BF16 if prec == "bf16" else G.PREC_FP32
+    with G.Graph(rp, col, od, batched=True) as g:
+        x0, it0, st0 = g.ppr(seeds, tol=1e-6, max_iter=100, precision=p, loop=G.LOOP_PERSISTENT)
+        x1, it1, st1 = g.ppr(seeds, tol=1e-6, max_iter=100, precision=p, loop=G.LOOP_GRAPH)
+    np.testing.assert_array_equal(x0, x1)
+    np.testing.assert_array_equal(it0, it1)
+    assert st1.iterations == st0.iterations
+    assert st1.refine_iterations == st0.refine_iterations
+    # one launch per sweep plus the launch that finds the phase done
+    assert st1.gpu_launches > st0.gpu_launches
+
+
+def test_ppr_graph_loop_hub_chunks_and_cap(G, O):
+    """A hub of 60,000 in-edges (many chunks summed by the last arriving warp)
+    in graph mode, and the max_iter cap of the graph loop."""
+    rp, col, od = star(60000)
+    seeds = np.array([0, 1, 12345], dtype=np.int32)
+    ref, ref_it = O.ppr_f64(rp, col, od, seeds, tol=1e-6, max_iter=100)
+    with G.Graph(rp, col, od, batched=True) as g:
+        x, it, st = g.ppr(seeds, tol=1e-6, max_iter=100, loop=G.LOOP_GRAPH)
+        xc, itc, stc = g.ppr(seeds, tol=0.0, max_iter=4, loop=G.LOOP_GRAPH)
+        xp, itp, stp = g.ppr(seeds, tol=0.0, max_iter=4)
+    assert np.all(l1_per_vector(x, ref) <= 1e-5)
+    assert np.all(np.abs(it - ref_it) <= 1)
+    assert stc.iterations == 4 and np.all(itc == 4)
+    np.testing.assert_array_equal(xc, xp)
