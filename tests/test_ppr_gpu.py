@@ -101,3 +101,19 @@ def test_ppr_graph_loop_hub_chunks_and_cap(G, O):
     assert np.all(np.abs(it - ref_it) <= 1)
     assert stc.iterations == 4 and np.all(itc == 4)
     np.testing.assert_array_equal(xc, xp)
+
+
+@pytest.mark.parametrize("loop", ["persistent", "graph"])
+def test_ppr_graphs_without_edges(G, O, loop):
+    """No row has an in-edge: no work units, an empty packet table; every
+    seed keeps its mass (x = e_seed after one sweep), as in the oracle."""
+    lp = G.LOOP_GRAPH if loop == "graph" else G.LOOP_PERSISTENT
+    col = np.zeros(0, np.int32)
+    for m, seeds in ((5, [0, 3, 3]), (1, [0])):
+        rp, od = np.zeros(m + 1, np.int32), np.zeros(m, np.int32)
+        seeds = np.array(seeds, np.int32)
+        ref, ref_it = O.ppr_f64(rp, col, od, seeds, tol=1e-6, max_iter=100)
+        with G.Graph(rp, col, od, batched=True) as g:
+            x, it, st = g.ppr(seeds, tol=1e-6, max_iter=100, loop=lp)
+        np.testing.assert_array_equal(x, ref.astype(np.float32))
+        np.testing.assert_array_equal(it, ref_it)
