@@ -114,8 +114,23 @@ int dmalloc(void **p, size_t bytes, const char *what) {
   return GPR_OK;
 }
 
+namespace {
+thread_local std::vector<void *> *t_deferred = nullptr;
+}  // namespace
+
+DeferFrees::DeferFrees() : prev_(t_deferred) { t_deferred = &list_; }
+
+DeferFrees::~DeferFrees() {
+  t_deferred = prev_;
+  for (void *p : list_) dfree(p);
+}
+
 void dfree(void *p) {
   if (!p) return;
+  if (t_deferred) {
+    t_deferred->push_back(p);
+    return;
+  }
   std::unique_lock<std::mutex> lk(g_mu);
   auto it = g_live.find(p);
   if (it == g_live.end()) {

@@ -5,6 +5,8 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <vector>
+
 #include "gpr.h"
 
 namespace gpr {
@@ -19,6 +21,22 @@ int dalloc(T **p, size_t count, const char *what) {
   return dmalloc(reinterpret_cast<void **>(p), (count ? count : 1) * sizeof(T), what);
 }
 void dfree(void *p);
+
+// While an instance lives, dfree on this thread only records the pointers;
+// the destructor frees them.  A free synchronises the device (cudaFree, or
+// the block cache's wait before reuse), so code that overlaps a copy on one
+// stream with work on another holds one until both streams are done.
+class DeferFrees {
+ public:
+  DeferFrees();
+  ~DeferFrees();
+  DeferFrees(const DeferFrees &) = delete;
+  DeferFrees &operator=(const DeferFrees &) = delete;
+
+ private:
+  std::vector<void *> list_;
+  std::vector<void *> *prev_;
+};
 
 // True if `p` is device (or managed) memory of the current context.
 bool is_device_ptr(const void *p);
@@ -95,15 +113,21 @@ __host__ __device__ inline int slice_class(const PrClasses &c, int s) {
 int make_packets(long long *cost, int n_units, long long want, int **pk_out, int *npk_out,
                  cudaStream_t st);
 
+// Relabelled layout of a pull graph.  When col_ready is given, d_col may
+// still be arriving (a copy recorded on another stream): the build does all
+// that needs only the row offsets and out-degrees first, then waits for the
+// event and checks the column range before reading columns.
 int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
                     const int *d_outdeg, int lane_max, int chunk_min, int chunk,
-                    bool keep_csr, PrLayout *L, cudaStream_t st);
+                    bool keep_csr, PrLayout *L, cudaStream_t st, cudaEvent_t col_ready = nullptr);
 void free_pr_layout(PrLayout *L);
 
 // Validates a device CSR (rowptr[0] = 0, monotone, rowptr[m] = nnz, every
-// column in [0, ncols)) and, when d_outdeg is given, out-degrees >= 0.
+// column in [0, ncols) when d_col is given) and, when d_outdeg is given,
+// out-degrees >= 0.  validate_cols checks the columns alone.
 int validate_csr(int m, long long nnz, int ncols, const int *d_rowptr,
                  const int *d_col, const int *d_outdeg, cudaStream_t st);
+int validate_cols(long long nnz, int ncols, const int *d_col, cudaStream_t st);
 
 // ---------------------------------------------------------------------------
 // SpMV layout: natural row order.  Rows with more than sell_max entries are

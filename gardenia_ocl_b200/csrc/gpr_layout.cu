@@ -203,7 +203,7 @@ int validate_csr(int m, long long nnz, int ncols, const int *d_rowptr, const int
   GPR_TRY(dalloc(&flag, 1, "validation flag"));
   cudaMemsetAsync(flag, 0, sizeof(int), st);
   k_validate_rows<<<grid_for((long long)m + 1), 256, 0, st>>>(m, nnz, d_rowptr, d_outdeg, flag);
-  if (nnz > 0) {
+  if (nnz > 0 && d_col) {
     long long g = grid_for(nnz);
     if (g > 148 * 64) g = 148 * 64;
     k_validate_cols<<<(unsigned)g, 256, 0, st>>>(nnz, ncols, d_col, flag);
@@ -224,9 +224,33 @@ int validate_csr(int m, long long nnz, int ncols, const int *d_rowptr, const int
   return GPR_OK;
 }
 
+int validate_cols(long long nnz, int ncols, const int *d_col, cudaStream_t st) {
+  if (nnz <= 0) return GPR_OK;
+  int *flag = nullptr;
+  GPR_TRY(dalloc(&flag, 1, "validation flag"));
+  cudaMemsetAsync(flag, 0, sizeof(int), st);
+  long long g = grid_for(nnz);
+  if (g > 148 * 64) g = 148 * 64;
+  k_validate_cols<<<(unsigned)g, 256, 0, st>>>(nnz, ncols, d_col, flag);
+  int h = 0;
+  cudaError_t e = cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  gpr::dfree(flag);
+  if (e != cudaSuccess) {
+    set_error("CSR validation: %s", cudaGetErrorString(e));
+    return GPR_ECUDA;
+  }
+  if (h) {
+    set_error("malformed CSR (flags 0x%x: 1 rowptr[0]!=0, 2 rowptr[m]!=nnz, 4 rowptr not "
+              "monotone, 8 column out of range, 16 negative degree)", h);
+    return GPR_EINVAL;
+  }
+  return GPR_OK;
+}
+
 int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
                     const int *d_outdeg, int lane_max, int chunk_min, int chunk, bool keep_csr,
-                    PrLayout *L, cudaStream_t st) {
+                    PrLayout *L, cudaStream_t st, cudaEvent_t col_ready) {
   *L = PrLayout();
   L->m = m;
   L->nnz = nnz;
@@ -317,13 +341,8 @@ int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
   }
   GPR_TRY(dalloc(&L->long_col, (size_t)L->long_elems, "long rows"));
   GPR_TRY(dalloc(&L->chunk_row, (size_t)L->n_chunks, "chunk rows"));
-  if (L->n_long > 0) {
-    unsigned g = grid_for(32LL * L->n_long);
-    if (g > 148u * 32u) g = 148u * 32u;
-    k_fill_chunk_row<<<g, 256, 0, st>>>(L->n_long, L->row_cbeg, L->chunk_row);
-    k_fill_long<<<g, 256, 0, st>>>(L->n_long, m, L->perm, inv, d_rowptr, d_col, L->long_ptr,
-                                   L->long_col);
-  }
+  const unsigned g_long = std::min(grid_for(32LL * L->n_long), 148u * 32u);
+  if (L->n_long > 0) k_fill_chunk_row<<<g_long, 256, 0, st>>>(L->n_long, L->row_cbeg, L->chunk_row);
 
   // SELL-32 slices over rows [n_long, n_nz).
   GPR_TRY(dalloc(&L->slice_ptr, (size_t)L->n_slices + 1, "slice offsets"));
@@ -334,6 +353,17 @@ int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
                            cudaMemcpyDeviceToHost, st));
   GPR_CUDA(cudaStreamSynchronize(st));
   GPR_TRY(dalloc(&L->sell_col, (size_t)L->sell_elems, "sell slices"));
+
+  // Everything above needs only the row offsets and out-degrees; the column
+  // indices are read from here on.  When they are still being copied in
+  // (col_ready), wait for them and check their range first.
+  if (col_ready) {
+    GPR_CUDA(cudaStreamWaitEvent(st, col_ready, 0));
+    GPR_TRY(validate_cols(nnz, m, d_col, st));
+  }
+  if (L->n_long > 0)
+    k_fill_long<<<g_long, 256, 0, st>>>(L->n_long, m, L->perm, inv, d_rowptr, d_col, L->long_ptr,
+                                        L->long_col);
   if (L->n_slices > 0)
     k_fill_sell<<<grid_for(32LL * L->n_slices), 256, 0, st>>>(
         L->n_slices, m, C, L->perm, inv, d_rowptr, d_col, sdeg, L->slice_ptr, L->sell_col);

@@ -603,16 +603,54 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
   cudaStream_t st = g->st;
   void *rp = nullptr, *cp = nullptr, *dp = nullptr;
   bool orp = false, ocp = false, odp = false;
-  int rc = gpr::to_device(any_rowptr, sizeof(int) * ((size_t)m + 1), &rp, &orp, st, "rowptr");
-  if (rc == GPR_OK) rc = gpr::to_device(any_col, sizeof(int) * (size_t)nnz, &cp, &ocp, st, "col");
-  if (rc == GPR_OK)
-    rc = gpr::to_device(any_outdeg, sizeof(int) * (size_t)m, &dp, &odp, st, "outdeg");
-  if (rc == GPR_OK)
-    rc = gpr::validate_csr(m, nnz, m, (const int *)rp, (const int *)cp, (const int *)dp, st);
-  if (rc == GPR_OK)
-    rc = gpr::build_pr_layout(m, nnz, (const int *)rp, (const int *)cp, (const int *)dp,
-                              lane_max, chunk_min, chunk, keep_csr, &g->L, st);
-  cudaStreamSynchronize(st);
+  int rc = GPR_OK;
+  {
+    // No device-wide synchronisation (a free) while the column copy runs.
+    gpr::DeferFrees defer;
+    rc = gpr::to_device(any_rowptr, sizeof(int) * ((size_t)m + 1), &rp, &orp, st, "rowptr");
+    if (rc == GPR_OK)
+      rc = gpr::to_device(any_outdeg, sizeof(int) * (size_t)m, &dp, &odp, st, "outdeg");
+    // Column indices in host memory (the largest copy) go on a second stream
+    // after the row offsets and out-degrees, so that the layout's degree work
+    // runs while they arrive; the build waits for them before reading columns.
+    const bool host_col = nnz > 0 && any_col && !gpr::is_device_ptr(any_col);
+    cudaStream_t cs = nullptr;
+    cudaEvent_t ev_rows = nullptr, ev_col = nullptr;
+    if (rc == GPR_OK && host_col) {
+      const size_t bytes = sizeof(int) * (size_t)nnz;
+      rc = gpr::dmalloc(&cp, bytes, "col");
+      ocp = rc == GPR_OK;
+      if (rc == GPR_OK) {
+        cudaError_t e = cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_rows, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev_col, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_rows, st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(cs, ev_rows, 0);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(cp, any_col, bytes, cudaMemcpyHostToDevice, cs);
+        if (e == cudaSuccess) e = cudaEventRecord(ev_col, cs);
+        if (e != cudaSuccess) {
+          gpr::set_error("copy of col to the device: %s", cudaGetErrorString(e));
+          rc = GPR_ECUDA;
+        }
+      }
+    } else if (rc == GPR_OK) {
+      rc = gpr::to_device(any_col, sizeof(int) * (size_t)nnz, &cp, &ocp, st, "col");
+    }
+    if (rc == GPR_OK)
+      rc = gpr::validate_csr(m, nnz, m, (const int *)rp, host_col ? nullptr : (const int *)cp,
+                             (const int *)dp, st);
+    if (rc == GPR_OK)
+      rc = gpr::build_pr_layout(m, nnz, (const int *)rp, (const int *)cp, (const int *)dp,
+                                lane_max, chunk_min, chunk, keep_csr, &g->L, st,
+                                host_col ? ev_col : nullptr);
+    cudaStreamSynchronize(st);
+    if (cs) {
+      cudaStreamSynchronize(cs);  // the column copy is done before its buffer is freed
+      cudaStreamDestroy(cs);
+    }
+    if (ev_rows) cudaEventDestroy(ev_rows);
+    if (ev_col) cudaEventDestroy(ev_col);
+  }
   if (orp) gpr::dfree(rp);
   if (ocp) gpr::dfree(cp);
   if (odp) gpr::dfree(dp);
