@@ -139,10 +139,19 @@ def test_malformed_csr_rejected(G):
     with pytest.raises(G.GprError) as e:
         G.Graph(bad_rp, np.array([0, 1, 2], np.int32), np.ones(3, np.int32))
     assert e.value.status == G.GPR_EINVAL
-    with pytest.raises(G.GprError) as e:  # column out of range
-        G.Graph(np.array([0, 1, 2, 3], np.int32), np.array([0, 7, 1], np.int32),
-                np.ones(3, np.int32))
-    assert e.value.status == G.GPR_EINVAL
+    # columns out of range, from host arrays (checked by the layout build
+    # once their copy has landed) and from device arrays (checked up front)
+    import torch
+    rp, od = np.array([0, 1, 2, 3], np.int32), np.ones(3, np.int32)
+    for bad in ([0, 7, 1], [0, -1, 1]):
+        col = np.array(bad, np.int32)
+        for arrays in ((rp, col, od), tuple(torch.from_numpy(a).cuda() for a in (rp, col, od))):
+            with pytest.raises(G.GprError) as e:
+                G.Graph(*arrays)
+            assert e.value.status == G.GPR_EINVAL
+            assert "flags 0x8:" in str(e.value)
+    with G.Graph(*(torch.from_numpy(a).cuda() for a in (rp, np.array([0, 2, 1], np.int32), od))):
+        pass  # the same arrays with valid columns build
 
 
 def test_barrier_wait_is_bounded(G, O):
