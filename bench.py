@@ -744,6 +744,25 @@ def profile_ppr(args):
     return 0
 
 
+def profile_spmv(args):
+    """--profile-spmv calls of y += A x on the 27-point 128^3 stencil (for ncu)."""
+    import torch
+
+    import gardenia_ocl_b200 as G
+    A = G.gen_stencil27(128)
+    M = G.Matrix(A.rowptr, A.col, A.third, m=A.m, nnz=A.nnz)
+    x = torch.empty(A.m, dtype=torch.float32, device="cuda")
+    G.gen_uniform(A.m, 11, x)
+    y = torch.zeros(A.m, dtype=torch.float32, device="cuda")
+    for _ in range(args.profile_spmv):
+        M.spmv(x, y)
+    torch.cuda.synchronize()
+    log(json.dumps({"m": A.m, "nnz": A.nnz, "calls": args.profile_spmv}))
+    M.close()
+    A.close()
+    return 0
+
+
 def profile_symgs(args):
     """One SymGS apply of exactly --profile-symgs sweeps on the 27-point 128^3
     stencil with the 8-colour parity colouring (for ncu)."""
@@ -790,7 +809,11 @@ def main():
     ap.add_argument("--profile-symgs", type=int, default=0, metavar="SWEEPS",
                     help="one SymGS apply of SWEEPS sweeps on the 128^3 stencil "
                          "(the case profiled with ncu)")
+    ap.add_argument("--profile-spmv", type=int, default=0, metavar="CALLS",
+                    help="CALLS SpMV calls on the 128^3 stencil (the case profiled with ncu)")
     args = ap.parse_args()
+    if args.profile_spmv:
+        return profile_spmv(args)
     if args.profile_symgs:
         return profile_symgs(args)
     if args.profile_multigraph:

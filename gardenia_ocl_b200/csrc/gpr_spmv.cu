@@ -25,6 +25,10 @@ struct gpr_matrix {
 namespace {
 
 constexpr unsigned kFull = 0xffffffffu;
+// Entries per lane per round of a SELL row: each round loads kSpmvU column
+// indices and values, then gathers their x.  On the 27-point 128^3 stencil
+// 4 / 8 / 16 per round ran at 85% / 99% / 90% of the measured copy bandwidth.
+constexpr int kSpmvU = 8;
 
 struct SpArgs {
   int m, n_long, n_chunks, n_slices, chunk;
@@ -89,18 +93,18 @@ __device__ __forceinline__ void do_slice(const SpArgs &a, int s, int lane, uint6
   const float *pv = a.sell_val + b + lane;
   float acc = a.y[r];
   int j = 0;
-  for (; j + 4 <= d; j += 4) {
-    int c[4];
-    float v[4], xv[4];
+  for (; j + kSpmvU <= d; j += kSpmvU) {
+    int c[kSpmvU];
+    float v[kSpmvU], xv[kSpmvU];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
+    for (int q = 0; q < kSpmvU; ++q) {
       c[q] = ld_s32(pc + 32 * (j + q), pol);
       v[q] = ld_f32(pv + 32 * (j + q), pol);
     }
 #pragma unroll
-    for (int q = 0; q < 4; ++q) xv[q] = __ldg(a.x + c[q]);
+    for (int q = 0; q < kSpmvU; ++q) xv[q] = __ldg(a.x + c[q]);
 #pragma unroll
-    for (int q = 0; q < 4; ++q) acc = __fadd_rn(acc, __fmul_rn(xv[q], v[q]));
+    for (int q = 0; q < kSpmvU; ++q) acc = __fadd_rn(acc, __fmul_rn(xv[q], v[q]));
   }
   for (; j < d; ++j) {
     const int c = ld_s32(pc + 32 * j, pol);
