@@ -117,3 +117,21 @@ def test_ppr_graphs_without_edges(G, O, loop):
             x, it, st = g.ppr(seeds, tol=1e-6, max_iter=100, loop=lp)
         np.testing.assert_array_equal(x, ref.astype(np.float32))
         np.testing.assert_array_equal(it, ref_it)
+
+
+def test_ppr_barrier_wait_is_bounded(G, O):
+    """A grid barrier that expects one CTA too many never opens: every wait
+    gives up after timeout_s, the solve reports ETIMEOUT, and the graph
+    still solves correctly afterwards (no GPU fault, no hang)."""
+    rp, col, od = O.rmat_graph(10, 8, seed=1)
+    seeds = O.uniform_int(8, 5, len(rp) - 1)
+    with G.Graph(rp, col, od, batched=True) as g:
+        o = G.options(tol=1e-6, max_iter=10, loop=G.LOOP_PERSISTENT, timeout_s=0.05)
+        o.reserved[0] = 1
+        with pytest.raises(G.GprError) as e:
+            g.ppr(seeds, opts=o)
+        assert e.value.status == G.GPR_ETIMEOUT
+        x, it, st = g.ppr(seeds, tol=1e-6, max_iter=100)
+    ref, ref_it = O.ppr_f64(rp, col, od, seeds, tol=1e-6, max_iter=100)
+    assert np.all(l1_per_vector(x, ref) <= 1e-5)
+    assert np.all(np.abs(it - ref_it) <= 1)
