@@ -62,9 +62,17 @@ __global__ void __launch_bounds__(kSymgsBlock, 1) k_symgs(SymgsArgs a) {
   const int gw = blockIdx.x * (kSymgsBlock / 32) + (threadIdx.x >> 5);
   const int nw = gridDim.x * (kSymgsBlock / 32);
   const Policies pol = make_policies();
+  // A pass sets each row of its colour from the x of other colours only (no
+  // row has a neighbour of its own colour, the diagonal is not in the sum),
+  // so a pass that repeats the colour of the pass before it -- the turn from
+  // forward to backward, and colour 0 from one sweep to the next -- would
+  // write the same values again: it is skipped, with its barrier.
+  int prev = -1;
   for (int sw = 0; sw < a.sweeps; ++sw) {
     for (int p = 0; p < 2 * a.nc; ++p) {
       const int c = p < a.nc ? p : 2 * a.nc - 1 - p;
+      if (c == prev) continue;
+      prev = c;
       for (int s = a.cslice[c] + gw; s < a.cslice[c + 1]; s += nw) {
         const int k = s * 32 + lane;
         const int r = a.srow[k], len = a.slen[k];
