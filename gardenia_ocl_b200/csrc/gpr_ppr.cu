@@ -1,5 +1,6 @@
 // Batched personalized PageRank: k seed vectors solved together as a fused
-// pull-SpMM in one persistent cooperative launch.
+// pull-SpMM, all sweeps in one persistent cooperative launch or (loop
+// GPR_LOOP_GRAPH) one launch per sweep inside a CUDA-graph while loop.
 //
 // No reference file: the reference computes one global PageRank
 // (src/pr/omp_base.cc).  For each vector q with seed s_q:
@@ -18,11 +19,13 @@
 //   C = 4 (contiguous, one vector load per gather), so one warp-wide load
 //   instruction serves R rows and 8 gathers per lane are in flight.
 // Rows with in-degree 0 hold x = 0 except at seeds, so only rows with
-// in-edges and the k seed rows are updated.  Rows above chunk_min in-edges
-// are cut into chunks whose K-wide partial sums the last arriving warp adds
-// in a fixed order.  Residual and dangling sums are reduced per CTA and then
-// over CTAs in CTA order by the last CTA at the grid barrier (deterministic);
-// every barrier wait is bounded.
+// in-edges and the k seed rows are updated.  Rows longer than 8 sub-group
+// rounds are cut into chunks of 8192 / L edges whose K-wide partial sums the
+// last arriving warp adds in a fixed order; the other rows go in groups of R.
+// Warps take packets (runs of these units of about equal cost) from one
+// queue.  Residual and dangling sums are reduced per CTA and then over CTAs
+// in CTA order by the last CTA to finish the sweep (deterministic); every
+// barrier wait is bounded.
 #include <cub/cub.cuh>
 #include <cuda_bf16.h>
 #include <math.h>
@@ -31,6 +34,7 @@
 #include <algorithm>
 #include <vector>
 
+#include "gpr_device.cuh"
 #include "gpr_internal.cuh"
 
 namespace {
@@ -89,17 +93,8 @@ struct Shape {
   static constexpr int min_ctas = K <= 16 ? 3 : K <= 64 ? 2 : 4;
 };
 
-__device__ __forceinline__ unsigned ld_acquire(const unsigned *p) {
-  unsigned v;
-  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
-  return v;
-}
-
-__device__ __forceinline__ long long global_ns() {
-  long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-  return t;
-}
+using gpr::dev::global_ns;
+using gpr::dev::ld_acquire;
 
 __device__ __forceinline__ int ld_idx(const int *p) {
   int v;
