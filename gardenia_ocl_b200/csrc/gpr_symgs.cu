@@ -33,11 +33,15 @@ using namespace gpr::dev;
 namespace {
 
 constexpr int kSymgsBlock = 1024;
-// Entries per lane in flight: 24 is the most that fits the 64 registers of a
-// 1024-thread CTA without spills (a 27-point row, 26 off-diagonal entries,
-// takes two rounds).  Measured per sweep on the 128^3 stencil: 16 -> 0.296 ms,
-// 24 -> 0.288, 28 -> 0.302 and 32 -> 0.307 (spills).
-constexpr int kSymgsU = 24;
+// Two 1024-thread CTAs per SM (32 registers) and 4 entries per lane in
+// flight.  A pass is a chain of dependent loads per slice (row data, entries,
+// the gathered x) ended by a grid barrier; with twice the warps a colour's
+// 8,192 slices of the 128^3 stencil take one slice per warp instead of two.
+// Measured per sweep on that stencil (same box): one CTA per SM with 24
+// entries in flight 0.264 ms; two CTAs with 2 / 3 / 4 / 6 / 8 entries 0.218 /
+// 0.212 / 0.212 / 0.220 / 0.245 ms (8: spills).
+constexpr int kSymgsU = 4;
+constexpr int kSymgsCtasPerSm = 2;
 
 struct SymgsArgs {
   int nc;
@@ -57,7 +61,7 @@ struct SymgsArgs {
   long long timeout_ns;
 };
 
-__global__ void __launch_bounds__(kSymgsBlock, 1) k_symgs(SymgsArgs a) {
+__global__ void __launch_bounds__(kSymgsBlock, kSymgsCtasPerSm) k_symgs(SymgsArgs a) {
   const int lane = threadIdx.x & 31;
   const int gw = blockIdx.x * (kSymgsBlock / 32) + (threadIdx.x >> 5);
   const int nw = gridDim.x * (kSymgsBlock / 32);
@@ -307,7 +311,7 @@ int gpr_symgs_create(int m, long long nnz, const int *any_Ap, const int *any_Aj,
     }
     int most = 0;  // slices of the largest colour
     for (int c = 0; c < n_colors; ++c) most = std::max(most, co[c + 1] - co[c]);
-    h->grid = std::max(1, std::min(sms, (int)gpr::ceil_div(gpr::ceil_div(most, 32), 32)));
+    h->grid = std::max(1, std::min(sms * per_sm, (int)gpr::ceil_div(gpr::ceil_div(most, 32), 32)));
   }
   if (rc != GPR_OK) {
     destroy_symgs(h);
