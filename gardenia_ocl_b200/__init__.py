@@ -775,7 +775,7 @@ def set_device(device: int):
 
 
 def release_cached() -> int:
-    """Return the library's cached device blocks to the driver; returns bytes."""
+    """Return the library's cached device blocks to the CUDA driver; returns bytes."""
     n = C.c_longlong()
     _check(lib().gpr_release_cached(C.byref(n)))
     return n.value

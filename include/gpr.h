@@ -329,7 +329,7 @@ int gpr_free(void *d_ptr);
  * (at most 24 GiB, reused by later requests that fit them within 1/8), so
  * one-shot calls do not map and unmap gigabytes each time.  Freeing a block
  * synchronises the device first, as cudaFree does.  gpr_release_cached returns
- * every cached block to the driver (released_bytes may be NULL);
+ * every cached block to the CUDA driver (released_bytes may be NULL);
  * gpr_cached_bytes reports how much is held. */
 int gpr_release_cached(long long *released_bytes);
 int gpr_cached_bytes(long long *bytes);
