@@ -200,6 +200,36 @@ __device__ __forceinline__ double block_sum_double(double v) {
 // CTA order (deterministic) into *sum_out before it opens the next
 // generation.  Waits are bounded by timeout_ns of %globaltimer; on expiry
 // status[0] bit 0 is raised and false is returned.  Call from every thread.
+// Grid barrier without a reduction: `count` (zeroed before the launch) only
+// grows; episode e of a launch (1, 2, ...) is complete when it reaches
+// expect * e, so no CTA has to publish anything after the last arrival and a
+// waiter sees the release on its next poll.  The comparison is wrap-safe.
+// The wait is bounded by timeout_ns: on expiry status[0] bit 0 is raised and
+// false is returned.
+__device__ __forceinline__ bool grid_barrier_count(unsigned *count, unsigned target, int *status,
+                                                   long long timeout_ns) {
+  __shared__ int s_ok;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(count, 1u);
+    s_ok = 1;
+    const long long t0 = global_ns();
+    unsigned spins = 0;
+    while ((int)(ld_acquire(count) - target) < 0) {
+      if ((++spins & 63u) == 0 && global_ns() - t0 > timeout_ns) {
+        atomicOr(status, 1);
+        s_ok = 0;
+        break;
+      }
+      __nanosleep(50);
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return s_ok != 0;
+}
+
 __device__ __forceinline__ bool grid_barrier(unsigned *bar, unsigned expect, double *cta_part,
                                              double cta_value, double *sum_out, int *status,
                                              long long timeout_ns) {

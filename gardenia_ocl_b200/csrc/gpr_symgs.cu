@@ -72,6 +72,7 @@ __global__ void __launch_bounds__(kSymgsBlock, kSymgsCtasPerSm) k_symgs(SymgsArg
   // forward to backward, and colour 0 from one sweep to the next -- would
   // write the same values again: it is skipped, with its barrier.
   int prev = -1;
+  unsigned episode = 0;  // barriers passed in this launch
   for (int sw = 0; sw < a.sweeps; ++sw) {
     for (int p = 0; p < 2 * a.nc; ++p) {
       const int c = p < a.nc ? p : 2 * a.nc - 1 - p;
@@ -104,8 +105,7 @@ __global__ void __launch_bounds__(kSymgsBlock, kSymgsCtasPerSm) k_symgs(SymgsArg
           if (d != 0.f) a.x[r] = __fdiv_rn(__fsub_rn(a.b[r], rsum), d);
         }
       }
-      if (!grid_barrier(a.bar, a.bar_expect, nullptr, 0.0, nullptr, a.status, a.timeout_ns))
-        return;
+      if (!grid_barrier_count(a.bar, a.bar_expect * ++episode, a.status, a.timeout_ns)) return;
     }
   }
 }
