@@ -558,6 +558,19 @@ def multigraph_leg(G, torch, dev, stream, plain_gteps, args):
                      "achieved_gbs": byts / (st.loop_ms / 1e3) / 1e9,
                      "frac": byts / (st.loop_ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind,
                      "gpu_launches": st.gpu_launches}
+    # the FP32 solve again as a CUDA-graph loop (one launch per sweep)
+    best = None
+    for _ in range(2):
+        scores.copy_(init)
+        _, it, res, st = mg.pagerank(scores, tol=TOL, max_iter=MG_MAX_ITER, damping=DAMPING,
+                                     loop=G.LOOP_GRAPH)
+        if best is None or st.loop_ms < best[0].loop_ms:
+            best = (st, it.copy())
+    st, it = best
+    edges = float((nnz_g * it).sum())
+    out["fp32_graph_loop"] = {"launch_sweeps": st.iterations, "loop_ms": st.loop_ms,
+                              "gteps": edges / (st.loop_ms / 1e3) / 1e9,
+                              "gpu_launches": st.gpu_launches}
     mg.close()
     A.close()
     return out

@@ -83,6 +83,7 @@ struct MultiArgs {
   double tol;
   int max_iter, bar_expect;
   long long timeout_ns;
+  unsigned long long cond;  // graph mode: while-node condition handle (0: none)
 };
 
 template <typename T>
@@ -246,6 +247,24 @@ __device__ __forceinline__ void finish_units(const MultiArgs &a, int g, int done
 // queue head and graph counter that sweep it + 2 reuses, and opens the next
 // generation.  Waits are bounded by timeout_ns; on expiry status[0] bit 0 is
 // raised and the caller returns.
+// Closing of sweep it, by one thread of the last CTA to finish it (every
+// CTA's work of the sweep visible): settles the graphs that have no heavy
+// units (their residual is 0 from sweep 2 on) and resets the queue head and
+// graph counter that sweep it + 2 reuses.
+__device__ void multi_close(const MultiArgs &a, int it) {
+  if (it >= 2)
+    for (int i = 0; i < a.n_lazy; ++i) {
+      const int g = a.lazy[i];
+      if (it < __ldcg(a.stop + g)) {
+        a.gres[g] = 0.0;
+        if (0.0 < a.tol || it + 1 >= a.cap[g]) atomicExch(a.stop + g, it + 1);
+        else atomicAdd(a.n_next + ((it + 1) & 1), 1);
+      }
+    }
+  atomicExch(a.wq + (it & 1), 0);
+  atomicExch(a.n_next + (it & 1), 0);
+}
+
 __device__ bool multi_barrier(const MultiArgs &a, int it) {
   __shared__ int s_state;
   __syncthreads();
@@ -256,17 +275,7 @@ __device__ bool multi_barrier(const MultiArgs &a, int it) {
     s_state = 0;
     if (arrived == (unsigned)a.bar_expect - 1u) {
       __threadfence();
-      if (it >= 2)
-        for (int i = 0; i < a.n_lazy; ++i) {
-          const int g = a.lazy[i];
-          if (it < __ldcg(a.stop + g)) {
-            a.gres[g] = 0.0;
-            if (0.0 < a.tol || it + 1 >= a.cap[g]) atomicExch(a.stop + g, it + 1);
-            else atomicAdd(a.n_next + ((it + 1) & 1), 1);
-          }
-        }
-      atomicExch(a.wq + (it & 1), 0);
-      atomicExch(a.n_next + (it & 1), 0);
+      multi_close(a, it);
       atomicExch(a.bar, 0u);
       __threadfence();
       atomicAdd(a.bar + 1, 1u);
@@ -288,47 +297,56 @@ __device__ bool multi_barrier(const MultiArgs &a, int it) {
   return s_state != 2;
 }
 
+// The units of sweep it: warps take packets from the queue, skip the units
+// of frozen graphs, and close the graphs whose last unit they finish.
+template <int U, int U4, typename T>
+__device__ __forceinline__ void multi_sweep(const MultiArgs &a, int it, int lane,
+                                            const Policies &pol) {
+  const T *cin = static_cast<const T *>((it & 1) ? a.c1 : a.c0);
+  T *cout = static_cast<T *>((it & 1) ? a.c0 : a.c1);
+  const GlobalGather<T> gat{cin, pol.keep};
+  const int n_pk = it < 2 ? a.n_pk : a.n_hpk;
+  for (;;) {
+    int p = 0;
+    if (lane == 0) p = atomicAdd(a.wq + (it & 1), 1);
+    p = __shfl_sync(kFull, p, 0);
+    if (p >= n_pk) break;
+    const int u0 = __ldg(a.pk + p), u1 = __ldg(a.pk + p + 1);
+    int cur = -1, done = 0;
+    bool act = false;
+    float base = 0.f;
+    for (int u = u0; u < u1; ++u) {
+      const int4 md = __ldg(a.meta + u);
+      const int g = md.w >> 8;
+      if (g != cur) {
+        if (done) finish_units(a, cur, done, it, lane);
+        cur = g;
+        done = 0;
+        act = it < __ldcg(a.stop + g);
+        base = __fdiv_rn(__fsub_rn(1.0f, a.damp), __int2float_rn(__ldg(a.gm + g)));
+      }
+      if (!act) continue;
+      const int kind = (md.w >> 4) & 15;
+      double err;
+      if (kind == kUnitChunk) err = m_chunk<U4>(a, gat, cout, u, md, base, lane, pol);
+      else if (kind == kUnitSlice) err = m_slice<U>(a, gat, cout, u, md, base, lane, pol);
+      else err = m_zero(a, cout, md, base, lane, it, pol);
+      err = warp_sum(err);
+      if (lane == 0) a.uerr[u] = err;
+      ++done;
+    }
+    if (done) finish_units(a, cur, done, it, lane);
+  }
+}
+
+// All sweeps in one cooperative launch, a bounded grid barrier between them.
 template <int U, int U4, typename T>
 __global__ void __launch_bounds__(kMultiBlock, 1) k_multi(MultiArgs a) {
   const int lane = threadIdx.x & 31;
   const Policies pol = make_policies();
   int it = 0;
   while (it < a.max_iter) {
-    const T *cin = static_cast<const T *>((it & 1) ? a.c1 : a.c0);
-    T *cout = static_cast<T *>((it & 1) ? a.c0 : a.c1);
-    const GlobalGather<T> gat{cin, pol.keep};
-    const int n_pk = it < 2 ? a.n_pk : a.n_hpk;
-    for (;;) {
-      int p = 0;
-      if (lane == 0) p = atomicAdd(a.wq + (it & 1), 1);
-      p = __shfl_sync(kFull, p, 0);
-      if (p >= n_pk) break;
-      const int u0 = __ldg(a.pk + p), u1 = __ldg(a.pk + p + 1);
-      int cur = -1, done = 0;
-      bool act = false;
-      float base = 0.f;
-      for (int u = u0; u < u1; ++u) {
-        const int4 md = __ldg(a.meta + u);
-        const int g = md.w >> 8;
-        if (g != cur) {
-          if (done) finish_units(a, cur, done, it, lane);
-          cur = g;
-          done = 0;
-          act = it < __ldcg(a.stop + g);
-          base = __fdiv_rn(__fsub_rn(1.0f, a.damp), __int2float_rn(__ldg(a.gm + g)));
-        }
-        if (!act) continue;
-        const int kind = (md.w >> 4) & 15;
-        double err;
-        if (kind == kUnitChunk) err = m_chunk<U4>(a, gat, cout, u, md, base, lane, pol);
-        else if (kind == kUnitSlice) err = m_slice<U>(a, gat, cout, u, md, base, lane, pol);
-        else err = m_zero(a, cout, md, base, lane, it, pol);
-        err = warp_sum(err);
-        if (lane == 0) a.uerr[u] = err;
-        ++done;
-      }
-      if (done) finish_units(a, cur, done, it, lane);
-    }
+    multi_sweep<U, U4, T>(a, it, lane, pol);
     if (!multi_barrier(a, it)) return;
     const int n = __ldcg(a.n_next + ((it + 1) & 1));
     ++it;
@@ -338,6 +356,48 @@ __global__ void __launch_bounds__(kMultiBlock, 1) k_multi(MultiArgs a) {
     a.status[1] = it;
     a.status[2] = 1;
   }
+}
+
+// One sweep per launch (graph mode): the body of a CUDA-graph while node.
+// status[1] holds the sweeps done and status[2] the done flag, so the
+// captured launch needs no host input; the last CTA to finish a sweep closes
+// it (no CTA waits for another, so the grid need not be co-resident).  The
+// node's condition starts at 1 and is only cleared: by the CTA that closes
+// the last sweep, by a launch that finds the solve done, and by CTA 0 of the
+// max_iter-th launch (status[3] counts launches).
+template <int U, int U4, typename T>
+__global__ void __launch_bounds__(kMultiBlock, 1) k_multi_step(MultiArgs a) {
+  __shared__ int s_it, s_last;
+  if (threadIdx.x == 0) {
+    const int n_done = *(volatile int *)(a.status + 1);
+    const bool fin = *(volatile int *)(a.status + 2) != 0;
+    s_it = !fin && n_done < a.max_iter ? n_done : -1;
+    if (a.cond && blockIdx.x == 0) {
+      const int n = atomicAdd(a.status + 3, 1) + 1;
+      if (s_it < 0 || n >= a.max_iter) cudaGraphSetConditional(a.cond, 0u);
+    }
+  }
+  __syncthreads();
+  const int it = s_it;
+  if (it < 0) return;
+  const Policies pol = make_policies();
+  multi_sweep<U, U4, T>(a, it, threadIdx.x & 31, pol);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(a.bar, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last || threadIdx.x != 0) return;
+  __threadfence();
+  multi_close(a, it);
+  atomicExch(a.bar, 0u);
+  const int n = __ldcg(a.n_next + ((it + 1) & 1));
+  const bool done = n == 0 || it + 1 >= a.max_iter;
+  a.status[1] = it + 1;
+  if (done) a.status[2] = 1;
+  __threadfence();
+  if (a.cond && done) cudaGraphSetConditional(a.cond, 0u);
 }
 
 template <typename T>
@@ -539,6 +599,10 @@ namespace {
 
 const void *multi_kernel(bool bf) {
   return bf ? (const void *)k_multi<16, 4, bf16> : (const void *)k_multi<16, 4, float>;
+}
+
+const void *multi_step_kernel(bool bf) {
+  return bf ? (const void *)k_multi_step<16, 4, bf16> : (const void *)k_multi_step<16, 4, float>;
 }
 
 void destroy_multi(gpr_multigraph *g) {
@@ -877,6 +941,45 @@ int solve_phase(gpr_multigraph *g, float *d_scores, const gpr_pr_opts &o, bool b
   a.n_hpk = g->n_hpk;
   a.n_pk = g->n_pk;
   a.timeout_ns = (long long)(o.timeout_s * 1e9);
+  a.cond = 0;
+  // Graph mode when asked for, or when the persistent kernel cannot be
+  // co-resident: the sweep loop as a CUDA-graph while node whose body is one
+  // k_multi_step launch, built here and released after the phase.
+  const bool graph_mode = o.loop == GPR_LOOP_GRAPH || !g->coop_ok;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  if (max_cap > 0 && graph_mode) {
+    cudaGraphConditionalHandle h = 0;
+    cudaGraphNodeParams cp = {};
+    cudaGraphNode_t cn = nullptr, kn = nullptr;
+    cudaError_t e = cudaGraphCreate(&graph, 0);
+    if (e == cudaSuccess)
+      e = cudaGraphConditionalHandleCreate(&h, graph, 1u, cudaGraphCondAssignDefault);
+    if (e == cudaSuccess) {
+      cp.type = cudaGraphNodeTypeConditional;
+      cp.conditional.handle = h;
+      cp.conditional.type = cudaGraphCondTypeWhile;
+      cp.conditional.size = 1;
+      e = cudaGraphAddNode(&cn, graph, nullptr, 0, &cp);
+    }
+    MultiArgs ac = a;
+    ac.cond = h;
+    void *kargs[] = {&ac};
+    cudaKernelNodeParams kp;
+    memset(&kp, 0, sizeof(kp));
+    kp.func = const_cast<void *>(multi_step_kernel(bf));
+    kp.gridDim = dim3(g->grid);
+    kp.blockDim = dim3(kMultiBlock);
+    kp.kernelParams = kargs;
+    if (e == cudaSuccess) e = cudaGraphAddKernelNode(&kn, cp.conditional.phGraph_out[0], nullptr, 0, &kp);
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (e != cudaSuccess) {
+      if (exec) cudaGraphExecDestroy(exec);
+      if (graph) cudaGraphDestroy(graph);
+      gpr::set_error("multi-graph loop graph: %s", cudaGetErrorString(e));
+      return GPR_ECUDA;
+    }
+  }
   int launches = 0;
   GPR_CUDA(cudaEventRecord(g->e0, st));
   if (bf)
@@ -887,7 +990,16 @@ int solve_phase(gpr_multigraph *g, float *d_scores, const gpr_pr_opts &o, bool b
                                                                         d_scores, g->s, g->c0, g->c1);
   ++launches;
   GPR_CUDA(cudaEventRecord(g->e2, st));
-  if (max_cap > 0) {
+  if (max_cap > 0 && graph_mode) {
+    cudaError_t e = cudaGraphLaunch(exec, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaGraphExecDestroy(exec);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) {
+      gpr::set_error("multi-graph loop graph: %s", cudaGetErrorString(e));
+      return GPR_ECUDA;
+    }
+  } else if (max_cap > 0) {
     void *args[] = {&a};
     cudaError_t e = cudaLaunchCooperativeKernel(multi_kernel(bf), dim3(g->grid), dim3(kMultiBlock),
                                                 args, 0, st);
@@ -916,7 +1028,7 @@ int solve_phase(gpr_multigraph *g, float *d_scores, const gpr_pr_opts &o, bool b
   out->iterations = max_cap > 0 ? hs[1] : 0;
   out->solve_ms = ms;
   out->loop_ms = lms;
-  out->gpu_launches = launches;
+  out->gpu_launches = launches + (max_cap > 0 && graph_mode ? hs[3] : 0);
   double rmax = 0.0;
   for (double r : *res) rmax = std::max(rmax, r);
   out->residual = rmax;
@@ -953,10 +1065,6 @@ int multi_pagerank_impl(gpr_multigraph *g, float *any_scores, const gpr_pr_opts 
   if (!any_scores) {
     gpr::set_error("gpr_multigraph_pagerank: NULL scores");
     return GPR_EINVAL;
-  }
-  if (!g->coop_ok) {
-    gpr::set_error("gpr_multigraph_pagerank: the device cannot co-schedule the persistent kernel");
-    return GPR_EUNSUPPORTED;
   }
   cudaStream_t st = g->st;
   float *d_scores = any_scores;

@@ -188,7 +188,9 @@ int gpr_pagerank_push(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts,
  * gpr_multigraph_pagerank solves every graph as gpr_pagerank would solve it
  * alone -- base (1 - kDamp) / m_g, its own L1 residual, stop after its first
  * sweep with residual < tol or after max_iter sweeps -- all graphs in one
- * persistent launch.  any_scores: all vertices, initialised by the caller
+ * persistent launch (opts->loop GPR_LOOP_GRAPH, or a device that cannot
+ * co-schedule it: one launch per sweep in a CUDA-graph while loop, same
+ * results).  any_scores: all vertices, initialised by the caller
  * (the reference uses 1/m_g, src/pr/main.cc:27-28), updated in place.
  * h_iters / h_residuals (n_graphs entries each, may be NULL) receive each
  * graph's sweeps and last residual.  precision GPR_PREC_FP32, or

@@ -171,3 +171,31 @@ def test_barrier_timeout_is_reported(G, O):
         assert e.value.status == G.GPR_ETIMEOUT
         s, iters, _, _ = mg.pagerank(tol=1e-6, max_iter=20)  # still usable
         assert iters.min() > 0
+
+
+@pytest.mark.parametrize("prec", ["fp32", "bf16"])
+def test_graph_loop_matches_persistent(G, O, batch, prec):
+    """GPR_LOOP_GRAPH runs one sweep per launch inside a CUDA-graph while
+    loop (the last CTA to finish a sweep closes it, no CTA waits for another);
+    the sweep code is the persistent kernel's, so scores, per-graph sweep
+    counts and residuals are bit-identical."""
+    rp, col, od, voff = batch
+    p = G.PREC_BF16 if prec == "bf16" else G.PREC_FP32
+    with G.MultiGraph(rp, col, od, voff) as mg:
+        s0, it0, r0, st0 = mg.pagerank(tol=1e-6, max_iter=100, precision=p, loop=G.LOOP_PERSISTENT)
+        s1, it1, r1, st1 = mg.pagerank(tol=1e-6, max_iter=100, precision=p, loop=G.LOOP_GRAPH)
+    np.testing.assert_array_equal(s0, s1)
+    np.testing.assert_array_equal(it0, it1)
+    np.testing.assert_array_equal(r0, r1)
+    assert st1.iterations == st0.iterations
+    assert st1.gpu_launches > st0.gpu_launches  # one launch per sweep
+
+
+def test_graph_loop_caps_at_max_iter(G, O, batch):
+    rp, col, od, voff = batch
+    with G.MultiGraph(rp, col, od, voff) as mg:
+        s1, it1, _, st1 = mg.pagerank(tol=0.0, max_iter=6, loop=G.LOOP_GRAPH)
+        s0, it0, _, st0 = mg.pagerank(tol=0.0, max_iter=6)
+    assert st1.iterations == 6 and it1.max() == 6
+    np.testing.assert_array_equal(s0, s1)
+    np.testing.assert_array_equal(it0, it1)
