@@ -315,6 +315,11 @@ def run_ours(args):
     accuracy = {"fp64_residual_l1": resid,
                 "l1_error_bound_vs_fixed_point": resid / (1.0 - float(DAMPING)),
                 "sweeps_per_solve": sweeps_per_solve}
+    x_star, fp_it, fp_delta = fp64_fixed_point(torch, csr, m, scores)
+    accuracy.update(errors_vs(x_star, scores))
+    accuracy["fp64_fixed_point"] = {"how": "PyTorch FP64 sparse mat-vec on the GPU from the "
+                                           "solver's result", "iterations": fp_it,
+                                    "last_l1_change": fp_delta}
 
     line = {"metric": "pagerank_gteps_rmat24", "value": gteps, "unit": "GTEPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -357,7 +362,7 @@ def run_ours(args):
                                "via gpr_page_rank, pinned host buffers"}
 
     if not args.no_forms:
-        line["forms"] = forms_leg(G, torch, dev, g, m, nnz, gteps / world, args)
+        line["forms"] = forms_leg(G, torch, dev, g, m, nnz, gteps / world, args, x_star)
         line["forms"]["pr_bf16_refined"]["time_to_solution_vs_plain"] = (
             (ms / args.steps) / line["forms"]["pr_bf16_refined"]["loop_ms"])
     if not args.no_multigraph:
@@ -393,7 +398,42 @@ def run_ours(args):
     return 0
 
 
-def forms_leg(G, torch, dev, g, m, nnz, plain_gteps, args):
+def fp64_fixed_point(torch, csr, m, x0):
+    """FP64 fixed point of the plain recurrence x = (1 - d) / m + d A x
+    (A[v, u] = 1 / outdeg[u] over the in-CSR, d = (double)0.85f, as the
+    reference's FP64 restatement), computed with PyTorch's FP64 sparse
+    matrix-vector product on the GPU from x0 until the L1 change is below
+    1e-13.  A checker for the accuracy report: the solvers are not involved.
+    Returns (x, iterations, last L1 change)."""
+    import warnings
+    warnings.filterwarnings("ignore", message="Sparse")  # beta-status notices of torch.sparse
+    dev = x0.device
+    rp = torch.from_numpy(csr.rowptr.to_numpy().astype(np.int64)).to(dev)
+    col = torch.from_numpy(csr.col.to_numpy().astype(np.int64)).to(dev)
+    od = torch.from_numpy(csr.third.to_numpy()).to(dev).double()
+    inv = torch.where(od > 0, 1.0 / od.clamp(min=1.0), torch.zeros_like(od))
+    A = torch.sparse_csr_tensor(rp, col, inv[col], size=(m, m))
+    del rp, col, od, inv
+    d = float(np.float32(DAMPING))
+    base = (1.0 - d) / m
+    x = x0.double()
+    delta, k = float("inf"), 0
+    while k < 400 and delta >= 1e-13:
+        xn = base + d * torch.mv(A, x)
+        delta = float((xn - x).abs().sum())
+        x, k = xn, k + 1
+    del A
+    return x, k, delta
+
+
+def errors_vs(x_star, s):
+    """Max and L1 error of a float32 score vector against the FP64 fixed point."""
+    e = (s.double() - x_star).abs()
+    return {"l1_error_vs_fp64_fixed_point": float(e.sum()),
+            "max_error_vs_fp64_fixed_point": float(e.max())}
+
+
+def forms_leg(G, torch, dev, g, m, nnz, plain_gteps, args, x_star=None):
     """The forms the metric compares with the plain FP32 path, on the same
     graph: batched personalized PageRank (k seed vectors, one persistent
     launch) in FP32 and in BF16 with FP32 refinement.  Rates are edge-vector
@@ -415,6 +455,8 @@ def forms_leg(G, torch, dev, g, m, nnz, plain_gteps, args):
         "sweeps": best.iterations, "refine_sweeps": best.refine_iterations,
         "loop_ms": best.loop_ms, "gteps": nnz * best.iterations / (best.loop_ms / 1e3) / 1e9,
         "time_to_solution_vs_plain": None, "l1_error_bound_vs_fixed_point": resid / (1 - 0.85)}
+    if x_star is not None:
+        out["pr_bf16_refined"].update(errors_vs(x_star, scores))
     # push direction (atomic scatter) on the same graph, FP32
     best = None
     for _ in range(3):
@@ -426,6 +468,8 @@ def forms_leg(G, torch, dev, g, m, nnz, plain_gteps, args):
                            "gteps": nnz * best.iterations / (best.loop_ms / 1e3) / 1e9,
                            "vs_plain_fp32": nnz * best.iterations / (best.loop_ms / 1e3) / 1e9
                            / plain_gteps}
+    if x_star is not None:
+        out["pr_push_fp32"].update(errors_vs(x_star, scores))
     rng = np.random.default_rng(5)
     for k, prec, name in ((8, G.PREC_FP32, "ppr_k8_fp32"), (32, G.PREC_FP32, "ppr_k32_fp32"),
                           (32, G.PREC_BF16, "ppr_k32_bf16_refined")):
