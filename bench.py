@@ -426,6 +426,37 @@ def fp64_fixed_point(torch, csr, m, x0):
     return x, k, delta
 
 
+def ppr_fp64_fixed_point(torch, csr, m, seeds, x0):
+    """FP64 fixed point of the batched personalized PageRank recurrence (the
+    solver's): for vector q with seed s_q,
+      x_q = d A x_q + [v == s_q] ((1 - d) + d * sum of x_q over out-degree-0 v),
+    A[v, u] = 1 / outdeg[u] over the in-CSR, d = (double)0.85f, computed with
+    PyTorch's FP64 sparse x dense product on the GPU from x0 (m x k) until
+    every vector's L1 change is below 1e-13.  A checker only."""
+    import warnings
+    warnings.filterwarnings("ignore", message="Sparse")
+    dev = x0.device
+    rp = torch.from_numpy(csr.rowptr.to_numpy().astype(np.int64)).to(dev)
+    col = torch.from_numpy(csr.col.to_numpy().astype(np.int64)).to(dev)
+    od = torch.from_numpy(csr.third.to_numpy()).to(dev).double()
+    A = torch.sparse_csr_tensor(rp, col, (1.0 / od.clamp(min=1.0))[col], size=(m, m))
+    dang = (od == 0).double()
+    del rp, col, od
+    k = x0.shape[1]
+    rows = torch.from_numpy(np.asarray(seeds, np.int64)).to(dev)
+    cols = torch.arange(k, device=dev)
+    d = float(np.float32(DAMPING))
+    x = x0.double()
+    delta, it = float("inf"), 0
+    while it < 400 and delta >= 1e-13:
+        xn = d * (A @ x)
+        xn[rows, cols] += (1.0 - d) + d * (dang @ x)
+        delta = float((xn - x).abs().sum(0).max())
+        x, it = xn, it + 1
+    del A
+    return x
+
+
 def errors_vs(x_star, s):
     """Max and L1 error of a float32 score vector against the FP64 fixed point."""
     e = (s.double() - x_star).abs()
@@ -533,6 +564,13 @@ def ppr_leg(G, torch, dev, stream, args):
                                   "vector_sweeps_min": int(it.min()), "loop_ms": st.loop_ms,
                                   "edge_vector_gteps": rate, "vs_plain_fp32": rate / plain,
                                   "max_final_residual": st.residual}
+            # errors of the last solve's vectors against the FP64 fixed point
+            xk = buf.view(m, k)
+            x_star = ppr_fp64_fixed_point(torch, csr, m, seeds, xk)
+            e = (xk.double() - x_star).abs()
+            out[f"k{k}_{tag}"]["max_l1_error_vs_fp64_fixed_point"] = float(e.sum(0).max())
+            out[f"k{k}_{tag}"]["max_error_vs_fp64_fixed_point"] = float(e.max())
+            del x_star, e
         # the same FP32 solve as a CUDA-graph loop (one launch per sweep)
         bst = None
         for _ in range(2):

@@ -152,7 +152,9 @@ int gpr_page_rank(int m, int nnz, const int *row_offsets,
  * h_seeds[q], x_q = d * M x_q + ((1-d) + d * dangling_q) e_{seed_q}, from
  * x_q = e_{seed_q}; vector q stops after the first sweep whose FP64 L1 change
  * is below opts->tol.  opts->precision: GPR_PREC_FP32 or GPR_PREC_BF16
- * (contributions stored in BF16, FP32 accumulation).  any_x receives x as an
+ * (contributions stored in BF16 until the change is below max(tol, 1e-3),
+ * FP32 accumulation, then FP32 sweeps until it is below tol (1-d)/d, so that
+ * the BF16 start costs no accuracy).  any_x receives x as an
  * m x k row-major array (vertex-major, host or device); h_iters (k ints, may
  * be NULL) the sweeps of each vector.  opts->loop: GPR_LOOP_AUTO /
  * GPR_LOOP_PERSISTENT run all sweeps in one cooperative launch (grid barrier

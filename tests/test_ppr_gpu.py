@@ -33,15 +33,22 @@ def test_ppr_fp32_matches_fp64_oracle(G, O, k):
 
 
 def test_ppr_bf16_form(G, O):
+    """BF16 contributions to a change below 1e-3, then FP32 refinement until
+    the change is below tol (1-d)/d: the BF16 start leaves its error in the
+    slowest modes, and that stop bounds what is left of it by tol, so the
+    result is about as close to the FP64 fixed point as the FP32 form's."""
     rp, col, od = O.rmat_graph(12, 8, seed=32)
     m = len(rp) - 1
     seeds = O.uniform_int(32, 78, m)
-    ref, ref_it = O.ppr_f64(rp, col, od, seeds, tol=1e-6, max_iter=100)
+    fixed, _ = O.ppr_f64(rp, col, od, seeds, tol=1e-15, max_iter=3000)
     with G.Graph(rp, col, od, batched=True) as g:
-        x, it, st = g.ppr(seeds, tol=1e-6, max_iter=100, precision=G.PREC_BF16)
+        x, it, st = g.ppr(seeds, tol=1e-6, max_iter=200, precision=G.PREC_BF16)
+        x32, it32, _ = g.ppr(seeds, tol=1e-6, max_iter=200)
     assert st.refine_iterations > 0
-    assert np.all(l1_per_vector(x, ref) <= 1e-5)
-    assert np.all(it <= ref_it + 30)
+    e16, e32 = l1_per_vector(x, fixed), l1_per_vector(x32, fixed)
+    assert np.all(e16 <= 1e-5)
+    assert e16.max() <= 2 * e32.max() + 1.5e-6
+    assert np.all(it <= it32 + 60)
 
 
 def test_ppr_seed_without_in_edges_and_chunked_hub(G, O):
