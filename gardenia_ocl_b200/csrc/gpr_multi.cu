@@ -99,8 +99,8 @@ __device__ __forceinline__ double mrow_update(const MultiArgs &a, float base, in
 // single-graph kernel, so per-graph results match it bit for bit).
 template <int U4, typename T>
 __device__ __forceinline__ double m_chunk(const MultiArgs &a, const GlobalGather<T> &gat, T *cout,
-                                          int u, int4 md, float base, int lane,
-                                          const Policies &pol) {
+                                          int u, int4 md, long long b, long long e, float base,
+                                          int lane, const Policies &pol) {
   const int r = md.x, cb = md.y, nc = md.z;
   float so = 0.f;
   int od = 1;
@@ -108,7 +108,6 @@ __device__ __forceinline__ double m_chunk(const MultiArgs &a, const GlobalGather
     so = ld_f32_stream(a.s + r, pol.stream);
     od = ld_s32_stream(a.outdeg + r, pol.stream);
   }
-  const long long b = a.uoff[u], e = a.uoff[u + 1];
   float acc = 0.f;
   for (long long k0 = b + 4 * lane; k0 < e; k0 += 128 * U4) {
     int4 q[U4];
@@ -149,8 +148,8 @@ __device__ __forceinline__ double m_chunk(const MultiArgs &a, const GlobalGather
 // One SELL-32 slice of 32 >> lw rows, w = 1 << lw lanes per row.
 template <int U, typename T>
 __device__ __forceinline__ double m_slice(const MultiArgs &a, const GlobalGather<T> &gat, T *cout,
-                                          int u, int4 md, float base, int lane,
-                                          const Policies &pol) {
+                                          int u, int4 md, long long b, long long e, float base,
+                                          int lane, const Policies &pol) {
   const int lw = md.w & 15;
   const int r = md.x + (lane >> lw);
   const bool lead = (lane & ((1 << lw) - 1)) == 0;
@@ -161,8 +160,7 @@ __device__ __forceinline__ double m_slice(const MultiArgs &a, const GlobalGather
     so = ld_f32_stream(a.s + r, pol.stream);
     od = ld_s32_stream(a.outdeg + r, pol.stream);
   }
-  const long long b = a.uoff[u];
-  const int len = (int)((a.uoff[u + 1] - b) >> 5);
+  const int len = (int)((e - b) >> 5);
   const int *p = a.ecol + b + lane;
   float acc = 0.f;
   for (int j0 = 0; j0 < len; j0 += U) {
@@ -315,8 +313,21 @@ __device__ __forceinline__ void multi_sweep(const MultiArgs &a, int it, int lane
     int cur = -1, done = 0;
     bool act = false;
     float base = 0.f;
+    int4 md_n = make_int4(0, 0, 0, 0);
+    long long b_n = 0, e_n = 0;
+    if (u0 < u1) {
+      md_n = __ldg(a.meta + u0);
+      b_n = __ldg(a.uoff + u0);
+      e_n = __ldg(a.uoff + u0 + 1);
+    }
     for (int u = u0; u < u1; ++u) {
-      const int4 md = __ldg(a.meta + u);
+      const int4 md = md_n;
+      const long long ub = b_n, ue = e_n;
+      if (u + 1 < u1) {  // the next unit's descriptor and end offset are in flight meanwhile
+        md_n = __ldg(a.meta + u + 1);
+        b_n = ue;
+        e_n = __ldg(a.uoff + u + 2);
+      }
       const int g = md.w >> 8;
       if (g != cur) {
         if (done) finish_units(a, cur, done, it, lane);
@@ -328,8 +339,8 @@ __device__ __forceinline__ void multi_sweep(const MultiArgs &a, int it, int lane
       if (!act) continue;
       const int kind = (md.w >> 4) & 15;
       double err;
-      if (kind == kUnitChunk) err = m_chunk<U4>(a, gat, cout, u, md, base, lane, pol);
-      else if (kind == kUnitSlice) err = m_slice<U>(a, gat, cout, u, md, base, lane, pol);
+      if (kind == kUnitChunk) err = m_chunk<U4>(a, gat, cout, u, md, ub, ue, base, lane, pol);
+      else if (kind == kUnitSlice) err = m_slice<U>(a, gat, cout, u, md, ub, ue, base, lane, pol);
       else err = m_zero(a, cout, md, base, lane, it, pol);
       err = warp_sum(err);
       if (lane == 0) a.uerr[u] = err;
