@@ -16,6 +16,10 @@
  * CUDA device; "any" pointers may be either (the library checks with
  * cudaPointerGetAttributes and copies when needed).  Streams are passed as
  * void* (a cudaStream_t; NULL = the legacy default stream).
+ *
+ * A handle (graph, matrix, multi-graph batch, SymGS) is used by one host
+ * thread at a time: it caches per-handle tables and CUDA graphs.  Different
+ * handles may be used from different threads.
  */
 #ifndef GPR_H_
 #define GPR_H_
@@ -40,7 +44,9 @@ typedef enum {
 typedef enum {
   GPR_PREC_FP32 = 0,  /* plain form: FP32 everywhere, FP64 residual */
   GPR_PREC_BF16 = 1,  /* BF16 contributions, FP32 accumulation, FP32 refinement */
-  GPR_PREC_FP16 = 2   /* FP16 contributions with per-iteration power-of-two scaling */
+  GPR_PREC_FP16 = 2   /* reserved: every solver returns GPR_EUNSUPPORTED (the gather is
+                         bound by its request count, not its bytes, so a 2-byte form
+                         gains nothing; BF16 covers the mixed form) */
 } gpr_precision;
 
 /* How the iteration loop is driven. */

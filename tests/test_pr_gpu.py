@@ -224,3 +224,23 @@ def test_graph_loop_caps_and_reuse(G, O):
                 assert sb.iterations == mi
             ref, ref_it, _ = O.pr_plain_f32(rp, col, od, tol=tol, max_iter=mi)
             assert abs(sb.iterations - ref_it) <= 1
+
+
+def test_fp16_form_is_reported_unsupported(G, O):
+    """GPR_PREC_FP16 is reserved: each PageRank solver refuses it with
+    GPR_EUNSUPPORTED (and the handle stays usable)."""
+    rp, col, od = O.rmat_graph(8, 4, seed=1)
+    with G.Graph(rp, col, od, batched=True) as g:
+        with pytest.raises(G.GprError) as e:
+            g.pagerank(precision=G.PREC_FP16)
+        assert e.value.status == G.GPR_EUNSUPPORTED
+        with pytest.raises(G.GprError) as e:
+            g.ppr(np.array([0, 1], np.int32), precision=G.PREC_FP16)
+        assert e.value.status == G.GPR_EUNSUPPORTED
+        s, st = g.pagerank(tol=1e-4)
+        assert st.iterations > 0
+    voff = np.array([0, len(rp) - 1], np.int32)
+    with G.MultiGraph(rp, col, od, voff) as mg:
+        with pytest.raises(G.GprError) as e:
+            mg.pagerank(precision=G.PREC_FP16)
+        assert e.value.status == G.GPR_EUNSUPPORTED
