@@ -398,24 +398,29 @@ def run_ours(args):
     return 0
 
 
-def fp64_fixed_point(torch, csr, m, x0):
-    """FP64 fixed point of the plain recurrence x = (1 - d) / m + d A x
-    (A[v, u] = 1 / outdeg[u] over the in-CSR, d = (double)0.85f, as the
-    reference's FP64 restatement), computed with PyTorch's FP64 sparse
-    matrix-vector product on the GPU from x0 until the L1 change is below
-    1e-13.  A checker for the accuracy report: the solvers are not involved.
-    Returns (x, iterations, last L1 change)."""
+def pull_matrix(torch, csr, m, dev):
+    """The in-CSR as a PyTorch FP64 sparse matrix, A[v, u] = 1 / outdeg[u]."""
     import warnings
     warnings.filterwarnings("ignore", message="Sparse")  # beta-status notices of torch.sparse
-    dev = x0.device
     rp = torch.from_numpy(csr.rowptr.to_numpy().astype(np.int64)).to(dev)
     col = torch.from_numpy(csr.col.to_numpy().astype(np.int64)).to(dev)
     od = torch.from_numpy(csr.third.to_numpy()).to(dev).double()
-    inv = torch.where(od > 0, 1.0 / od.clamp(min=1.0), torch.zeros_like(od))
-    A = torch.sparse_csr_tensor(rp, col, inv[col], size=(m, m))
-    del rp, col, od, inv
+    return torch.sparse_csr_tensor(rp, col, (1.0 / od.clamp(min=1.0))[col], size=(m, m))
+
+
+def fp64_fixed_point(torch, csr, m, x0, base=None, A=None):
+    """FP64 fixed point of the plain recurrence x = base + d A x (A[v, u] =
+    1 / outdeg[u] over the in-CSR, d = (double)0.85f, base (1 - d) / m, or
+    per vertex (1 - d) / m_g for a batch of graphs, as the reference's FP64
+    restatement), computed with PyTorch's FP64 sparse matrix-vector product
+    on the GPU from x0 until the L1 change is below 1e-13.  A checker for the
+    accuracy report: the solvers are not involved.  Returns (x, iterations,
+    last L1 change)."""
+    if A is None:
+        A = pull_matrix(torch, csr, m, x0.device)
     d = float(np.float32(DAMPING))
-    base = (1.0 - d) / m
+    if base is None:
+        base = (1.0 - d) / m
     x = x0.double()
     delta, k = float("inf"), 0
     while k < 400 and delta >= 1e-13:
@@ -433,15 +438,9 @@ def ppr_fp64_fixed_point(torch, csr, m, seeds, x0):
     A[v, u] = 1 / outdeg[u] over the in-CSR, d = (double)0.85f, computed with
     PyTorch's FP64 sparse x dense product on the GPU from x0 (m x k) until
     every vector's L1 change is below 1e-13.  A checker only."""
-    import warnings
-    warnings.filterwarnings("ignore", message="Sparse")
     dev = x0.device
-    rp = torch.from_numpy(csr.rowptr.to_numpy().astype(np.int64)).to(dev)
-    col = torch.from_numpy(csr.col.to_numpy().astype(np.int64)).to(dev)
-    od = torch.from_numpy(csr.third.to_numpy()).to(dev).double()
-    A = torch.sparse_csr_tensor(rp, col, (1.0 / od.clamp(min=1.0))[col], size=(m, m))
-    dang = (od == 0).double()
-    del rp, col, od
+    A = pull_matrix(torch, csr, m, dev)
+    dang = torch.from_numpy((csr.third.to_numpy() == 0).astype(np.float64)).to(dev)
     k = x0.shape[1]
     rows = torch.from_numpy(np.asarray(seeds, np.int64)).to(dev)
     cols = torch.arange(k, device=dev)
@@ -621,6 +620,7 @@ def multigraph_leg(G, torch, dev, stream, plain_gteps, args):
            "tuning": tuned,
            "bins": sorted({(d["sell_max"], d["chunk_min"], d["chunk"]) for d in layouts})
            if layouts else "defaults"}
+    x_star = None
     for prec, name in ((G.PREC_FP32, "fp32"), (G.PREC_BF16, "bf16_refined")):
         best = None
         for _ in range(3):
@@ -640,6 +640,16 @@ def multigraph_leg(G, torch, dev, stream, plain_gteps, args):
                      "achieved_gbs": byts / (st.loop_ms / 1e3) / 1e9,
                      "frac": byts / (st.loop_ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind,
                      "gpu_launches": st.gpu_launches}
+        # every graph's errors against the batch's FP64 fixed point (each
+        # graph with its own teleport (1 - d) / m_g); all graphs have m_g > 0
+        if x_star is None:
+            base = np.repeat((1.0 - float(np.float32(DAMPING))) / m_g, m_g)
+            x_star, _, _ = fp64_fixed_point(torch, A, A.m, scores,
+                                            base=torch.from_numpy(base).to(dev))
+        e = (scores.double() - x_star).abs().cpu().numpy()
+        out[name]["max_l1_error_vs_fp64_fixed_point"] = float(np.add.reduceat(e, voff[:-1]).max())
+        out[name]["max_error_vs_fp64_fixed_point"] = float(e.max())
+    del x_star
     # the FP32 solve again as a CUDA-graph loop (one launch per sweep)
     best = None
     for _ in range(2):

@@ -46,3 +46,21 @@ def test_ppr_fixed_point_matches_oracle(O):
     x = bench.ppr_fp64_fixed_point(torch, _CSR(rp, col, od), m, seeds,
                                    torch.from_numpy(start.astype(np.float32)))
     np.testing.assert_allclose(x.numpy(), ref, rtol=0, atol=1e-12)
+
+
+def test_batch_fixed_point_matches_per_graph_oracle(O):
+    """A block-diagonal batch with each graph's own teleport (1 - d) / m_g:
+    the batch's fixed point is every graph's own fixed point."""
+    rp, col, od, voff = O.multigraph(4, 100, 2000, seed=2)
+    M = len(rp) - 1
+    m_g = np.diff(voff).astype(np.int64)
+    base = np.repeat((1.0 - float(np.float32(0.85))) / m_g, m_g)
+    start = np.repeat(1.0 / m_g, m_g).astype(np.float32)
+    x, it, delta = bench.fp64_fixed_point(torch, _CSR(rp, col, od), M, torch.from_numpy(start),
+                                          base=torch.from_numpy(base))
+    assert delta < 1e-13
+    for g in range(len(voff) - 1):
+        a, b = voff[g], voff[g + 1]
+        e0, e1 = rp[a], rp[b]
+        ref, _, _ = O.pr_f64(rp[a:b + 1] - e0, col[e0:e1] - a, od[a:b], tol=1e-15, max_iter=3000)
+        np.testing.assert_allclose(x.numpy()[a:b], ref, rtol=0, atol=1e-12)
