@@ -65,3 +65,12 @@ def test_reference_arm_under_torchrun_two_ranks():
     line = lines[0]
     assert line["impl"] == "reference" and line["n_gpus"] == 2 and line["value"] > 0
     assert line["cpu_baseline"]["kind"] in ("reference", "port")
+    # the keys the reference arm's line carries besides the value
+    assert line["metric"] == "pagerank_gteps_rmat24" and line["unit"] == "GTEPS"
+    assert line["higher_is_better"] is True and line["steps"] == 1 and line["warmup"] == 3
+    cb = line["cpu_baseline"]
+    assert cb["value"] == line["value"] and cb["cores"] >= 1 and cb["sample"]
+    e2e = line["e2e"]
+    assert e2e["value"] == line["value"] and e2e["unit"] == "GTEPS"
+    assert e2e["h2d_bytes_per_step"] == 0 and e2e["d2h_bytes_per_step"] == 0
+    assert line["config"]["workload"].startswith("pagerank_rmat10")
