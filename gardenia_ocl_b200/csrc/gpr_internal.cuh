@@ -241,4 +241,11 @@ constexpr int kHotMax = 56832;         // 222 KB: the most one CTA may take
 __host__ __device__ inline long long ceil_div(long long a, long long b) {
   return (a + b - 1) / b;
 }
+
+// Sweeps the reference's loop counts on a graph with no vertices
+// (src/pr/omp_base.cc:23-43): every sweep's residual is 0, so the loop stops
+// after the first sweep when 0 < tol and runs to max_iter otherwise.
+inline int empty_graph_sweeps(double tol, int max_iter) {
+  return max_iter <= 0 ? 0 : (0.0 < tol ? 1 : max_iter);
+}
 }  // namespace gpr

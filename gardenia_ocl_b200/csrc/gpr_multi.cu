@@ -1067,9 +1067,11 @@ int multi_pagerank_impl(gpr_multigraph *g, float *any_scores, const gpr_pr_opts 
   gpr_pr_stats sl;
   memset(&sl, 0, sizeof(sl));
   const int G = g->G, M = g->M;
+  // a graph with no vertices runs empty sweeps with residual 0
+  const int empty_sweeps = gpr::empty_graph_sweeps(o.tol, o.max_iter);
   if (M == 0) {
     if (stats) *stats = sl;
-    if (h_iters) memset(h_iters, 0, sizeof(int) * G);
+    if (h_iters) for (int ug = 0; ug < G; ++ug) h_iters[ug] = empty_sweeps;
     if (h_res) memset(h_res, 0, sizeof(double) * G);
     return GPR_OK;
   }
@@ -1122,7 +1124,7 @@ int multi_pagerank_impl(gpr_multigraph *g, float *any_scores, const gpr_pr_opts 
   if (rc == GPR_OK) {
     for (int ug = 0; ug < G; ++ug) {
       const int r = g->rank[ug];
-      if (h_iters) h_iters[ug] = it1[r];
+      if (h_iters) h_iters[ug] = g->ivoff[r + 1] > g->ivoff[r] ? it1[r] : empty_sweeps;
       if (h_res) h_res[ug] = r1[r];
     }
   }

@@ -195,6 +195,8 @@ int gpr_pagerank_noalloc(int m, int nnz, const int *d_rowptr, const int *d_col,
   gpr_pr_stats st;
   memset(&st, 0, sizeof(st));
   if (m == 0 || o.max_iter == 0) {
+    // no vertices: the sweeps are empty and their residuals 0
+    if (m == 0) st.iterations = gpr::empty_graph_sweeps(o.tol, o.max_iter);
     if (stats) *stats = st;
     return GPR_OK;
   }

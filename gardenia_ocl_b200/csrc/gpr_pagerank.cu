@@ -854,11 +854,15 @@ int pagerank_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts_in,
   gpr_pr_stats st_local;
   memset(&st_local, 0, sizeof(st_local));
   if (m == 0 || any_scores == nullptr) {
-    if (stats) *stats = st_local;
     if (m != 0) {
+      if (stats) *stats = st_local;
       gpr::set_error("gpr_pagerank: NULL scores");
       return GPR_EINVAL;
     }
+    // no vertices: the sweeps are empty and their residuals 0
+    st_local.iterations = gpr::empty_graph_sweeps(o.tol, o.max_iter);
+    g->last_sweeps = st_local.iterations;
+    if (stats) *stats = st_local;
     return GPR_OK;
   }
   cudaStream_t st = g->st;
@@ -1004,8 +1008,11 @@ int gpr_graph_residuals(const gpr_graph *g, double *h_out, int n) {
     return GPR_EINVAL;
   }
   const int k = n < g->last_sweeps ? n : g->last_sweeps;
-  if (k > 0)
+  if (k > 0 && g->L.m == 0) {
+    for (int i = 0; i < k; ++i) h_out[i] = 0.0;  // empty sweeps (nothing on the device)
+  } else if (k > 0) {
     GPR_CUDA(cudaMemcpy(h_out, g->err_hist, sizeof(double) * (size_t)k, cudaMemcpyDeviceToHost));
+  }
   return GPR_OK;
 }
 

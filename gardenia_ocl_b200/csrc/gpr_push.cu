@@ -195,7 +195,11 @@ int push_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts &o, gpr_pr_stat
   const gpr::PrLayout &L = g->L;
   const int m = L.m;
   memset(out, 0, sizeof(*out));
-  if (m == 0) return GPR_OK;
+  if (m == 0) {  // no vertices: the sweeps are empty and their residuals 0
+    out->iterations = gpr::empty_graph_sweeps(o.tol, o.max_iter);
+    g->last_sweeps = out->iterations;
+    return GPR_OK;
+  }
   if (!g->push_src) GPR_TRY(build_push_edges(g));
   cudaStream_t st = g->st;
   float *d_scores = any_scores;

@@ -71,7 +71,9 @@ typedef struct {
 } gpr_pr_opts;
 
 typedef struct {
-  int iterations;       /* sweeps executed (the reference prints the same number, gather.cu:83) */
+  int iterations;       /* sweeps executed (the reference prints the same number, gather.cu:83);
+                           m = 0: the empty sweeps the reference's loop counts, 1 when
+                           tol > 0 and max_iter when tol = 0 (omp_base.cc:23-43) */
   int refine_iterations;/* FP32 sweeps spent in the refinement tail (mixed precision) */
   double residual;      /* L1 change of the last sweep (FP64) */
   double solve_ms;      /* device time of the solve (CUDA events), excluding copies */
@@ -201,7 +203,8 @@ int gpr_pagerank_push(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts,
  * results).  any_scores: all vertices, initialised by the caller
  * (the reference uses 1/m_g, src/pr/main.cc:27-28), updated in place.
  * h_iters / h_residuals (n_graphs entries each, may be NULL) receive each
- * graph's sweeps and last residual.  precision GPR_PREC_FP32, or
+ * graph's sweeps and last residual (a graph with no vertices: the empty
+ * sweeps the reference's loop counts, residual 0).  precision GPR_PREC_FP32, or
  * GPR_PREC_BF16 (BF16 contributions to max(tol, 1e-3), then FP32 sweeps to
  * tol); stats->iterations is the launch's sweep count (the largest graph
  * count per phase). */

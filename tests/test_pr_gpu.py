@@ -116,6 +116,27 @@ def test_device_scores_in_place(G, O):
     assert np.abs(d.cpu().numpy() - ref).max() <= ABS_TOL
 
 
+@pytest.mark.filterwarnings("ignore:divide by zero")
+@pytest.mark.parametrize("tol,max_iter", [(1e-3, 30), (0.0, 7), (1e-3, 0)])
+def test_empty_graph_sweep_count(G, O, tol, max_iter):
+    """m = 0: the reference's loop still counts its empty sweeps (residual 0:
+    one when tol > 0, max_iter when tol = 0), for pull, push and the
+    no-allocation entry alike."""
+    rp, col, od = np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32)
+    _, ref_it, ref_hist = O.pr_plain_f32(rp, col, od, tol=tol, max_iter=max_iter)
+    with G.Graph(rp, col, od, push=True) as g:
+        s, st = g.pagerank(tol=tol, max_iter=max_iter)
+        assert s.size == 0 and st.iterations == ref_it and st.residual == 0.0
+        assert np.array_equal(g.residuals(), ref_hist)
+        _, st = g.pagerank_push(tol=tol, max_iter=max_iter)
+        assert st.iterations == ref_it
+    import torch
+    d = [torch.zeros(n, dtype=t, device="cuda") for n, t in ((1, torch.int32), (0, torch.int32),
+                                                             (0, torch.int32), (0, torch.float32))]
+    st = G.pagerank_noalloc(0, 0, *d, tol=tol, max_iter=max_iter)
+    assert st.iterations == ref_it
+
+
 def test_edge_cases(G, O):
     # one vertex, no edges
     s, st, _, _ = solve(G, np.array([0, 0], np.int32), np.array([], np.int32),
