@@ -171,8 +171,9 @@ int csr_from_keys(long long ne, int m, uint64_t *k0, uint64_t *k1, int **d_rowpt
     if ((rc = gpr::dalloc(&rowptr, (size_t)m + 1, "rowptr")) != GPR_OK) break;
     if ((rc = gpr::dalloc(&col, (size_t)nnz, "col")) != GPR_OK) break;
     if ((rc = gpr::dalloc(&outdeg, (size_t)m, "outdeg")) != GPR_OK) break;
-    cudaMemsetAsync(rowptr, 0, sizeof(int) * ((size_t)m + 1), st);
-    cudaMemsetAsync(outdeg, 0, sizeof(int) * (size_t)m, st);
+    if ((rc = GPR_CUDA_RC(cudaMemsetAsync(rowptr, 0, sizeof(int) * ((size_t)m + 1), st))) != GPR_OK)
+      break;
+    if ((rc = GPR_CUDA_RC(cudaMemsetAsync(outdeg, 0, sizeof(int) * (size_t)m, st))) != GPR_OK) break;
     k_split_keys<<<capped_grid(nnz), 256, 0, st>>>(nnz, uniq, col, rowptr, outdeg);
     gpr::dfree(tmp);
     tmp = nullptr;
@@ -285,6 +286,9 @@ int gpr_gen_rmat(int scale, int edge_factor, double a, double b, double c,
   if (rc == GPR_OK) {
     k_rmat_keys<<<capped_grid(ne), 256>>>(ne, scale, t0, t1, t2, seed, do_scramble,
                                            make_scramble(scale, seed), k0);
+    rc = GPR_CUDA_RC(cudaGetLastError());
+  }
+  if (rc == GPR_OK) {
     rc = csr_from_keys(ne, m, k0, k1, d_rowptr, d_col, d_outdeg, nnz_out);
   }
   gpr::dfree(k0);
@@ -344,12 +348,21 @@ int gpr_gen_multigraph(int n_graphs, int m_min, int m_max, int er_deg, int cl_de
   if (rc == GPR_OK) rc = gpr::dalloc(&deoff, (size_t)n_graphs + 1, "draw offsets");
   if (rc == GPR_OK) rc = gpr::dalloc(&dgs, (size_t)n_graphs, "graph seeds");
   if (rc == GPR_OK) rc = gpr::dalloc(&dP, (size_t)m_big, "Chung-Lu prefix");
+  if (rc == GPR_OK)
+    rc = GPR_CUDA_RC(cudaMemcpy(dvoff, voff.data(), sizeof(int) * voff.size(), cudaMemcpyHostToDevice));
+  if (rc == GPR_OK)
+    rc = GPR_CUDA_RC(
+        cudaMemcpy(deoff, eoff.data(), sizeof(long long) * eoff.size(), cudaMemcpyHostToDevice));
+  if (rc == GPR_OK)
+    rc = GPR_CUDA_RC(
+        cudaMemcpy(dgs, gs.data(), sizeof(unsigned long long) * gs.size(), cudaMemcpyHostToDevice));
+  if (rc == GPR_OK)
+    rc = GPR_CUDA_RC(cudaMemcpy(dP, P.data(), sizeof(double) * P.size(), cudaMemcpyHostToDevice));
   if (rc == GPR_OK) {
-    cudaMemcpy(dvoff, voff.data(), sizeof(int) * voff.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(deoff, eoff.data(), sizeof(long long) * eoff.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(dgs, gs.data(), sizeof(unsigned long long) * gs.size(), cudaMemcpyHostToDevice);
-    cudaMemcpy(dP, P.data(), sizeof(double) * P.size(), cudaMemcpyHostToDevice);
     k_multi_keys<<<capped_grid(ne), 256>>>(ne, n_graphs, deoff, dvoff, dgs, dP, k0);
+    rc = GPR_CUDA_RC(cudaGetLastError());
+  }
+  if (rc == GPR_OK) {
     rc = csr_from_keys(ne, voff[n_graphs], k0, k1, d_rowptr, d_col, d_outdeg, nnz_out);
   }
   gpr::dfree(k0);

@@ -101,9 +101,14 @@ int check_range(int m, long long n, const int *d_row, const int *d_col, cudaStre
   int *flag = nullptr;
   GPR_TRY(gpr::dalloc(&flag, 1, "range flag"));
   int h = 0;
-  cudaMemsetAsync(flag, 0, sizeof(int), st);
-  k_check_range<<<grid_for(n), 256, 0, st>>>(n, m, d_row, d_col, flag);
-  cudaError_t e = cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), st);
+  if (e == cudaSuccess) {
+    k_check_range<<<grid_for(n), 256, 0, st>>>(n, m, d_row, d_col, flag);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    e = cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   gpr::dfree(flag);
   if (e != cudaSuccess) {
@@ -195,8 +200,8 @@ int build_csr(int m, long long n, const int *d_row, const int *d_col, const floa
   int rc = gpr::dalloc(&rowptr, (size_t)m + 1, "rowptr");
   if (rc == GPR_OK) rc = gpr::dalloc(&col, (size_t)cur, "col");
   if (rc == GPR_OK && out_wt) rc = gpr::dalloc(&wt, (size_t)cur, "weight");
+  if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemsetAsync(rowptr, 0, sizeof(int) * ((size_t)m + 1), st));
   if (rc == GPR_OK) {
-    cudaMemsetAsync(rowptr, 0, sizeof(int) * ((size_t)m + 1), st);
     if (cur > 0)
       k_emit<<<grid_for(cur), 256, 0, st>>>(cur, idx, d_row, d_col, d_wt, rowptr + 1, col, wt);
     size_t tb = 0;
@@ -248,6 +253,36 @@ int parse(const char *path, bool symmetrize, HostPushes *H) {
   return GPR_OK;
 }
 
+// Row lengths of a device CSR into a new device array: the out-degree the
+// reference's read fills (include/graph_io.h:289-294).
+int row_lengths(int m, const int *d_rowptr, int **out) {
+  int *deg = nullptr;
+  GPR_TRY(gpr::dalloc(&deg, (size_t)m, "degree"));
+  int rc = GPR_OK;
+  if (m > 0) {
+    k_row_lengths<<<(m + 255) / 256, 256>>>(m, d_rowptr, deg);
+    rc = GPR_CUDA_RC(cudaGetLastError());
+  }
+  if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaDeviceSynchronize());
+  if (rc != GPR_OK) {
+    gpr::dfree(deg);
+    return rc;
+  }
+  *out = deg;
+  return GPR_OK;
+}
+
+// Releases a device CSR handed out by gpr_csr_from_edges (NULL-safe).
+void free_csr(int **rowptr, int **col, float **wt) {
+  gpr::dfree(*rowptr);
+  gpr::dfree(*col);
+  *rowptr = *col = nullptr;
+  if (wt) {
+    gpr::dfree(*wt);
+    *wt = nullptr;
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -295,11 +330,11 @@ int gpr_read_graph_gpu(const char *path, int symmetrize, int transpose, int sort
   }
   GPR_TRY(gpr_csr_from_edges(H.m, H.n, H.row, H.col, H.wt, sorted, remove_selfloops,
                              remove_redundents, d_rowptr, d_col, d_wt, nnz_out));
-  int *deg = nullptr;
-  GPR_TRY(gpr::dalloc(&deg, (size_t)H.m, "degree"));
-  if (H.m > 0) k_row_lengths<<<(H.m + 255) / 256, 256>>>(H.m, *d_rowptr, deg);
-  GPR_CUDA(cudaDeviceSynchronize());
-  *d_degree = deg;
+  const int rc = row_lengths(H.m, *d_rowptr, d_degree);
+  if (rc != GPR_OK) {
+    free_csr(d_rowptr, d_col, d_wt);
+    return rc;
+  }
   *m_out = H.m;
   return GPR_OK;
 }
@@ -320,13 +355,15 @@ int gpr_read_graph_pr(const char *path, int symmetrize, int *m_out, long long *n
   // Transposed read: the same pushes with row and column swapped (with
   // symmetrize the reference ignores the transpose flag: the same lists).
   const int *in_row = symmetrize ? H.row : H.col, *in_col = symmetrize ? H.col : H.row;
-  GPR_TRY(gpr_csr_from_edges(H.m, H.n, in_row, in_col, nullptr, 0, 1, 1, d_in_rowptr, d_in_col,
-                             nullptr, nnz_in_csr));
-  int *deg = nullptr;
-  GPR_TRY(gpr::dalloc(&deg, (size_t)H.m, "out-degree"));
-  if (H.m > 0) k_row_lengths<<<(H.m + 255) / 256, 256>>>(H.m, *d_out_rowptr, deg);
-  GPR_CUDA(cudaDeviceSynchronize());
-  *d_out_degree = deg;
+  *d_in_rowptr = *d_in_col = nullptr;
+  int rc = gpr_csr_from_edges(H.m, H.n, in_row, in_col, nullptr, 0, 1, 1, d_in_rowptr, d_in_col,
+                              nullptr, nnz_in_csr);
+  if (rc == GPR_OK) rc = row_lengths(H.m, *d_out_rowptr, d_out_degree);
+  if (rc != GPR_OK) {
+    free_csr(d_out_rowptr, d_out_col, nullptr);
+    free_csr(d_in_rowptr, d_in_col, nullptr);
+    return rc;
+  }
   *m_out = H.m;
   return GPR_OK;
 }

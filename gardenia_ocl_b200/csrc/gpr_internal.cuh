@@ -171,6 +171,17 @@ void free_spmv_layout(SpmvLayout *L);
     }                                                                         \
   } while (0)
 
+namespace gpr {
+// Status of one CUDA call, for code that must release buffers before it
+// returns (GPR_CUDA returns at once): GPR_OK, or GPR_ECUDA with the error set.
+inline int cuda_status(cudaError_t e, const char *file, int line, const char *what) {
+  if (e == cudaSuccess) return GPR_OK;
+  set_error("%s:%d: %s: %s", file, line, what, cudaGetErrorString(e));
+  return GPR_ECUDA;
+}
+}  // namespace gpr
+#define GPR_CUDA_RC(call) gpr::cuda_status((call), __FILE__, __LINE__, #call)
+
 #define GPR_TRY(call)                                                         \
   do {                                                                        \
     int s_ = (call);                                                          \

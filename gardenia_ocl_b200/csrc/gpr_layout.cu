@@ -201,15 +201,20 @@ int validate_csr(int m, long long nnz, int ncols, const int *d_rowptr, const int
   }
   int *flag = nullptr;
   GPR_TRY(dalloc(&flag, 1, "validation flag"));
-  cudaMemsetAsync(flag, 0, sizeof(int), st);
-  k_validate_rows<<<grid_for((long long)m + 1), 256, 0, st>>>(m, nnz, d_rowptr, d_outdeg, flag);
-  if (nnz > 0 && d_col) {
-    long long g = grid_for(nnz);
-    if (g > 148 * 64) g = 148 * 64;
-    k_validate_cols<<<(unsigned)g, 256, 0, st>>>(nnz, ncols, d_col, flag);
-  }
   int h = 0;
-  cudaError_t e = cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), st);
+  if (e == cudaSuccess) {
+    k_validate_rows<<<grid_for((long long)m + 1), 256, 0, st>>>(m, nnz, d_rowptr, d_outdeg, flag);
+    if (nnz > 0 && d_col) {
+      long long g = grid_for(nnz);
+      if (g > 148 * 64) g = 148 * 64;
+      k_validate_cols<<<(unsigned)g, 256, 0, st>>>(nnz, ncols, d_col, flag);
+    }
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    e = cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   gpr::dfree(flag);
   if (e != cudaSuccess) {
@@ -228,12 +233,17 @@ int validate_cols(long long nnz, int ncols, const int *d_col, cudaStream_t st) {
   if (nnz <= 0) return GPR_OK;
   int *flag = nullptr;
   GPR_TRY(dalloc(&flag, 1, "validation flag"));
-  cudaMemsetAsync(flag, 0, sizeof(int), st);
-  long long g = grid_for(nnz);
-  if (g > 148 * 64) g = 148 * 64;
-  k_validate_cols<<<(unsigned)g, 256, 0, st>>>(nnz, ncols, d_col, flag);
   int h = 0;
-  cudaError_t e = cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaMemsetAsync(flag, 0, sizeof(int), st);
+  if (e == cudaSuccess) {
+    long long g = grid_for(nnz);
+    if (g > 148 * 64) g = 148 * 64;
+    k_validate_cols<<<(unsigned)g, 256, 0, st>>>(nnz, ncols, d_col, flag);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    e = cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   gpr::dfree(flag);
   if (e != cudaSuccess) {

@@ -656,9 +656,12 @@ int build_multi(gpr_multigraph *g, const int *h_voff, const int *d_rowptr, const
   GPR_TRY(T.get(&flag, 1, "validation flag"));
   GPR_CUDA(cudaMemcpyAsync(dvoff, h_voff, sizeof(int) * ((size_t)G + 1), cudaMemcpyHostToDevice, st));
   k_gather_eoff<<<grid_for((long long)G + 1), 256, 0, st>>>(G, dvoff, d_rowptr, deoff);
+  GPR_CUDA(cudaGetLastError());
   GPR_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));
-  if (g->nnz > 0)
+  if (g->nnz > 0) {
     k_check_blocks<<<capped(g->nnz), 256, 0, st>>>(g->nnz, G, deoff, dvoff, d_col, flag);
+    GPR_CUDA(cudaGetLastError());
+  }
   std::vector<int> eoff(G + 1);
   int hflag = 0;
   GPR_CUDA(cudaMemcpyAsync(eoff.data(), deoff, sizeof(int) * eoff.size(), cudaMemcpyDeviceToHost, st));
@@ -695,6 +698,7 @@ int build_multi(gpr_multigraph *g, const int *h_voff, const int *d_rowptr, const
   GPR_TRY(gpr::dalloc(&g->outdeg, (size_t)M, "out-degree"));
   GPR_CUDA(cudaMemcpyAsync(drank, g->rank.data(), sizeof(int) * G, cudaMemcpyHostToDevice, st));
   k_vertex_keys<<<grid_for(M), 256, 0, st>>>(M, G, dvoff, drank, d_rowptr, key, iota);
+  GPR_CUDA(cudaGetLastError());
   {
     int gbits = 1;
     while ((1LL << gbits) < G) ++gbits;
@@ -713,6 +717,7 @@ int build_multi(gpr_multigraph *g, const int *h_voff, const int *d_rowptr, const
   }
   k_multi_relabel<<<grid_for(M), 256, 0, st>>>(M, g->perm, d_outdeg, d_rowptr, g->outdeg, sdeg,
                                                inv);
+  GPR_CUDA(cudaGetLastError());
   // Per-graph bins (thresholds as in the single-graph layout).
   std::vector<int> lane_max(G), chunk_min(G), chunk(G), th(8 * (size_t)G, 0);
   const int nth = 7;
@@ -735,6 +740,7 @@ int build_multi(gpr_multigraph *g, const int *h_voff, const int *d_rowptr, const
   GPR_CUDA(cudaMemcpyAsync(divoff, g->ivoff.data(), sizeof(int) * ((size_t)G + 1),
                            cudaMemcpyHostToDevice, st));
   k_multi_bounds<<<grid_for((long long)G * nth), 256, 0, st>>>(G, divoff, sdeg, dth, nth, dbounds);
+  GPR_CUDA(cudaGetLastError());
   std::vector<int> bounds(8 * (size_t)G);
   GPR_CUDA(cudaMemcpyAsync(bounds.data(), dbounds, sizeof(int) * bounds.size(),
                            cudaMemcpyDeviceToHost, st));
@@ -793,6 +799,7 @@ int build_multi(gpr_multigraph *g, const int *h_voff, const int *d_rowptr, const
   GPR_CUDA(cudaMemcpyAsync(g->meta, meta.data(), sizeof(int4) * (size_t)U, cudaMemcpyHostToDevice, st));
   GPR_CUDA(cudaMemcpyAsync(dchunk, chunk.data(), sizeof(int) * (size_t)G, cudaMemcpyHostToDevice, st));
   k_unit_lens<<<grid_for((long long)U + 1), 256, 0, st>>>(U, g->meta, sdeg, dchunk, g->uoff);
+  GPR_CUDA(cudaGetLastError());
   {
     size_t tb = 0;
     GPR_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb, g->uoff, g->uoff, U + 1, st));
@@ -844,9 +851,11 @@ int build_multi(gpr_multigraph *g, const int *h_voff, const int *d_rowptr, const
     GPR_CUDA(cudaMemcpyAsync(g->pk, pk.data(), sizeof(int) * pk.size(), cudaMemcpyHostToDevice, st));
     GPR_CUDA(cudaStreamSynchronize(st));
   }
-  if (U > 0)
+  if (U > 0) {
     k_fill_units<<<capped(32LL * U), 256, 0, st>>>(U, M, g->meta, g->uoff, dchunk, g->perm, inv,
                                                    sdeg, d_rowptr, d_col, g->ecol);
+    GPR_CUDA(cudaGetLastError());
+  }
   // Per-graph state.
   GPR_TRY(gpr::dalloc(&g->gm, (size_t)G, "graph sizes"));
   GPR_TRY(gpr::dalloc(&g->hb, (size_t)G + 1, "heavy ranges"));
@@ -1198,7 +1207,11 @@ int gpr_multigraph_create(int n_graphs, const int *h_voff, long long nnz, const 
       rc = gpr::validate_csr(M, nnz, M, (const int *)rp, (const int *)cp, (const int *)dp, g->st);
     if (rc == GPR_OK && M > 0)
       rc = build_multi(g, h_voff, (const int *)rp, (const int *)cp, (const int *)dp, h_lopts);
-    cudaStreamSynchronize(g->st);
+    const cudaError_t se = cudaStreamSynchronize(g->st);
+    if (rc == GPR_OK && se != cudaSuccess) {
+      gpr::set_error("gpr_multigraph_create: %s", cudaGetErrorString(se));
+      rc = GPR_ECUDA;
+    }
   } while (0);
   if (orp) gpr::dfree(rp);
   if (ocp) gpr::dfree(cp);

@@ -1053,13 +1053,16 @@ int gpr_pr_residual_f64(gpr_graph *g, const float *any_scores, float damping, do
   o.damping = damping;
   PrArgs a = make_args(g, o, 0);
   const double d = (double)damping, base = (1.0 - d) / (double)m;
-  cudaMemsetAsync(acc, 0, sizeof(double) * ((size_t)L.n_long + 1), st);
-  k_res_prologue<<<grid_for((long long)m + 1), 256, 0, st>>>(m, L.perm, L.outdeg,
-                                                             (const float *)dv, cd, sd);
-  const long long units = (long long)L.n_chunks + L.n_slices + L.n_zblk;
-  k_res_sweep<<<grid_for(units * 32), 256, 0, st>>>(a, cd, sd, d, base, acc, out);
-  if (L.n_long) k_res_long<<<grid_for(L.n_long), 256, 0, st>>>(L.n_long, acc, sd, d, base, out);
-  cudaError_t e = cudaGetLastError();
+  cudaError_t e = cudaMemsetAsync(acc, 0, sizeof(double) * ((size_t)L.n_long + 1), st);
+  if (e == cudaSuccess) {
+    k_res_prologue<<<grid_for((long long)m + 1), 256, 0, st>>>(m, L.perm, L.outdeg,
+                                                               (const float *)dv, cd, sd);
+    const long long units = (long long)L.n_chunks + L.n_slices + L.n_zblk;
+    k_res_sweep<<<grid_for(units * 32), 256, 0, st>>>(a, cd, sd, d, base, acc, out);
+    if (L.n_long)
+      k_res_long<<<grid_for(L.n_long), 256, 0, st>>>(L.n_long, acc, sd, d, base, out);
+    e = cudaGetLastError();
+  }
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(residual, out, sizeof(double), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);

@@ -672,11 +672,17 @@ int build_chunk_table(gpr_graph *g, int dmax, int chunk, cudaStream_t st) {
   const gpr::PrLayout &L = g->L;
   int *cnt = nullptr;
   GPR_TRY(gpr::dalloc(&cnt, 1, "chunk count"));
-  cudaMemsetAsync(cnt, 0, sizeof(int), st);
-  if (L.n_nz > 0)
-    k_b_count<<<(unsigned)gpr::ceil_div(L.n_nz, 256), 256, 0, st>>>(L.n_nz, L.csr_ptr, dmax, cnt);
   int nlong = 0;
-  cudaError_t e = cudaMemcpyAsync(&nlong, cnt, sizeof(int), cudaMemcpyDeviceToHost, st);
+  cudaError_t e = cudaMemsetAsync(cnt, 0, sizeof(int), st);
+  if (e == cudaSuccess) {
+    if (L.n_nz > 0)
+      k_b_count<<<(unsigned)gpr::ceil_div(L.n_nz, 256), 256, 0, st>>>(L.n_nz, L.csr_ptr, dmax,
+                                                                       cnt);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) {
+    e = cudaMemcpyAsync(&nlong, cnt, sizeof(int), cudaMemcpyDeviceToHost, st);
+  }
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   gpr::dfree(cnt);
   if (e != cudaSuccess) {
@@ -754,12 +760,15 @@ int build_packets(gpr_graph *g, int R, long long want, cudaStream_t st) {
   const int n_units = g->b_nchunks + (int)gpr::ceil_div((long long)L.n_nz - g->b_nlong, R);
   long long *cost = nullptr;
   GPR_TRY(gpr::dalloc(&cost, (size_t)std::max(1, n_units), "packet costs"));
-  if (n_units > 0)
+  int rc = GPR_OK;
+  if (n_units > 0) {
     k_pk_cost<<<(unsigned)gpr::ceil_div(n_units, 256), 256, 0, st>>>(
         g->b_nchunks, n_units, R, g->b_nlong, L.n_nz, reinterpret_cast<const int4 *>(g->b_cdesc),
         L.csr_ptr, cost);
+    rc = GPR_CUDA_RC(cudaGetLastError());
+  }
   int npk = 0;
-  const int rc = gpr::make_packets(cost, n_units, want, &g->b_pk, &npk, st);
+  if (rc == GPR_OK) rc = gpr::make_packets(cost, n_units, want, &g->b_pk, &npk, st);
   gpr::dfree(cost);
   GPR_TRY(rc);
   g->b_npk = npk;

@@ -166,8 +166,10 @@ int build_push_edges(gpr_graph *g) {
     int bits = 1;
     while ((1LL << bits) < L.m) ++bits;
     size_t tb = 0;
-    cudaError_t e = cub::DeviceRadixSort::SortPairs(nullptr, tb, L.csr_col, src, rows, dst, (int)n,
-                                                    0, bits, st);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+      e = cub::DeviceRadixSort::SortPairs(nullptr, tb, L.csr_col, src, rows, dst, (int)n, 0, bits,
+                                          st);
     void *tmp = nullptr;
     if (e == cudaSuccess) rc = gpr::dmalloc(&tmp, tb, "sort scratch");
     if (e == cudaSuccess && rc == GPR_OK)
