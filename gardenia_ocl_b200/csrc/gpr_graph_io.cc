@@ -15,11 +15,17 @@
 #include <string.h>
 
 #include <algorithm>
+#include <new>
 #include <string>
 #include <thread>
 #include <vector>
 
 #include "gardenia_graph_io.h"
+#include "gpr.h"
+
+namespace gpr {
+void set_error(const char *fmt, ...);
+}
 
 namespace {
 
@@ -123,6 +129,7 @@ void fill_data(int m, int &nnz, int *&row_offsets, int *&column_indices, WeightT
     printf(" %d redundent edges are removed\n", num_redundents);
   }
   row_offsets = (int *)malloc((size_t)(m + 1) * sizeof(int));
+  if (!row_offsets) throw std::bad_alloc();
   long long count = 0;
   for (int i = 0; i < m; i++) {
     row_offsets[i] = (int)count;
@@ -135,6 +142,7 @@ void fill_data(int m, int &nnz, int *&row_offsets, int *&column_indices, WeightT
   printf("num_vertices %d num_edges %d\n", m, nnz);
   column_indices = (int *)malloc((size_t)(count > 0 ? count : 1) * sizeof(int));
   weight = (WeightT *)malloc((size_t)(count > 0 ? count : 1) * sizeof(WeightT));
+  if (!column_indices || !weight) throw std::bad_alloc();
   long long k = 0;
   for (int i = 0; i < m; i++)
     for (const Edge &e : vertices[i]) {
@@ -157,10 +165,14 @@ inline void add_edge(std::vector<std::vector<Edge>> &v, int src, int dst, Weight
 
 bool in_range(int x, int m) { return x >= 0 && x < m; }
 
-[[noreturn]] void bad(const char *path, const char *why) {
-  fprintf(stderr, "read_graph: %s: %s\n", path, why);
-  exit(EXIT_FAILURE);
-}
+// An unreadable or malformed file.  read_graph turns it into the
+// reference's message and exit; the C entry points into a status.
+struct ReadError {
+  const char *path;
+  const char *why;
+};
+
+[[noreturn]] void bad(const char *path, const char *why) { throw ReadError{path, why}; }
 
 void mtx2csr(const char *path, int &m, int &n, int &nnz, int *&rowptr, int *&col, WeightT *&w,
              bool symmetrize, bool transpose, bool sorted, bool rm_self, bool rm_dup) {
@@ -172,7 +184,7 @@ void mtx2csr(const char *path, int &m, int &n, int &nnz, int *&rowptr, int *&col
   while (b < e && R.buf[b] == '%')
     if (!R.line(&b, &e)) bad(path, "missing size line");
   const char *p = R.buf.data() + b, *pe = R.buf.data() + e;
-  if (!parse_int(p, pe, &m) || !parse_int(p, pe, &n) || !parse_int(p, pe, &nnz))
+  if (!parse_int(p, pe, &m) || !parse_int(p, pe, &n) || !parse_int(p, pe, &nnz) || m < 0)
     bad(path, "bad size line");
   if (m != n) printf("Warning, m(%d) != n(%d)\n", m, n);
   std::vector<std::vector<Edge>> v((size_t)m);
@@ -210,7 +222,7 @@ void graph2csr(const char *path, int &m, int &nnz, int *&rowptr, int *&col, Weig
   size_t b, e;
   if (!R.line(&b, &e)) bad(path, "empty file");
   const char *p = R.buf.data() + b, *pe = R.buf.data() + e;
-  if (!parse_int(p, pe, &m) || !parse_int(p, pe, &nnz)) bad(path, "bad size line");
+  if (!parse_int(p, pe, &m) || !parse_int(p, pe, &nnz) || m < 0) bad(path, "bad size line");
   std::vector<std::vector<Edge>> v((size_t)m);
   for (int src = 0; src < m; src++) {
     if (!R.line(&b, &e)) break;
@@ -240,7 +252,7 @@ void gr2csr(const char *path, int &m, int &nnz, int *&rowptr, int *&col, WeightT
   if (p < pe) ++p;
   while (p < pe && (*p == ' ' || *p == '\t')) ++p;
   while (p < pe && *p != ' ' && *p != '\t') ++p;
-  if (!parse_int(p, pe, &m) || !parse_int(p, pe, &nnz)) bad(path, "bad problem line");
+  if (!parse_int(p, pe, &m) || !parse_int(p, pe, &nnz) || m < 0) bad(path, "bad problem line");
   std::vector<std::vector<Edge>> v((size_t)m);
   int src = 0, dst = 0;  // kept across lines: a missing number keeps its last value
   for (int i = 0; i < nnz; i++) {
@@ -258,8 +270,43 @@ void gr2csr(const char *path, int &m, int &nnz, int *&rowptr, int *&col, WeightT
   fill_data(m, nnz, rowptr, col, w, v, symmetrize, sorted, rm_self, rm_dup);
 }
 
+enum class Format { kMtx, kGraph, kGr, kUnknown };
+
+// graph_io.h:281-291: the format is chosen by the first matching substring.
+Format format_of(const char *path) {
+  if (strstr(path, ".mtx")) return Format::kMtx;
+  if (strstr(path, ".graph")) return Format::kGraph;
+  if (strstr(path, ".gr")) return Format::kGr;
+  return Format::kUnknown;
+}
+
+// read_graph for a file of a known format; throws ReadError or
+// std::bad_alloc, after which the output pointers hold what was allocated.
+void read_known(Format f, const char *path, int &m, int &n, int &nnz, int *&row_offsets,
+                int *&column_indices, int *&degree, WeightT *&weight, bool is_symmetrize,
+                bool is_transpose, bool sorted, bool remove_selfloops, bool remove_redundents) {
+  if (f == Format::kMtx) {
+    mtx2csr(path, m, n, nnz, row_offsets, column_indices, weight, is_symmetrize, is_transpose,
+            sorted, remove_selfloops, remove_redundents);
+  } else if (f == Format::kGraph) {
+    graph2csr(path, m, nnz, row_offsets, column_indices, weight, is_symmetrize, is_transpose,
+              sorted, remove_selfloops, remove_redundents);
+    n = m;
+  } else {
+    gr2csr(path, m, nnz, row_offsets, column_indices, weight, is_symmetrize, is_transpose,
+           sorted, remove_selfloops, remove_redundents);
+    n = m;
+  }
+  printf("Calculating degree...");
+  degree = (int *)malloc((size_t)(m > 0 ? m : 1) * sizeof(int));
+  if (!degree) throw std::bad_alloc();
+  for (int i = 0; i < m; i++) degree[i] = row_offsets[i + 1] - row_offsets[i];
+  printf(" Done\n");
+}
+
 }  // namespace
 
+// The reference's behaviour on a bad file is kept here: a message and exit.
 void read_graph(int argc, char *argv[], int &m, int &n, int &nnz, int *&row_offsets,
                 int *&column_indices, int *&degree, WeightT *&weight, bool is_symmetrize,
                 bool is_transpose, bool sorted, bool remove_selfloops, bool remove_redundents) {
@@ -268,25 +315,21 @@ void read_graph(int argc, char *argv[], int &m, int &n, int &nnz, int *&row_offs
     exit(EXIT_FAILURE);
   }
   const char *path = argv[1];
-  if (strstr(path, ".mtx")) {
-    mtx2csr(path, m, n, nnz, row_offsets, column_indices, weight, is_symmetrize, is_transpose,
-            sorted, remove_selfloops, remove_redundents);
-  } else if (strstr(path, ".graph")) {
-    graph2csr(path, m, nnz, row_offsets, column_indices, weight, is_symmetrize, is_transpose,
-              sorted, remove_selfloops, remove_redundents);
-    n = m;
-  } else if (strstr(path, ".gr")) {
-    gr2csr(path, m, nnz, row_offsets, column_indices, weight, is_symmetrize, is_transpose,
-           sorted, remove_selfloops, remove_redundents);
-    n = m;
-  } else {
+  const Format f = format_of(path);
+  if (f == Format::kUnknown) {
     printf("Unrecognizable input file format\n");
     exit(0);
   }
-  printf("Calculating degree...");
-  degree = (int *)malloc((size_t)(m > 0 ? m : 1) * sizeof(int));
-  for (int i = 0; i < m; i++) degree[i] = row_offsets[i + 1] - row_offsets[i];
-  printf(" Done\n");
+  try {
+    read_known(f, path, m, n, nnz, row_offsets, column_indices, degree, weight, is_symmetrize,
+               is_transpose, sorted, remove_selfloops, remove_redundents);
+  } catch (const ReadError &e) {
+    fprintf(stderr, "read_graph: %s: %s\n", e.path, e.why);
+    exit(EXIT_FAILURE);
+  } catch (const std::bad_alloc &) {
+    fprintf(stderr, "read_graph: %s: out of host memory\n", path);
+    exit(EXIT_FAILURE);
+  }
 }
 
 namespace {
@@ -552,8 +595,9 @@ void parse_pushes_sequential(const char *path, bool symmetrize, bool transpose, 
     if (p < pe) ++p;
     while (p < pe && (*p == ' ' || *p == '\t')) ++p;
     while (p < pe && *p != ' ' && *p != '\t') ++p;
-    if (!parse_int(p, pe, &m) || !parse_int(p, pe, &nnz)) bad(path, "bad problem line");
-  } else if (!parse_int(p, pe, &m) || !parse_int(p, pe, &n) || !parse_int(p, pe, &nnz)) {
+    if (!parse_int(p, pe, &m) || !parse_int(p, pe, &nnz) || m < 0) bad(path, "bad problem line");
+  } else if (!parse_int(p, pe, &m) || !parse_int(p, pe, &n) || !parse_int(p, pe, &nnz) ||
+             m < 0) {
     bad(path, "bad size line");
   }
   int src = 0, dst = 0;
@@ -607,7 +651,16 @@ extern "C" int gpr_parse_edges(const char *path, int symmetrize, int transpose, 
   }
   if (rc == -2) {
     P = Pushes();
-    parse_pushes_sequential(path, symmetrize != 0, transpose != 0, &m, &nnz, &P);
+    try {
+      parse_pushes_sequential(path, symmetrize != 0, transpose != 0, &m, &nnz, &P);
+    } catch (const ReadError &e) {
+      fprintf(stderr, "gpr_parse_edges: %s: %s\n", e.path, e.why);
+      gpr::set_error("gpr_parse_edges: %s: %s", e.path, e.why);
+      return 1;
+    } catch (const std::bad_alloc &) {
+      gpr::set_error("gpr_parse_edges: %s: out of host memory", path);
+      return 2;
+    }
   }
   const size_t k = P.row.size();
   *row = (int *)malloc(sizeof(int) * (k ? k : 1));
@@ -631,15 +684,44 @@ extern "C" int gpr_read_graph(const char *path, int symmetrize, int transpose, i
                               int remove_selfloops, int remove_redundents, int *m_out,
                               int *nnz_out, int **row_offsets, int **column_indices,
                               int **degree, float **weight) {
-  char *argv[2] = {(char *)"gpr", (char *)path};
+  if (!path || !m_out || !nnz_out || !row_offsets || !column_indices || !degree || !weight) {
+    gpr::set_error("gpr_read_graph: NULL argument");
+    return GPR_EINVAL;
+  }
+  const Format f = format_of(path);
+  if (f == Format::kUnknown) {
+    gpr::set_error("gpr_read_graph: %s: unrecognizable input file format", path);
+    return GPR_EINVAL;
+  }
   int m = 0, n = 0, nnz = 0;
-  read_graph(2, argv, m, n, nnz, *row_offsets, *column_indices, *degree, *weight,
-             symmetrize != 0, transpose != 0, sorted != 0, remove_selfloops != 0,
-             remove_redundents != 0);
+  int *rp = nullptr, *ci = nullptr, *deg = nullptr;
+  WeightT *w = nullptr;
+  int rc = GPR_OK;
+  try {
+    read_known(f, path, m, n, nnz, rp, ci, deg, w, symmetrize != 0, transpose != 0, sorted != 0,
+               remove_selfloops != 0, remove_redundents != 0);
+  } catch (const ReadError &e) {
+    gpr::set_error("gpr_read_graph: %s: %s", e.path, e.why);
+    rc = GPR_EINVAL;
+  } catch (const std::bad_alloc &) {
+    gpr::set_error("gpr_read_graph: %s: out of host memory", path);
+    rc = GPR_ENOMEM;
+  }
+  fflush(stdout);
+  if (rc != GPR_OK) {
+    free(rp);
+    free(ci);
+    free(deg);
+    free(w);
+    return rc;
+  }
   *m_out = m;
   *nnz_out = nnz;
-  fflush(stdout);
-  return 0;
+  *row_offsets = rp;
+  *column_indices = ci;
+  *degree = deg;
+  *weight = w;
+  return GPR_OK;
 }
 
 extern "C" void gpr_read_graph_free(void *p) { free(p); }

@@ -358,7 +358,11 @@ int gpr_set_device(int device);
 /* ---- graph_io (host) ------------------------------------------------------
  * read_graph of include/graph_io.h:280 for foreign callers: same parsers and
  * flags as the C++ read_graph in gardenia_graph_io.h; arrays are malloc'd and
- * released with gpr_read_graph_free. */
+ * released with gpr_read_graph_free.  Where the C++ read_graph prints a
+ * message and exits (as the reference does), this returns GPR_EINVAL (a file
+ * that cannot be opened, of no known format, or malformed: missing lines,
+ * a negative vertex count, an index out of range) or GPR_ENOMEM, with the
+ * reason in gpr_last_error() and nothing left allocated. */
 int gpr_read_graph(const char *path, int symmetrize, int transpose, int sorted,
                    int remove_selfloops, int remove_redundents, int *m, int *nnz,
                    int **row_offsets, int **column_indices, int **degree,
