@@ -615,8 +615,7 @@ def parse_edges(path, symmetrize=False, transpose=False, threads=0):
     p = [C.c_void_p() for _ in range(3)]
     st = L.gpr_parse_edges(os.fsencode(path), int(symmetrize), int(transpose), int(threads),
                            C.byref(m), C.byref(nnz), C.byref(n), *[C.byref(q) for q in p])
-    if st != 0:
-        raise GprError(GPR_EINVAL, f"cannot parse {path}")
+    _check(st)
     k = n.value
 
     def take(ptr, ct, dt):

@@ -15,6 +15,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <exception>
 #include <new>
 #include <string>
 #include <thread>
@@ -639,34 +640,42 @@ void parse_pushes_sequential(const char *path, bool symmetrize, bool transpose, 
 extern "C" int gpr_parse_edges(const char *path, int symmetrize, int transpose, int threads,
                                int *m_out, int *nnz_header, long long *n_push, int **row,
                                int **col, float **wt) {
-  if (!path || !m_out || !nnz_header || !n_push || !row || !col || !wt) return 1;
-  Pushes P;
-  const char *why = "";
-  int m = 0, nnz = 0;
-  const int rc = parse_pushes(path, symmetrize != 0, transpose != 0,
-                              threads > 0 ? threads : io_threads(), &m, &nnz, &P, &why);
-  if (rc == -1) {
-    fprintf(stderr, "gpr_parse_edges: %s: %s\n", path, why);
+  if (!path || !m_out || !nnz_header || !n_push || !row || !col || !wt) {
+    gpr::set_error("gpr_parse_edges: NULL argument");
     return 1;
   }
-  if (rc == -2) {
-    P = Pushes();
-    try {
+  Pushes P;
+  int m = 0, nnz = 0;
+  try {
+    const char *why = "";
+    const int rc = parse_pushes(path, symmetrize != 0, transpose != 0,
+                                threads > 0 ? threads : io_threads(), &m, &nnz, &P, &why);
+    if (rc == -1) bad(path, why);
+    if (rc == -2) {
+      P = Pushes();
       parse_pushes_sequential(path, symmetrize != 0, transpose != 0, &m, &nnz, &P);
-    } catch (const ReadError &e) {
-      fprintf(stderr, "gpr_parse_edges: %s: %s\n", e.path, e.why);
-      gpr::set_error("gpr_parse_edges: %s: %s", e.path, e.why);
-      return 1;
-    } catch (const std::bad_alloc &) {
-      gpr::set_error("gpr_parse_edges: %s: out of host memory", path);
-      return 2;
     }
+  } catch (const ReadError &e) {
+    fprintf(stderr, "gpr_parse_edges: %s: %s\n", e.path, e.why);
+    gpr::set_error("gpr_parse_edges: %s: %s", e.path, e.why);
+    return 1;
+  } catch (const std::exception &e) {  // host memory or threads
+    gpr::set_error("gpr_parse_edges: %s: %s", path, e.what());
+    return 2;
   }
   const size_t k = P.row.size();
   *row = (int *)malloc(sizeof(int) * (k ? k : 1));
   *col = (int *)malloc(sizeof(int) * (k ? k : 1));
   *wt = (float *)malloc(sizeof(float) * (k ? k : 1));
-  if (!*row || !*col || !*wt) return 2;
+  if (!*row || !*col || !*wt) {
+    free(*row);
+    free(*col);
+    free(*wt);
+    *row = *col = nullptr;
+    *wt = nullptr;
+    gpr::set_error("gpr_parse_edges: %s: out of host memory", path);
+    return 2;
+  }
   if (k) {
     memcpy(*row, P.row.data(), sizeof(int) * k);
     memcpy(*col, P.col.data(), sizeof(int) * k);

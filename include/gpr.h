@@ -373,8 +373,9 @@ void gpr_read_graph_free(void *p);
  * per-vertex lists (graph_io.h:133-261): entry k appends (col[k], wt[k]) to
  * the list of vertex row[k]; symmetrize / transpose as in read_graph.
  * Parsed by `threads` threads (<= 0: all cores, GPR_IO_THREADS overrides);
- * arrays malloc'd, released with gpr_read_graph_free.  Returns 0, or
- * non-zero when the file cannot be read. */
+ * arrays malloc'd, released with gpr_read_graph_free.  Returns GPR_OK,
+ * GPR_EINVAL when the file cannot be read or is malformed, or GPR_ENOMEM;
+ * the reason is in gpr_last_error() and nothing is left allocated. */
 int gpr_parse_edges(const char *path, int symmetrize, int transpose, int threads,
                     int *m, int *nnz_header, long long *n_push, int **row,
                     int **col, float **wt);
