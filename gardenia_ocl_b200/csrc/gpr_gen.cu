@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "gpr_internal.cuh"
+#include "gpr_guard.h"
 
 namespace {
 
@@ -263,6 +264,7 @@ extern "C" {
 int gpr_gen_rmat(int scale, int edge_factor, double a, double b, double c,
                  unsigned long long seed, int do_scramble, int **d_rowptr, int **d_col,
                  int **d_outdeg, long long *nnz_out) {
+  GPR_ENTRY_BEGIN
   if (scale < 1 || scale > 30 || edge_factor < 1 || !d_rowptr || !d_col || !d_outdeg ||
       !nnz_out || !(a >= 0 && b >= 0 && c >= 0 && a + b + c <= 1.0)) {
     gpr::set_error("gpr_gen_rmat: invalid arguments");
@@ -294,11 +296,13 @@ int gpr_gen_rmat(int scale, int edge_factor, double a, double b, double c,
   gpr::dfree(k0);
   gpr::dfree(k1);
   return rc;
+  GPR_ENTRY_END("gpr_gen_rmat")
 }
 
 int gpr_gen_multigraph(int n_graphs, int m_min, int m_max, int er_deg, int cl_deg, double gamma,
                        unsigned long long seed, int *h_voff, int **d_rowptr, int **d_col,
                        int **d_outdeg, long long *nnz_out) {
+  GPR_ENTRY_BEGIN
   if (n_graphs < 1 || m_min < 1 || m_max < m_min || er_deg < 1 || cl_deg < 1 ||
       !(gamma > 1.0) || !h_voff || !d_rowptr || !d_col || !d_outdeg || !nnz_out) {
     gpr::set_error("gpr_gen_multigraph: invalid arguments");
@@ -373,9 +377,11 @@ int gpr_gen_multigraph(int n_graphs, int m_min, int m_max, int er_deg, int cl_de
   gpr::dfree(dP);
   if (rc == GPR_OK) memcpy(h_voff, voff.data(), sizeof(int) * voff.size());
   return rc;
+  GPR_ENTRY_END("gpr_gen_multigraph")
 }
 
 int gpr_gen_stencil27(int n, int **d_Ap, int **d_Aj, float **d_Ax, long long *nnz_out) {
+  GPR_ENTRY_BEGIN
   if (n < 1 || n > 1290 || !d_Ap || !d_Aj || !d_Ax || !nnz_out) {
     gpr::set_error("gpr_gen_stencil27: invalid arguments");
     return GPR_EINVAL;
@@ -420,6 +426,7 @@ int gpr_gen_stencil27(int n, int **d_Ap, int **d_Aj, float **d_Ax, long long *nn
   *d_Ax = Ax;
   *nnz_out = nnz;
   return GPR_OK;
+  GPR_ENTRY_END("gpr_gen_stencil27")
 }
 
 int gpr_gen_uniform(long long n, unsigned long long seed, float *d_out) {

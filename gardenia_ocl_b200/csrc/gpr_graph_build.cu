@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "gpr_internal.cuh"
+#include "gpr_guard.h"
 
 extern "C" int gpr_parse_edges(const char *path, int symmetrize, int transpose, int threads,
                                int *m_out, int *nnz_header, long long *n_push, int **row,
@@ -291,6 +292,7 @@ int gpr_csr_from_edges(int m, long long n, const int *any_row, const int *any_co
                        const float *any_wt, int sorted, int remove_selfloops,
                        int remove_redundents, int **d_rowptr, int **d_col, float **d_wt,
                        long long *nnz_out) {
+  GPR_ENTRY_BEGIN
   if (m < 0 || n < 0 || n > 0x7fffffffLL || (n > 0 && (!any_row || !any_col)) || !d_rowptr ||
       !d_col || !nnz_out) {
     gpr::set_error("gpr_csr_from_edges: invalid arguments");
@@ -312,12 +314,14 @@ int gpr_csr_from_edges(int m, long long n, const int *any_row, const int *any_co
   if (ocol) gpr::dfree(c);
   if (owt) gpr::dfree(w);
   return rc;
+  GPR_ENTRY_END("gpr_csr_from_edges")
 }
 
 int gpr_read_graph_gpu(const char *path, int symmetrize, int transpose, int sorted,
                        int remove_selfloops, int remove_redundents, int *m_out,
                        long long *nnz_out, int **d_rowptr, int **d_col, int **d_degree,
                        float **d_wt) {
+  GPR_ENTRY_BEGIN
   if (!path || !m_out || !nnz_out || !d_rowptr || !d_col || !d_degree) {
     gpr::set_error("gpr_read_graph_gpu: NULL argument");
     return GPR_EINVAL;
@@ -337,11 +341,13 @@ int gpr_read_graph_gpu(const char *path, int symmetrize, int transpose, int sort
   }
   *m_out = H.m;
   return GPR_OK;
+  GPR_ENTRY_END("gpr_read_graph_gpu")
 }
 
 int gpr_read_graph_pr(const char *path, int symmetrize, int *m_out, long long *nnz_out_csr,
                       long long *nnz_in_csr, int **d_out_rowptr, int **d_out_col,
                       int **d_out_degree, int **d_in_rowptr, int **d_in_col) {
+  GPR_ENTRY_BEGIN
   if (!path || !m_out || !nnz_out_csr || !nnz_in_csr || !d_out_rowptr || !d_out_col ||
       !d_out_degree || !d_in_rowptr || !d_in_col) {
     gpr::set_error("gpr_read_graph_pr: NULL argument");
@@ -366,6 +372,7 @@ int gpr_read_graph_pr(const char *path, int symmetrize, int *m_out, long long *n
   }
   *m_out = H.m;
   return GPR_OK;
+  GPR_ENTRY_END("gpr_read_graph_pr")
 }
 
 }  // extern "C"

@@ -39,6 +39,7 @@
 
 #include "gpr_device.cuh"
 #include "gpr_internal.cuh"
+#include "gpr_guard.h"
 
 using namespace gpr::dev;
 
@@ -1148,6 +1149,7 @@ extern "C" {
 int gpr_multigraph_create(int n_graphs, const int *h_voff, long long nnz, const int *any_rowptr,
                           const int *any_col, const int *any_outdeg,
                           const gpr_layout_opts *h_lopts, gpr_multigraph **out) {
+  GPR_ENTRY_BEGIN
   if (!out) {
     gpr::set_error("gpr_multigraph_create: NULL out");
     return GPR_EINVAL;
@@ -1222,6 +1224,7 @@ int gpr_multigraph_create(int n_graphs, const int *h_voff, long long nnz, const 
   }
   *out = g;
   return GPR_OK;
+  GPR_ENTRY_END("gpr_multigraph_create")
 }
 
 int gpr_multigraph_destroy(gpr_multigraph *g) {
@@ -1256,6 +1259,7 @@ int gpr_multigraph_set_stream(gpr_multigraph *g, void *stream) {
 
 int gpr_multigraph_pagerank(gpr_multigraph *g, float *any_scores, const gpr_pr_opts *opts,
                             int *h_iters, double *h_residuals, gpr_pr_stats *stats) {
+  GPR_ENTRY_BEGIN
   if (!g) {
     gpr::set_error("gpr_multigraph_pagerank: NULL handle");
     return GPR_EINVAL;
@@ -1266,6 +1270,7 @@ int gpr_multigraph_pagerank(gpr_multigraph *g, float *any_scores, const gpr_pr_o
   int rc = multi_pagerank_impl(g, any_scores, opts, h_iters, h_residuals, stats);
   if (cur != g->device && cur >= 0) cudaSetDevice(cur);
   return rc;
+  GPR_ENTRY_END("gpr_multigraph_pagerank")
 }
 
 }  // extern "C"

@@ -30,6 +30,7 @@
 #include <mutex>
 
 #include "gpr_internal.cuh"
+#include "gpr_guard.h"
 
 namespace {
 
@@ -173,6 +174,7 @@ long long gpr_pagerank_noalloc_max_vertices(void) { return kNoAllocMaxVertices; 
 int gpr_pagerank_noalloc(int m, int nnz, const int *d_rowptr, const int *d_col,
                          const int *d_outdeg, float *d_scores, const gpr_pr_opts *opts,
                          gpr_pr_stats *stats, void *stream) {
+  GPR_ENTRY_BEGIN
   gpr_pr_opts o;
   if (opts) o = *opts;
   else gpr_pr_opts_default(&o);
@@ -251,6 +253,7 @@ int gpr_pagerank_noalloc(int m, int nnz, const int *d_rowptr, const int *d_col,
   st.loop_ms = st.solve_ms;
   if (stats) *stats = st;
   return GPR_OK;
+  GPR_ENTRY_END("gpr_pagerank_noalloc")
 }
 
 }  // extern "C"

@@ -31,6 +31,7 @@
 
 #include "gpr_device.cuh"
 #include "gpr_internal.cuh"
+#include "gpr_guard.h"
 
 using gpr::PrLayout;
 
@@ -920,6 +921,7 @@ int gpr_graph_create(int m, long long nnz, const int *any_rowptr, const int *any
 
 int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr, const int *any_col,
                         const int *any_outdeg, const gpr_layout_opts *lopts, gpr_graph **out) {
+  GPR_ENTRY_BEGIN
   int lane_max = gpr::kSellMaxDefault, chunk = gpr::kChunkDefault,
       chunk_min = gpr::kChunkMinDefault, hot_max = gpr::kHotDefault;
   if (lopts && lopts->sell_max) lane_max = lopts->sell_max;
@@ -958,6 +960,7 @@ int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr, const int *
   }
   *out = g;
   return GPR_OK;
+  GPR_ENTRY_END("gpr_graph_create_ex")
 }
 
 int gpr_graph_destroy(gpr_graph *g) {
@@ -1017,6 +1020,7 @@ int gpr_graph_residuals(const gpr_graph *g, double *h_out, int n) {
 }
 
 int gpr_pagerank(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts, gpr_pr_stats *stats) {
+  GPR_ENTRY_BEGIN
   if (!g) {
     gpr::set_error("gpr_pagerank: NULL graph");
     return GPR_EINVAL;
@@ -1027,9 +1031,11 @@ int gpr_pagerank(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts, gpr_p
   int rc = pagerank_impl(g, any_scores, opts, stats);
   if (cur != g->device && cur >= 0) cudaSetDevice(cur);
   return rc;
+  GPR_ENTRY_END("gpr_pagerank")
 }
 
 int gpr_pr_residual_f64(gpr_graph *g, const float *any_scores, float damping, double *residual) {
+  GPR_ENTRY_BEGIN
   if (!g || !any_scores || !residual) {
     gpr::set_error("gpr_pr_residual_f64: NULL argument");
     return GPR_EINVAL;
@@ -1072,24 +1078,29 @@ int gpr_pr_residual_f64(gpr_graph *g, const float *any_scores, float damping, do
     return GPR_ECUDA;
   }
   return GPR_OK;
+  GPR_ENTRY_END("gpr_pr_residual_f64")
 }
 
 int gpr_page_rank(int m, int nnz, const int *row_offsets, const int *column_indices,
                   const int *degree, float *scores, const gpr_pr_opts *opts,
                   gpr_pr_stats *stats) {
+  GPR_ENTRY_BEGIN
   gpr_graph *g = nullptr;
   GPR_TRY(gpr_graph_create(m, nnz, row_offsets, column_indices, degree, &g));
   int rc = gpr_pagerank(g, scores, opts, stats);
   gpr_graph_destroy(g);
   return rc;
+  GPR_ENTRY_END("gpr_page_rank")
 }
 
 int gpr_pr_solver(int m, int nnz, const int *in_row_offsets, const int *in_column_indices,
                   const int *out_row_offsets, const int *out_column_indices, const int *degree,
                   float *scores, const gpr_pr_opts *opts, gpr_pr_stats *stats) {
+  GPR_ENTRY_BEGIN
   (void)out_row_offsets;  // pull variants ignore the out-CSR (src/pr/gather.cu:41)
   (void)out_column_indices;
   return gpr_page_rank(m, nnz, in_row_offsets, in_column_indices, degree, scores, opts, stats);
+  GPR_ENTRY_END("gpr_pr_solver")
 }
 
 }  // extern "C"

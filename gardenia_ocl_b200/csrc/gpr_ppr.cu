@@ -36,6 +36,7 @@
 
 #include "gpr_device.cuh"
 #include "gpr_internal.cuh"
+#include "gpr_guard.h"
 
 namespace {
 
@@ -828,6 +829,7 @@ struct Bufs {
 
 extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
                        const gpr_pr_opts *opts_in, int *h_iters, gpr_pr_stats *stats) {
+  GPR_ENTRY_BEGIN
   gpr_pr_opts o;
   if (opts_in) o = *opts_in;
   else gpr_pr_opts_default(&o);
@@ -1117,4 +1119,5 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
     }
   }
   return GPR_OK;
+  GPR_ENTRY_END("gpr_ppr")
 }

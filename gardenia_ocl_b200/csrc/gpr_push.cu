@@ -32,6 +32,7 @@
 
 #include "gpr_device.cuh"
 #include "gpr_internal.cuh"
+#include "gpr_guard.h"
 
 using namespace gpr::dev;
 
@@ -298,6 +299,7 @@ int push_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts &o, gpr_pr_stat
 
 extern "C" int gpr_pagerank_push(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts,
                                  gpr_pr_stats *stats) {
+  GPR_ENTRY_BEGIN
   if (!g) {
     gpr::set_error("gpr_pagerank_push: NULL graph");
     return GPR_EINVAL;
@@ -322,4 +324,5 @@ extern "C" int gpr_pagerank_push(gpr_graph *g, float *any_scores, const gpr_pr_o
   if (stats) *stats = st;
   if (cur != g->device && cur >= 0) cudaSetDevice(cur);
   return rc;
+  GPR_ENTRY_END("gpr_pagerank_push")
 }

@@ -11,6 +11,7 @@
 #include <string.h>
 
 #include "gpr_internal.cuh"
+#include "gpr_guard.h"
 
 using gpr::SpmvLayout;
 
@@ -206,6 +207,7 @@ extern "C" {
 
 int gpr_matrix_create(int m, long long nnz, const int *any_Ap, const int *any_Aj,
                       const float *any_Ax, gpr_matrix **out) {
+  GPR_ENTRY_BEGIN
   if (!out) {
     gpr::set_error("gpr_matrix_create: NULL out");
     return GPR_EINVAL;
@@ -230,6 +232,7 @@ int gpr_matrix_create(int m, long long nnz, const int *any_Ap, const int *any_Aj
   }
   *out = A;
   return GPR_OK;
+  GPR_ENTRY_END("gpr_matrix_create")
 }
 
 int gpr_matrix_destroy(gpr_matrix *A) {
@@ -284,6 +287,7 @@ int gpr_matrix_layout(const gpr_matrix *A, int *n_long, int *n_chunks, int *n_sl
 
 int gpr_spmv_solver(int m, int nnz, const int *Ap, const int *Aj, const float *Ax, const float *x,
                     float *y) {
+  GPR_ENTRY_BEGIN
   if (m < 0 || (m > 0 && (!x || !y))) {
     gpr::set_error("gpr_spmv_solver: invalid arguments");
     return GPR_EINVAL;
@@ -312,6 +316,7 @@ int gpr_spmv_solver(int m, int nnz, const int *Ap, const int *Aj, const float *A
   if (oy) gpr::dfree(dy);
   gpr_matrix_destroy(A);
   return rc;
+  GPR_ENTRY_END("gpr_spmv_solver")
 }
 
 }  // extern "C"

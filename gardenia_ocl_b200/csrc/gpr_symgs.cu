@@ -27,6 +27,7 @@
 
 #include "gpr_device.cuh"
 #include "gpr_internal.cuh"
+#include "gpr_guard.h"
 
 using namespace gpr::dev;
 
@@ -267,6 +268,7 @@ extern "C" {
 int gpr_symgs_create(int m, long long nnz, const int *any_Ap, const int *any_Aj,
                      const float *any_Ax, const int *any_indices, const int *any_color_offsets,
                      int n_colors, gpr_symgs **out) {
+  GPR_ENTRY_BEGIN
   if (!out) {
     gpr::set_error("gpr_symgs_create: NULL out");
     return GPR_EINVAL;
@@ -319,6 +321,7 @@ int gpr_symgs_create(int m, long long nnz, const int *any_Ap, const int *any_Aj,
   }
   *out = h;
   return GPR_OK;
+  GPR_ENTRY_END("gpr_symgs_create")
 }
 
 int gpr_symgs_destroy(gpr_symgs *h) {
@@ -327,6 +330,7 @@ int gpr_symgs_destroy(gpr_symgs *h) {
 }
 
 int gpr_symgs_apply(gpr_symgs *h, float *any_x, const float *any_b, int sweeps, double *loop_ms) {
+  GPR_ENTRY_BEGIN
   if (!h || !any_x || !any_b || sweeps < 0) {
     gpr::set_error("gpr_symgs_apply: invalid arguments");
     return GPR_EINVAL;
@@ -382,16 +386,19 @@ int gpr_symgs_apply(gpr_symgs *h, float *any_x, const float *any_b, int sweeps, 
     return GPR_ETIMEOUT;
   }
   return GPR_OK;
+  GPR_ENTRY_END("gpr_symgs_apply")
 }
 
 int gpr_symgs_solver(int m, int nnz, const int *Ap, const int *Aj, const int *indices,
                      const float *Ax, float *x, const float *b, const int *color_offsets,
                      int n_colors) {
+  GPR_ENTRY_BEGIN
   gpr_symgs *h = nullptr;
   GPR_TRY(gpr_symgs_create(m, nnz, Ap, Aj, Ax, indices, color_offsets, n_colors, &h));
   const int rc = gpr_symgs_apply(h, x, b, 1, nullptr);
   gpr_symgs_destroy(h);
   return rc;
+  GPR_ENTRY_END("gpr_symgs_solver")
 }
 
 }  // extern "C"

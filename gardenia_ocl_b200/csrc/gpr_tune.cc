@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "gpr.h"
+#include "gpr_guard.h"
 
 namespace {
 
@@ -178,24 +179,29 @@ void descend(Cfg *x, double *best, const std::vector<T> &vals, F apply,
 extern "C" {
 
 int gpr_tune_signature(int m, long long nnz, const int *h_rowptr, int batch, char *buf, int len) {
+  GPR_ENTRY_BEGIN
   if (m < 0 || nnz < 0 || (m > 0 && !h_rowptr) || !buf || len < 1) return GPR_EINVAL;
   const std::string s = signature(m, nnz, h_rowptr, 0, batch == 0);
   snprintf(buf, (size_t)len, "%s", s.c_str());
   return GPR_OK;
+  GPR_ENTRY_END("gpr_tune_signature")
 }
 
 int gpr_tune_cache_lookup(const char *cache_path, const char *sig, gpr_tune_result *out) {
+  GPR_ENTRY_BEGIN
   if (!cache_path || !sig || !out) return GPR_EINVAL;
   auto c = load_cache(cache_path);
   auto it = c.find(sig);
   if (it == c.end()) return GPR_EINVAL;
   fill_result(out, sig, it->second.first, it->second.second, 0.0, 0, 1);
   return GPR_OK;
+  GPR_ENTRY_END("gpr_tune_cache_lookup")
 }
 
 int gpr_tune_graph(int m, long long nnz, const int *any_rowptr, const int *any_col,
                    const int *any_outdeg, const char *cache_path, int sweeps,
                    gpr_tune_result *out) {
+  GPR_ENTRY_BEGIN
   if (m < 1 || nnz < 0 || !any_rowptr || !any_outdeg || (nnz > 0 && !any_col) || sweeps < 1 ||
       !out)
     return GPR_EINVAL;
@@ -230,11 +236,13 @@ int gpr_tune_graph(int m, long long nnz, const int *any_rowptr, const int *any_c
   save_cache(cache_path, sig, x, best);
   fill_result(out, sig, x, best, t0, B.cands, 0);
   return GPR_OK;
+  GPR_ENTRY_END("gpr_tune_graph")
 }
 
 int gpr_tune_multigraph(int n_graphs, const int *h_voff, long long nnz, const int *any_rowptr,
                         const int *any_col, const int *any_outdeg, const char *cache_path,
                         int sweeps, gpr_layout_opts *h_lopts_out, gpr_tune_result *out) {
+  GPR_ENTRY_BEGIN
   if (n_graphs < 1 || !h_voff || !any_rowptr || !any_outdeg || sweeps < 1 || !h_lopts_out)
     return GPR_EINVAL;
   const int M = h_voff[n_graphs];
@@ -319,6 +327,7 @@ int gpr_tune_multigraph(int n_graphs, const int *h_voff, long long nnz, const in
                 cands == 1 ? 1 : 0);
   }
   return GPR_OK;
+  GPR_ENTRY_END("gpr_tune_multigraph")
 }
 
 }  // extern "C"
