@@ -105,6 +105,38 @@ def test_no_device_reports_enodev(G):
     assert e.value.status == G.GPR_ENODEV
 
 
+def _strip_comments(src):
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return re.sub(r"//[^\n]*", "", src)
+
+
+def _function_body(src, signature):
+    i = src.index("{", src.index(signature))
+    depth = 0
+    for j in range(i, len(src)):
+        depth += {"{": 1, "}": -1}.get(src[j], 0)
+        if depth == 0:
+            return src[i:j + 1]
+    raise ValueError(signature)
+
+
+def test_c_abi_never_exits_the_process():
+    """Only the reference-shaped C++ drop-ins print and exit, as the reference
+    does (gpr_dropin.cc, and read_graph in gpr_graph_io.cc); no other library
+    source exits, aborts or traps, so a C-ABI caller always gets a status."""
+    csrc = os.path.join(ROOT, "gardenia_ocl_b200", "csrc")
+    checked = 0
+    for name in sorted(os.listdir(csrc)):
+        if not name.endswith((".cu", ".cc", ".cuh", ".h")) or name == "gpr_dropin.cc":
+            continue
+        src = _strip_comments(open(os.path.join(csrc, name)).read())
+        if name == "gpr_graph_io.cc":
+            src = src.replace(_function_body(src, "\nvoid read_graph("), "")
+        assert not re.search(r"\b(exit|abort|quick_exit|_Exit|__trap)\s*\(", src), name
+        checked += 1
+    assert checked >= 15
+
+
 def test_invalid_arguments_rejected_before_device(G):
     with pytest.raises(G.GprError) as e:
         G.Graph(np.array([0, 0], np.int32), np.array([], np.int32), np.array([0], np.int32),
