@@ -137,6 +137,17 @@ def test_c_abi_never_exits_the_process():
     assert checked >= 15
 
 
+@pytest.mark.parametrize("tol,max_iter", [(1e-3, 30), (0.0, 7), (1e-3, 0)])
+def test_empty_graph_sweep_count_matches_oracle(G, O, tol, max_iter):
+    """m = 0 needs no device: the no-allocation entry counts the empty sweeps
+    the reference's loop counts (omp_base.cc:23-43), as the oracle does."""
+    with np.errstate(divide="ignore"):
+        _, ref_it, _ = O.pr_plain_f32(np.zeros(1, np.int32), np.zeros(0, np.int32),
+                                      np.zeros(0, np.int32), tol=tol, max_iter=max_iter)
+    st = G.pagerank_noalloc(0, 0, None, None, None, None, tol=tol, max_iter=max_iter)
+    assert st.iterations == ref_it and st.residual == 0.0
+
+
 def test_invalid_arguments_rejected_before_device(G):
     with pytest.raises(G.GprError) as e:
         G.Graph(np.array([0, 0], np.int32), np.array([], np.int32), np.array([0], np.int32),
