@@ -214,7 +214,12 @@ def run_reference(args):
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": 1e3 * total / len(times), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded RMAT)",
-        "config": workload_config(args.scale, m, len(col)),
+        "config": dict(workload_config(args.scale, m, len(col)),
+                       workload=f"pagerank_rmat{args.scale}_ef{EDGE_FACTOR}_rate_sample",
+                       sample=f"{SAMPLE_SWEEPS}-sweep rate sample (tol 0) per step of the "
+                              f"full graph, not a tol {TOL:g} solve; the rate per sweep is "
+                              "what a full solve sustains",
+                       precision="plain fp32 (fp64 residual), reference OpenMP PRSolver"),
         "cpu_baseline": {"value": gteps, "unit": "GTEPS", "cores": cores, "kind": kind,
                          "sample": sample},
         "e2e": {"value": gteps, "unit": "GTEPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -1,7 +1,7 @@
 // Guard for the bodies of C entry points: a C++ exception from host code
 // (out of host memory in a std::vector, a thread that cannot start) becomes a
 // gpr_status with a message instead of crossing the C boundary, where it would
-// end the caller's process.
+// end the caller's process.  Exceptions of any type are caught.
 //
 //   int gpr_x(...) {
 //     GPR_ENTRY_BEGIN
@@ -29,6 +29,10 @@ void set_error(const char *fmt, ...);
   }                                                                           \
   catch (const std::exception &e_) {                                          \
     gpr::set_error("%s: %s", name, e_.what());                                \
+    return GPR_EINVAL;                                                        \
+  }                                                                           \
+  catch (...) {                                                               \
+    gpr::set_error("%s: unknown host exception", name);                       \
     return GPR_EINVAL;                                                        \
   }
 

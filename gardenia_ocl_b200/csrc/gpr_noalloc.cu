@@ -178,8 +178,8 @@ int gpr_pagerank_noalloc(int m, int nnz, const int *d_rowptr, const int *d_col,
   gpr_pr_opts o;
   if (opts) o = *opts;
   else gpr_pr_opts_default(&o);
-  if (m < 0 || nnz < 0 || (m > 0 && (!d_rowptr || !d_outdeg || !d_scores)) ||
-      (nnz > 0 && !d_col)) {
+  if (m < 0 || nnz < 0 || (m == 0 && nnz != 0) ||
+      (m > 0 && (!d_rowptr || !d_outdeg || !d_scores)) || (nnz > 0 && !d_col)) {
     gpr::set_error("gpr_pagerank_noalloc: invalid arguments (m=%d nnz=%d)", m, nnz);
     return GPR_EINVAL;
   }
@@ -196,9 +196,9 @@ int gpr_pagerank_noalloc(int m, int nnz, const int *d_rowptr, const int *d_col,
   }
   gpr_pr_stats st;
   memset(&st, 0, sizeof(st));
-  if (m == 0 || o.max_iter == 0) {
+  if (m == 0) {
     // no vertices: the sweeps are empty and their residuals 0
-    if (m == 0) st.iterations = gpr::empty_graph_sweeps(o.tol, o.max_iter);
+    st.iterations = gpr::empty_graph_sweeps(o.tol, o.max_iter);
     if (stats) *stats = st;
     return GPR_OK;
   }
@@ -224,6 +224,7 @@ int gpr_pagerank_noalloc(int m, int nnz, const int *d_rowptr, const int *d_col,
   const unsigned grid = (unsigned)((m + kNoAllocBlock - 1) / kNoAllocBlock);
   GPR_CUDA(cudaMemsetAsync(a.words, 0, sizeof(int) * 8, s));
   k_na_validate<<<148 * 8, 256, 0, s>>>(m, nnz, d_rowptr, d_col, d_outdeg, a.words);
+  GPR_CUDA(cudaGetLastError());
   int words[4];
   GPR_CUDA(cudaMemcpyAsync(words, a.words, sizeof(words), cudaMemcpyDeviceToHost, s));
   GPR_CUDA(cudaStreamSynchronize(s));
@@ -231,7 +232,12 @@ int gpr_pagerank_noalloc(int m, int nnz, const int *d_rowptr, const int *d_col,
     gpr::set_error("gpr_pagerank_noalloc: malformed CSR (flags 0x%x)", words[3]);
     return GPR_EINVAL;
   }
+  if (o.max_iter == 0) {
+    if (stats) *stats = st;
+    return GPR_OK;
+  }
   k_na_prologue<<<grid, kNoAllocBlock, 0, s>>>(a);
+  GPR_CUDA(cudaGetLastError());
   int launches = 2, issued = 0, done = 0;
   while (!done && issued < o.max_iter) {
     for (int q = 0; q < 8 && issued < o.max_iter; ++q, ++issued) {
@@ -244,9 +250,12 @@ int gpr_pagerank_noalloc(int m, int nnz, const int *d_rowptr, const int *d_col,
     done = words[2];
   }
   st.iterations = words[1];
-  if (st.iterations > 0)
-    GPR_CUDA(cudaMemcpy(&st.residual, a.hist + st.iterations - 1, sizeof(double),
-                        cudaMemcpyDeviceToHost));
+  if (st.iterations > 0) {
+    // on the caller's stream: no device-wide synchronisation
+    GPR_CUDA(cudaMemcpyAsync(&st.residual, a.hist + st.iterations - 1, sizeof(double),
+                             cudaMemcpyDeviceToHost, s));
+    GPR_CUDA(cudaStreamSynchronize(s));
+  }
   st.gpu_launches = launches;
   st.solve_ms =
       std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();

@@ -267,11 +267,14 @@ int gpr_tune_cache_lookup(const char *cache_path, const char *signature,
  * scratch in a fixed device array inside the library (about 8 MiB, held by
  * every GPU that loads the library until exit).  Limits: m <= 1,048,576
  * vertices (gpr_pagerank_noalloc_max_vertices) and max_iter <= 1000, else
- * GPR_EINVAL.  The first call on a device looks up the array's device address
- * and should come before any stream capture.  Calls share the array, so calls
- * that overlap on the GPU race; run them one at a time.  Synchronous; scores
- * follow the reference's float arithmetic row by row; opts->loop / variant /
- * precision are ignored. */
+ * GPR_EINVAL.  The CSR is validated on the device on every call with m > 0
+ * (row offsets monotone from 0 to nnz, columns in range, out-degrees >= 0),
+ * also when max_iter is 0; m == 0 with nnz != 0 is rejected.  The first call
+ * on a device looks up the array's device address and should come before any
+ * stream capture.  Calls share the array, so calls that overlap on the GPU
+ * race; run them one at a time.  Synchronous: the call waits for `stream`
+ * (and only that stream) before it returns.  Scores follow the reference's
+ * float arithmetic row by row; opts->loop / variant / precision are ignored. */
 int gpr_pagerank_noalloc(int m, int nnz, const int *d_rowptr, const int *d_col,
                          const int *d_outdeg, float *d_scores,
                          const gpr_pr_opts *opts, gpr_pr_stats *stats,

@@ -39,15 +39,12 @@ KDAMP = np.float32(0.85)  # include/common.h:18
 
 def reference_root() -> str:
     """The reference tree the recipe in oracle/Makefile compiles from: its
-    REF_ROOT (environment first, then the Makefile's default)."""
+    REF_ROOT (environment first, then the Makefile's default, the directory
+    `reference` beside the repository's parent)."""
     env = os.environ.get("REF_ROOT")
     if env:
         return env
-    with open(os.path.join(_HERE, "Makefile")) as f:
-        for line in f:
-            if line.startswith("REF_ROOT ?="):
-                return line.split("?=", 1)[1].strip()
-    return ""
+    return os.path.abspath(os.path.join(_HERE, "..", "..", "reference"))
 
 
 def build() -> None:

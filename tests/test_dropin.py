@@ -42,3 +42,33 @@ def test_reference_driver_runs_on_libgpr(O, name, tol, max_iter):
     ok = O.push_check(ld[key + ":rowptr"], ld[key + ":col"], pr[f"{name}:outdeg"],
                       pr[f"{name}:{tol:g}:{max_iter}:scores"]) < 1e-3
     assert ("Correct" in out.stdout) == ok
+
+
+@pytest.mark.parametrize("name", ["test_pr.mtx", "chesapeake.mtx", "graph_small.mtx",
+                                  "graph_dups.mtx", "graph_simple.mtx"])
+@pytest.mark.parametrize("tol,max_iter", [(1e-3, 30), (1e-4, 100)])
+def test_prsolver_scores_match_reference(G, O, capfd, monkeypatch, name, tol, max_iter):
+    """libgpr's PRSolver symbol (src/pr/pr.h:23) called directly on the graphs
+    the reference solved: its scores equal the reference's scores (golden
+    fixture) within 1e-6, and bit for bit the oracle's at the same sweep
+    count (every row of these graphs has at most 64 in-edges)."""
+    import ctypes as C
+    pr = np.load(os.path.join(GOLD, "pr.npz"))
+    rp, col, od = (np.ascontiguousarray(pr[f"{name}:{k}"], dtype=np.int32)
+                   for k in ("in_rowptr", "in_col", "outdeg"))
+    m, nnz = len(rp) - 1, len(col)
+    orp, ocol = (np.ascontiguousarray(a, dtype=np.int32) for a in O.transpose_csr(m, rp, col))
+    s = np.full(m, np.float32(1.0) / np.float32(m), dtype=np.float32)
+    monkeypatch.setenv("GPR_TOL", str(tol))
+    monkeypatch.setenv("GPR_MAX_ITER", str(max_iter))
+    lib = C.CDLL(G.LIB_PATH)
+    fn = getattr(lib, "_Z8PRSolveriiPiS_S_S_S_Pf")
+    P = lambda a: a.ctypes.data_as(C.c_void_p)
+    fn(C.c_int(m), C.c_int(nnz), P(rp), P(col), P(orp), P(ocol), P(od), P(s))
+    C.CDLL(None).fflush(None)
+    out = capfd.readouterr().out
+    sweeps = int(re.search(r"iterations = (\d+)\.", out).group(1))
+    ref = pr[f"{name}:{tol:g}:{max_iter}:scores"]
+    assert np.abs(s - ref).max() <= 1e-6
+    exact, _, _ = O.pr_plain_f32(rp, col, od, tol=0.0, max_iter=sweeps)
+    assert np.array_equal(s, exact)
