@@ -24,6 +24,8 @@ LIB_PATH = os.path.join(_HERE, "lib", "libgpr.so")
 GPR_OK, GPR_EINVAL, GPR_ENOMEM, GPR_ECUDA, GPR_ETIMEOUT, GPR_ENODEV, GPR_EUNSUPPORTED = range(7)
 PREC_FP32, PREC_BF16, PREC_FP16 = 0, 1, 2
 LOOP_AUTO, LOOP_PERSISTENT, LOOP_GRAPH = 0, 1, 2
+FORM_AUTO, FORM_EXACT, FORM_BLOCKED = 0, 1, 2
+LAYOUT_BATCHED, LAYOUT_PUSH, LAYOUT_BLOCKED = 1, 2, 4
 KDAMP = np.float32(0.85)  # include/common.h:18
 EPSILON = 0.001           # src/pr/pr.h:4
 MAX_ITER = 30             # src/pr/pr.h:5
@@ -38,12 +40,14 @@ class GprError(RuntimeError):
 class PrOptions(C.Structure):
     _fields_ = [("damping", C.c_float), ("tol", C.c_double), ("max_iter", C.c_int),
                 ("precision", C.c_int), ("loop", C.c_int), ("timeout_s", C.c_double),
-                ("refine_max", C.c_int), ("variant", C.c_int), ("reserved", C.c_int * 7)]
+                ("refine_max", C.c_int), ("variant", C.c_int), ("reserved", C.c_int * 1),
+                ("form", C.c_int), ("pad", C.c_int * 5)]
 
 
 class LayoutOptions(C.Structure):
     _fields_ = [("sell_max", C.c_int), ("chunk", C.c_int), ("chunk_min", C.c_int),
-                ("hot_entries", C.c_int), ("flags", C.c_int), ("reserved", C.c_int * 3)]
+                ("hot_entries", C.c_int), ("flags", C.c_int), ("block_rows", C.c_int),
+                ("tile_words", C.c_int), ("reserved", C.c_int * 1)]
 
 
 class PrStats(C.Structure):
@@ -196,12 +200,12 @@ def _ptr(a, dtype=None):
 
 
 def options(tol=EPSILON, max_iter=MAX_ITER, damping=KDAMP, precision=PREC_FP32,
-            loop=LOOP_AUTO, timeout_s=5.0, refine_max=64, variant=0) -> PrOptions:
+            loop=LOOP_AUTO, timeout_s=5.0, refine_max=64, variant=0, form=FORM_AUTO) -> PrOptions:
     o = PrOptions()
     _check(lib().gpr_pr_opts_default(C.byref(o)))
     o.tol, o.max_iter, o.damping = float(tol), int(max_iter), float(damping)
     o.precision, o.loop, o.timeout_s, o.refine_max = int(precision), int(loop), float(timeout_s), int(refine_max)
-    o.variant = int(variant)
+    o.variant, o.form = int(variant), int(form)
     return o
 
 
@@ -247,7 +251,8 @@ class Graph:
     the out-degree of every vertex (src/pr/omp_base.cc:9 arguments)."""
 
     def __init__(self, rowptr, col, outdeg, m=None, nnz=None, sell_max=0, chunk=0, chunk_min=0,
-                 hot_entries=0, batched=False, push=False):
+                 hot_entries=0, batched=False, push=False, blocked=False, block_rows=0,
+                 tile_words=0):
         L = lib()
         m = int(len(rowptr) - 1) if m is None else int(m)
         nnz = int(len(col)) if nnz is None else int(nnz)
@@ -256,7 +261,8 @@ class Graph:
         pd, k2 = _ptr(outdeg, np.int32)
         h = C.c_void_p()
         lo = LayoutOptions(int(sell_max), int(chunk), int(chunk_min), int(hot_entries),
-                           (1 if batched else 0) | (2 if push else 0))
+                           (LAYOUT_BATCHED if batched else 0) | (LAYOUT_PUSH if push else 0) |
+                           (LAYOUT_BLOCKED if blocked else 0), int(block_rows), int(tile_words))
         _check(L.gpr_graph_create_ex(m, nnz, pr, pc, pd, C.byref(lo), C.byref(h)))
         self._h, self.m, self.nnz = h, m, nnz
         self.last_stats = None

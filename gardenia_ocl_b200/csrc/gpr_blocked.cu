@@ -1,0 +1,353 @@
+// Destination-blocked, source-ordered layout of the pull graph (the blocked
+// form of the sweep).
+//
+// A pull sweep gathers contrib[u] for every edge u -> v.  In CSR order the
+// sources of consecutive gathers are unrelated, so on a large power-law graph
+// nearly every gather outside the shared-memory hot prefix is its own L2
+// request (one request per edge is the bound of the exact-order kernel).
+// Here the rows with at most chunk_min in-edges (the rows the exact-order
+// kernel puts in SELL slices) are cut into blocks of R consecutive rows of
+// the relabelled order, and the edges of each block are sorted by SOURCE: a
+// warp's 32 gathers then fall on one or two 128-byte lines, and a block's
+// edges fetch each contribution line about once (RMAT scale 24, R = 12288:
+// ~0.16 sectors per edge instead of ~0.64 requests).  The sums are formed in
+// shared memory by the CTA that owns the block (gpr_pagerank.cu, k_pr_blocked).
+//
+// Storage, per block b (rows [row0, row0 + nrows)):
+//   entries  one 32-bit word per edge: (source & 0xFFFF) << 16 | (row - row0),
+//            grouped by the 65536-source segment (source >> 16) and, inside a
+//            group, by source; every group starts on a multiple of 4 words
+//            (padding words are 0xFFFFFFFF and read nothing)
+//   runs     {first word, segment << 16 | words}: at most kRunWords words of one
+//            group (one warp's unit of work)
+//   tiles    {block, first run, end run, words}: consecutive runs of one block,
+//            at most tile_slots words and kTileRuns runs (one CTA's unit), in
+//            descending size (the CTA queue hands out the heaviest first)
+//   blocks   {row0, nrows, tiles, 0}
+// Rows of heavier in-degree (chunked) and rows without in-edges keep the
+// exact-order layout's work units.
+//
+// Construction: every in-edge of a blocked row gets the key (block << 32 |
+// source) and the value (row - row0); one radix sort orders them; the group
+// starts are selected on the device and the run / tile tables (a few hundred
+// thousand entries) are cut on the host.
+#include <cub/cub.cuh>
+
+#include <algorithm>
+#include <vector>
+
+#include "gpr_internal.cuh"
+
+namespace gpr {
+
+namespace {
+
+__global__ void k_inverse(int m, const int *__restrict__ perm, int *inv) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < m) inv[perm[i]] = i;
+}
+
+// One warp per original row: the keys and values of its in-edges when its
+// new label falls in [n_long, n_nz); other edges get the key ~0 (sorted last).
+__global__ void k_block_keys(int m, const int *__restrict__ rowptr, const int *__restrict__ col,
+                             const int *__restrict__ inv, int n_long, int n_nz, int R,
+                             unsigned long long *key, unsigned *val) {
+  const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (w >= m) return;
+  const int o = (int)w;
+  const int r = inv[o];
+  const bool in = r >= n_long && r < n_nz;
+  const unsigned long long blk = in ? (unsigned long long)((r - n_long) / R) : 0ull;
+  const unsigned dl = in ? (unsigned)((r - n_long) % R) : 0u;
+  for (int e = rowptr[o] + lane; e < rowptr[o + 1]; e += 32) {
+    key[e] = in ? (blk << 32) | (unsigned)inv[col[e]] : ~0ull;
+    val[e] = dl;
+  }
+}
+
+// First index whose key is ~0 (the blocked edges precede it): one thread.
+__global__ void k_count_blocked(long long n, const unsigned long long *__restrict__ key,
+                                long long *out) {
+  long long lo = 0, hi = n;
+  while (lo < hi) {
+    const long long mid = (lo + hi) / 2;
+    if (key[mid] == ~0ull) hi = mid;
+    else lo = mid + 1;
+  }
+  *out = lo;
+}
+
+__global__ void k_group_flags(long long n, const unsigned long long *__restrict__ key,
+                              int *flag) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) flag[i] = (i == 0 || (key[i] >> 16) != (key[i - 1] >> 16)) ? 1 : 0;
+}
+
+__global__ void k_group_keys(int ng, const int *__restrict__ gstart,
+                             const unsigned long long *__restrict__ key, int *gblk, int *gseg) {
+  const int g = blockIdx.x * blockDim.x + threadIdx.x;
+  if (g < ng) {
+    const unsigned long long k = key[gstart[g]];
+    gblk[g] = (int)(k >> 32);
+    gseg[g] = (int)((k & 0xFFFFFFFFull) >> 16);
+  }
+}
+
+// Entry i of the sorted edges goes to word gpos[gid] + (i - gstart[gid]),
+// gid = (inclusive count of group starts up to i) - 1.
+__global__ void k_place(long long n, const unsigned long long *__restrict__ key,
+                        const unsigned *__restrict__ val, const int *__restrict__ gid1,
+                        const int *__restrict__ gstart, const long long *__restrict__ gpos,
+                        unsigned *entry) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int g = gid1[i] - 1;
+  const unsigned src = (unsigned)(key[i] & 0xFFFFFFFFull);
+  entry[gpos[g] + (i - gstart[g])] = ((src & 0xFFFFu) << 16) | val[i];
+}
+
+unsigned grid_of(long long n, int block = 256) {
+  const long long g = (n + block - 1) / block;
+  return (unsigned)(g < 1 ? 1 : g);
+}
+
+}  // namespace
+
+void free_blocked_layout(BlockedLayout *B) {
+  dfree(B->entry);
+  dfree(B->runs);
+  dfree(B->tiles);
+  dfree(B->blocks);
+  dfree(B->gacc);
+  dfree(B->bcnt);
+  *B = BlockedLayout();
+}
+
+int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
+                         const PrLayout &L, int R, int tile_slots, BlockedLayout *B,
+                         cudaStream_t st) {
+  *B = BlockedLayout();
+  B->R = R;
+  B->tile_slots = tile_slots;
+  const int n_rows = L.n_nz - L.n_long;
+  if (R < 1 || R > kBlockedMaxRows || tile_slots < kRunWords) {
+    set_error("blocked layout: block rows %d must be in [1, %d], tile words %d >= %d", R,
+              kBlockedMaxRows, tile_slots, kRunWords);
+    return GPR_EINVAL;
+  }
+  B->n_blocks = n_rows > 0 ? (int)ceil_div(n_rows, R) : 0;
+  if (n_rows <= 0 || nnz == 0) {
+    B->n_blocks = 0;
+    return GPR_OK;
+  }
+  // Keys and values of every edge; blocked ones first after the sort.
+  int *inv = nullptr;
+  unsigned long long *k0 = nullptr, *k1 = nullptr;
+  unsigned *v0 = nullptr, *v1 = nullptr;
+  void *tmp = nullptr;
+  int rc = GPR_OK;
+  auto fail = [&](int code) {
+    dfree(inv); dfree(k0); dfree(k1); dfree(v0); dfree(v1); dfree(tmp);
+    free_blocked_layout(B);
+    return code;
+  };
+  if ((rc = dalloc(&inv, (size_t)m + 2, "blocked: inverse")) != GPR_OK ||
+      (rc = dalloc(&k0, (size_t)nnz, "blocked: keys")) != GPR_OK ||
+      (rc = dalloc(&k1, (size_t)nnz, "blocked: keys")) != GPR_OK ||
+      (rc = dalloc(&v0, (size_t)nnz, "blocked: rows")) != GPR_OK ||
+      (rc = dalloc(&v1, (size_t)nnz, "blocked: rows")) != GPR_OK)
+    return fail(rc);
+  k_inverse<<<grid_of(m), 256, 0, st>>>(m, L.perm, inv);
+  k_block_keys<<<grid_of((long long)m * 32), 256, 0, st>>>(m, d_rowptr, d_col, inv, L.n_long,
+                                                           L.n_nz, R, k0, v0);
+  if ((rc = GPR_CUDA_RC(cudaGetLastError())) != GPR_OK) return fail(rc);
+  // Sort on (block, source): bits of the source ids, then of the block ids
+  // (the ~0 keys of the excluded edges have every bit set and sort last).
+  int blk_bits = 1;
+  while ((1LL << blk_bits) <= B->n_blocks) ++blk_bits;
+  const int end_bit = 32 + blk_bits;
+  {
+    size_t tb = 0;
+    cub::DoubleBuffer<unsigned long long> kb(k0, k1);
+    cub::DoubleBuffer<unsigned> vb(v0, v1);
+    if ((rc = GPR_CUDA_RC(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, (int)nnz, 0,
+                                                          end_bit, st))) != GPR_OK)
+      return fail(rc);
+    if ((rc = dmalloc(&tmp, tb, "blocked: sort scratch")) != GPR_OK) return fail(rc);
+    if ((rc = GPR_CUDA_RC(cub::DeviceRadixSort::SortPairs(tmp, tb, kb, vb, (int)nnz, 0, end_bit,
+                                                          st))) != GPR_OK)
+      return fail(rc);
+    dfree(tmp);
+    tmp = nullptr;
+    if (kb.Current() != k0) std::swap(k0, k1);
+    if (vb.Current() != v0) std::swap(v0, v1);
+  }
+  // Number of blocked edges: the keys before the first ~0.
+  long long n_edges = 0;
+  {
+    long long *d_n = reinterpret_cast<long long *>(inv);  // inv is no longer needed
+    k_count_blocked<<<1, 1, 0, st>>>(nnz, k0, d_n);
+    if ((rc = GPR_CUDA_RC(cudaGetLastError())) != GPR_OK ||
+        (rc = GPR_CUDA_RC(cudaMemcpyAsync(&n_edges, d_n, sizeof(n_edges), cudaMemcpyDeviceToHost,
+                                          st))) != GPR_OK ||
+        (rc = GPR_CUDA_RC(cudaStreamSynchronize(st))) != GPR_OK)
+      return fail(rc);
+  }
+  B->edges = n_edges;
+  if (n_edges == 0) {
+    dfree(inv); dfree(k0); dfree(k1); dfree(v0); dfree(v1);
+    B->n_blocks = 0;
+    return GPR_OK;
+  }
+  // Group starts (block, segment) and their keys.
+  int *flag = reinterpret_cast<int *>(k1);  // k1 is free now
+  int *gid1 = reinterpret_cast<int *>(v1);                       // so is v1
+  k_group_flags<<<grid_of(n_edges), 256, 0, st>>>(n_edges, k0, flag);
+  int *gstart = nullptr, *nsel = nullptr;
+  if ((rc = dalloc(&gstart, (size_t)n_edges, "blocked: groups")) != GPR_OK ||
+      (rc = dalloc(&nsel, 1, "blocked: group count")) != GPR_OK) {
+    dfree(gstart);
+    return fail(rc);
+  }
+  int ng = 0;
+  {
+    size_t tb = 0;
+    cub::CountingInputIterator<int> it(0);
+    rc = GPR_CUDA_RC(cub::DeviceSelect::Flagged(nullptr, tb, it, flag, gstart, nsel, (int)n_edges, st));
+    if (rc == GPR_OK) rc = dmalloc(&tmp, tb, "blocked: select scratch");
+    if (rc == GPR_OK)
+      rc = GPR_CUDA_RC(cub::DeviceSelect::Flagged(tmp, tb, it, flag, gstart, nsel, (int)n_edges, st));
+    dfree(tmp);
+    tmp = nullptr;
+    // inclusive count of group starts: the group of every entry
+    tb = 0;
+    if (rc == GPR_OK)
+      rc = GPR_CUDA_RC(cub::DeviceScan::InclusiveSum(nullptr, tb, flag, gid1, (int)n_edges, st));
+    if (rc == GPR_OK) rc = dmalloc(&tmp, tb, "blocked: scan scratch");
+    if (rc == GPR_OK)
+      rc = GPR_CUDA_RC(cub::DeviceScan::InclusiveSum(tmp, tb, flag, gid1, (int)n_edges, st));
+    dfree(tmp);
+    tmp = nullptr;
+    if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemcpyAsync(&ng, nsel, sizeof(int),
+                                                       cudaMemcpyDeviceToHost, st));
+    if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaStreamSynchronize(st));
+  }
+  dfree(nsel);
+  if (rc != GPR_OK) {
+    dfree(gstart);
+    return fail(rc);
+  }
+  std::vector<int> h_gstart(ng), h_gblk(ng), h_gseg(ng);
+  {
+    int *gblk = nullptr, *gseg = nullptr;
+    rc = dalloc(&gblk, (size_t)ng, "blocked: group blocks");
+    if (rc == GPR_OK) rc = dalloc(&gseg, (size_t)ng, "blocked: group segments");
+    if (rc == GPR_OK) {
+      k_group_keys<<<grid_of(ng), 256, 0, st>>>(ng, gstart, k0, gblk, gseg);
+      rc = GPR_CUDA_RC(cudaGetLastError());
+    }
+    if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemcpyAsync(h_gstart.data(), gstart, sizeof(int) * ng,
+                                                       cudaMemcpyDeviceToHost, st));
+    if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemcpyAsync(h_gblk.data(), gblk, sizeof(int) * ng,
+                                                       cudaMemcpyDeviceToHost, st));
+    if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemcpyAsync(h_gseg.data(), gseg, sizeof(int) * ng,
+                                                       cudaMemcpyDeviceToHost, st));
+    if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaStreamSynchronize(st));
+    dfree(gblk);
+    dfree(gseg);
+  }
+  if (rc != GPR_OK) {
+    dfree(gstart);
+    return fail(rc);
+  }
+  // Host: padded group offsets, runs, tiles, blocks.
+  std::vector<long long> gpos(ng + 1);
+  std::vector<uint2> runs;
+  std::vector<int4> tiles;
+  std::vector<int4> blocks(B->n_blocks);
+  for (int b = 0; b < B->n_blocks; ++b) {
+    const int row0 = L.n_long + b * R;
+    blocks[b] = make_int4(row0, std::min(R, L.n_nz - row0), 0, 0);
+  }
+  runs.reserve((size_t)(n_edges / kRunWords) + ng + 1);
+  long long pos = 0;
+  int g = 0;
+  while (g < ng) {
+    const int b = h_gblk[g];
+    // the groups of block b
+    int g1 = g;
+    while (g1 < ng && h_gblk[g1] == b) ++g1;
+    int tile_run0 = (int)runs.size(), tile_runs = 0;
+    long long tile_words = 0;
+    auto close_tile = [&]() {
+      if (tile_runs > 0) {
+        tiles.push_back(make_int4(b, tile_run0, (int)runs.size(), (int)tile_words));
+        blocks[b].z += 1;
+      }
+      tile_run0 = (int)runs.size();
+      tile_runs = 0;
+      tile_words = 0;
+    };
+    for (int q = g; q < g1; ++q) {
+      const long long size = (q + 1 < ng ? (long long)h_gstart[q + 1] : n_edges) - h_gstart[q];
+      const long long padded = (size + 3) / 4 * 4;
+      gpos[q] = pos;
+      for (long long off = 0; off < padded; off += kRunWords) {
+        const int len = (int)std::min<long long>(kRunWords, padded - off);
+        if (tile_runs > 0 && (tile_words + len > tile_slots || tile_runs == kTileRuns)) close_tile();
+        runs.push_back(make_uint2((unsigned)(pos + off), ((unsigned)h_gseg[q] << 16) | (unsigned)len));
+        ++tile_runs;
+        tile_words += len;
+      }
+      pos += padded;
+    }
+    close_tile();
+    g = g1;
+  }
+  gpos[ng] = pos;
+  if (pos > 0xFFFFFFF0LL) {
+    set_error("blocked layout: %lld entry words exceed 32-bit offsets", pos);
+    dfree(gstart);
+    return fail(GPR_EINVAL);
+  }
+  std::stable_sort(tiles.begin(), tiles.end(),
+                   [](const int4 &x, const int4 &y) { return x.w > y.w; });
+  B->slots = pos;
+  B->n_runs = (long long)runs.size();
+  B->n_tiles = (int)tiles.size();
+  // Device tables and the entries.
+  long long *d_gpos = nullptr;
+  rc = dalloc(&d_gpos, (size_t)ng, "blocked: group offsets");
+  if (rc == GPR_OK) rc = dalloc(&B->entry, (size_t)pos, "blocked: entries");
+  if (rc == GPR_OK) rc = dalloc(&B->runs, (size_t)B->n_runs, "blocked: runs");
+  if (rc == GPR_OK) rc = dalloc(&B->tiles, (size_t)B->n_tiles, "blocked: tiles");
+  if (rc == GPR_OK) rc = dalloc(&B->blocks, (size_t)B->n_blocks, "blocked: blocks");
+  if (rc == GPR_OK) rc = dalloc(&B->gacc, (size_t)n_rows, "blocked: cross-tile sums");
+  if (rc == GPR_OK) rc = dalloc(&B->bcnt, (size_t)B->n_blocks, "blocked: tile counters");
+  if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemcpyAsync(d_gpos, gpos.data(), sizeof(long long) * ng,
+                                                     cudaMemcpyHostToDevice, st));
+  if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemcpyAsync(B->runs, runs.data(), sizeof(uint2) * runs.size(),
+                                                     cudaMemcpyHostToDevice, st));
+  if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemcpyAsync(B->tiles, tiles.data(), sizeof(int4) * tiles.size(),
+                                                     cudaMemcpyHostToDevice, st));
+  if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemcpyAsync(B->blocks, blocks.data(), sizeof(int4) * blocks.size(),
+                                                     cudaMemcpyHostToDevice, st));
+  if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemsetAsync(B->entry, 0xFF, sizeof(unsigned) * (size_t)pos, st));
+  if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemsetAsync(B->gacc, 0, sizeof(unsigned long long) * n_rows, st));
+  if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemsetAsync(B->bcnt, 0, sizeof(int) * B->n_blocks, st));
+  if (rc == GPR_OK) {
+    k_place<<<grid_of(n_edges), 256, 0, st>>>(n_edges, k0, v0, gid1, gstart, d_gpos, B->entry);
+    rc = GPR_CUDA_RC(cudaGetLastError());
+  }
+  if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaStreamSynchronize(st));
+  dfree(d_gpos);
+  dfree(gstart);
+  if (rc != GPR_OK) return fail(rc);
+  dfree(inv); dfree(k0); dfree(k1); dfree(v0); dfree(v1);
+  B->device_bytes = 4 * pos + 8 * B->n_runs + 16LL * B->n_tiles + 16LL * B->n_blocks +
+                    8LL * n_rows + 4LL * B->n_blocks;
+  return GPR_OK;
+}
+
+}  // namespace gpr

@@ -122,6 +122,32 @@ int build_pr_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
                     bool keep_csr, PrLayout *L, cudaStream_t st, cudaEvent_t col_ready = nullptr);
 void free_pr_layout(PrLayout *L);
 
+// Destination-blocked, source-ordered layout of the rows [n_long, n_nz) of a
+// PrLayout (gpr_blocked.cu describes the storage).
+constexpr int kRunWords = 512;        // entry words of one run (a warp's unit)
+constexpr int kTileRuns = 1024;       // most runs in one tile (staged in shared memory)
+constexpr int kBlockedRows = 12288;   // rows per block (accumulators in shared memory)
+constexpr int kBlockedMaxRows = 12288;
+constexpr int kTileWordsDefault = 1 << 18;
+
+struct BlockedLayout {
+  int R = 0, tile_slots = 0;
+  int n_blocks = 0, n_tiles = 0;
+  long long n_runs = 0, slots = 0, edges = 0;
+  unsigned *entry = nullptr;             // [slots]
+  uint2 *runs = nullptr;                 // [n_runs] {first word, segment << 16 | words}
+  int4 *tiles = nullptr;                 // [n_tiles] {block, run0, run1, words}
+  int4 *blocks = nullptr;                // [n_blocks] {row0, nrows, tiles, 0}
+  unsigned long long *gacc = nullptr;    // [n_nz - n_long] sums of multi-tile blocks
+  int *bcnt = nullptr;                   // [n_blocks] tiles done in the current sweep
+  long long device_bytes = 0;
+};
+
+int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
+                         const PrLayout &L, int R, int tile_slots, BlockedLayout *B,
+                         cudaStream_t st);
+void free_blocked_layout(BlockedLayout *B);
+
 // Validates a device CSR (rowptr[0] = 0, monotone, rowptr[m] = nnz, every
 // column in [0, ncols) when d_col is given) and, when d_outdeg is given,
 // out-degrees >= 0.  validate_cols checks the columns alone.
@@ -236,6 +262,13 @@ struct gpr_graph {
   cudaGraph_t loop_graph = nullptr;
   cudaGraphExec_t loop_exec = nullptr;
   int loop_ki = -1;
+  // Blocked form (GPR_LAYOUT_BLOCKED): its layout, the persistent kernel's
+  // grid and co-residency, the tile-queue heads and the largest |score|.
+  gpr::BlockedLayout B;
+  bool has_blocked = false, blocked_ok = false;
+  int grid_blocked = 0;
+  int *tq = nullptr;
+  unsigned *fx_max = nullptr;
   alignas(8) unsigned char loop_args[512] = {0};
 };
 

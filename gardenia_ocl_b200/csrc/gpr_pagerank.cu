@@ -34,6 +34,8 @@
 #include "gpr_guard.h"
 
 using gpr::PrLayout;
+using gpr::kBlockedMaxRows;
+using gpr::kTileRuns;
 
 namespace {
 
@@ -63,6 +65,17 @@ struct PrArgs {
   int *wq;                // [2] work-queue heads of the hot kernel, by sweep parity
   int batch;              // units per work-queue grab
   unsigned long long cond;  // graph mode: while-node condition handle (0: none)
+  // blocked form (gpr_blocked.cu): tiles of source-ordered entries per block
+  int n_tiles;
+  const int4 *tiles;
+  const int4 *blocks;
+  const uint2 *runs;
+  const unsigned *entry;
+  unsigned long long *gacc;
+  int *bcnt;
+  int *tq;                // [2] tile-queue heads by sweep parity
+  float fx_scale;         // 2^S: contributions as 64-bit fixed point
+  double fx_inv;          // 2^-S
 };
 
 using namespace gpr::dev;
@@ -248,6 +261,7 @@ __device__ bool barrier_reduce(const PrArgs &a, int it, double cta_total) {
       if (threadIdx.x == 0) {
         a.err_hist[it] = t;
         if (a.wq) atomicExch(a.wq + (it & 1), 0);  // reused by sweep it + 2
+        if (a.tq) atomicExch(a.tq + (it & 1), 0);
         atomicExch(a.bar, 0u);
         __threadfence();
         atomicAdd(a.bar + 1, 1u);
@@ -325,6 +339,252 @@ __global__ void __launch_bounds__(1024, MINB) k_pr_hot(PrArgs a) {
     a.status[1] = it;
     a.status[2] = 1;
   }
+}
+
+// ---- blocked form -----------------------------------------------------------
+// Rows [n_long, n_nz) are summed block by block (gpr_blocked.cu): the CTA that
+// takes a tile zeroes one accumulator per row of the tile's block in shared
+// memory, its warps take the tile's runs (source-ordered entries, so a warp's
+// gathers share lines) and add each contribution to its row's accumulator.
+// The accumulators are 64-bit fixed point, value * 2^S, held as two 32-bit
+// words: the low word is added with an atomic that returns the old word, so
+// its carry is exact, and the high word gets the contribution's high bits
+// plus the carry (most contributions fit the low word).  Integer addition is
+// associative, so every row's sum is the same whatever the order in which
+// warps and tiles add: results do not change from run to run, and each sum is
+// the exact sum of the FP32 contributions rounded once to 2^-S.  The sum is
+// rounded to FP32 and the update uses the reference's float operations
+// (src/pr/omp_base.cc:39, 26).  A block cut into several tiles adds its
+// tiles' sums into a 64-bit global accumulator per row; the CTA that
+// completes the block's last tile finalizes it and clears the accumulators.
+__device__ __forceinline__ void use_u32(unsigned x) { asm volatile("" ::"r"(x)); }
+__device__ __forceinline__ void use_f32(float x) { asm volatile("" ::"f"(x)); }
+
+// Four entries of a run; lanes past the run's end read padding words.
+__device__ __forceinline__ uint4 ld_entry4(const unsigned *p, bool pred, uint64_t pol) {
+  uint4 v = make_uint4(0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu);
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " @p ld.global.nc.L1::no_allocate.L2::cache_hint.v4.u32 {%0,%1,%2,%3}, [%5], %6;\n}"
+      : "+r"(v.x), "+r"(v.y), "+r"(v.z), "+r"(v.w)
+      : "r"((int)pred), "l"(p), "l"(pol));
+  return v;
+}
+
+// Contribution of an entry's source (segment base | low 16 bits); padding
+// entries read nothing and give 0.
+__device__ __forceinline__ float gather_entry(const float *cin, unsigned segbase, unsigned w,
+                                              uint64_t pol) {
+  float v = 0.f;
+  const float *p = cin + (segbase | (w >> 16));
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.u32 p, %1, 0xFFFFFFFF;\n"
+      " @p ld.global.L2::cache_hint.f32 %0, [%2], %3;\n}"
+      : "+f"(v)
+      : "r"(w), "l"(p), "l"(pol));
+  return v;
+}
+
+// Rows row0 + i, i < nrows, from their fixed-point sums (shared accumulators
+// or, when `global`, the cross-tile accumulators, which are cleared); eight
+// rows per thread are loaded before any is updated.
+__device__ __forceinline__ double blocked_finalize(const PrArgs &a, float *cout, int row0,
+                                                   int nrows, const unsigned *acc, bool global,
+                                                   const Policies &pol) {
+  double err = 0.0;
+  for (int i0 = threadIdx.x; i0 < nrows; i0 += 8 * 1024) {
+    long long x[8];
+    float so[8];
+    int od[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int i = i0 + 1024 * k;
+      x[k] = 0;
+      so[k] = 0.f;
+      od[k] = 1;
+      if (i < nrows) {
+        const int r = row0 + i;
+        x[k] = global ? (long long)__ldcg(a.gacc + (r - a.n_long))
+                      : (long long)(((unsigned long long)acc[kBlockedMaxRows + i] << 32) | acc[i]);
+        so[k] = ld_f32_stream(a.s + r, pol.stream);
+        od[k] = ld_s32_stream(a.outdeg + r, pol.stream);
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+      const int i = i0 + 1024 * k;
+      if (i < nrows) {
+        const int r = row0 + i;
+        if (global) a.gacc[r - a.n_long] = 0ull;
+        const float sum = (float)((double)x[k] * a.fx_inv);
+        err += row_update(a, r, sum, so[k], od[k], cout, pol);
+      }
+    }
+  }
+  return err;
+}
+
+// One tile: zero the block's accumulators, add the tile's runs, then finalize
+// the block (single tile) or add into the cross-tile accumulators.
+template <int PV>
+__device__ __forceinline__ double blocked_tile(const PrArgs &a, const float *cin, float *cout,
+                                               int t, unsigned *acc, uint2 *s_runs, int *s_next,
+                                               int *s_last, const Policies &pol) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int4 td = a.tiles[t];
+  const int4 bd = a.blocks[td.x];
+  const int nr = td.z - td.y;
+  for (int i = threadIdx.x; i < nr; i += 1024) s_runs[i] = a.runs[td.y + i];
+  for (int i = threadIdx.x; i < bd.y; i += 1024) {
+    acc[i] = 0u;
+    acc[kBlockedMaxRows + i] = 0u;
+  }
+  if (threadIdx.x == 0) *s_next = 32;
+  __syncthreads();
+  int r = warp;
+  while (r < nr) {
+    const uint2 rd = s_runs[r];
+    int rn = 0;
+    if (lane == 0) rn = atomicAdd(s_next, 1);
+    const unsigned segbase = (rd.y >> 16) << 16;
+    const int len = (int)(rd.y & 0xFFFFu);
+    // all index loads of the run, then all gathers, then the additions
+    uint4 q[PV];
+#pragma unroll
+    for (int i = 0; i < PV; ++i)
+      q[i] = ld_entry4(a.entry + rd.x + 128 * i + 4 * lane, 128 * i + 4 * lane < len, pol.stream);
+#pragma unroll
+    for (int i = 0; i < PV; ++i) {
+      use_u32(q[i].x); use_u32(q[i].y); use_u32(q[i].z); use_u32(q[i].w);
+    }
+    float v[4 * PV];
+#pragma unroll
+    for (int i = 0; i < PV; ++i) {
+      v[4 * i + 0] = gather_entry(cin, segbase, q[i].x, pol.keep);
+      v[4 * i + 1] = gather_entry(cin, segbase, q[i].y, pol.keep);
+      v[4 * i + 2] = gather_entry(cin, segbase, q[i].z, pol.keep);
+      v[4 * i + 3] = gather_entry(cin, segbase, q[i].w, pol.keep);
+    }
+#pragma unroll
+    for (int i = 0; i < 4 * PV; ++i) use_f32(v[i]);
+    unsigned wv[4 * PV];
+#pragma unroll
+    for (int i = 0; i < PV; ++i) {
+      wv[4 * i + 0] = q[i].x; wv[4 * i + 1] = q[i].y; wv[4 * i + 2] = q[i].z; wv[4 * i + 3] = q[i].w;
+    }
+#pragma unroll
+    for (int h = 0; h < 4 * PV; h += 8) {
+      unsigned lo[8], hw[8], old[8];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const long long x = __float2ll_rn(v[h + i] * a.fx_scale);
+        lo[i] = (unsigned)x;
+        hw[i] = (unsigned)((unsigned long long)x >> 32);
+        old[i] = 0u;
+        if (wv[h + i] != 0xFFFFFFFFu) old[i] = atomicAdd(acc + (wv[h + i] & 0xFFFFu), lo[i]);
+      }
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const unsigned hc = hw[i] + (old[i] + lo[i] < old[i] ? 1u : 0u);
+        if (wv[h + i] != 0xFFFFFFFFu && hc) atomicAdd(acc + kBlockedMaxRows + (wv[h + i] & 0xFFFFu), hc);
+      }
+    }
+    r = __shfl_sync(kFull, rn, 0);
+  }
+  __syncthreads();
+  double err = 0.0;
+  if (bd.z == 1) {
+    err = blocked_finalize(a, cout, bd.x, bd.y, acc, false, pol);
+  } else {
+    for (int i = threadIdx.x; i < bd.y; i += 1024) {
+      const unsigned long long x = ((unsigned long long)acc[kBlockedMaxRows + i] << 32) | acc[i];
+      if (x) atomicAdd(a.gacc + (bd.x - a.n_long) + i, x);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      __threadfence();
+      *s_last = atomicAdd(a.bcnt + td.x, 1) == bd.z - 1;
+    }
+    __syncthreads();
+    if (*s_last) {
+      __threadfence();
+      err = blocked_finalize(a, cout, bd.x, bd.y, acc, true, pol);
+      if (threadIdx.x == 0) a.bcnt[td.x] = 0;
+    }
+  }
+  return err;
+}
+
+// All sweeps of the blocked form in one cooperative launch, one 1024-thread
+// CTA per SM.  Per sweep: CTAs take tiles from a queue (heaviest first; the
+// next tile is claimed while the current one runs), then warps take the
+// chunks of the rows above chunk_min in-edges, with the first contributions
+// staged in the shared memory the accumulators used, then the zero-in-degree
+// rows (sweeps 0 and 1), then the bounded grid barrier with the residual.
+template <int PV>
+__global__ void __launch_bounds__(1024, 1) k_pr_blocked(PrArgs a) {
+  extern __shared__ unsigned s_acc[];  // [2 * kBlockedMaxRows]: low / high words
+  __shared__ uint2 s_runs[kTileRuns];
+  __shared__ int s_tile, s_next_tile, s_last, s_next;
+  const int lane = threadIdx.x & 31;
+  const long long gw = (long long)blockIdx.x * 32 + (threadIdx.x >> 5);
+  const long long nw = (long long)gridDim.x * 32;
+  const Policies pol = make_policies();
+  int it = 0;
+  while (it < a.max_iter) {
+    const float *cin = static_cast<const float *>((it & 1) ? a.c1 : a.c0);
+    float *cout = static_cast<float *>((it & 1) ? a.c0 : a.c1);
+    double err = 0.0;
+    if (threadIdx.x == 0) s_next_tile = atomicAdd(a.tq + (it & 1), 1);
+    for (;;) {
+      __syncthreads();
+      if (threadIdx.x == 0) s_tile = s_next_tile;
+      __syncthreads();
+      const int t = s_tile;
+      if (t >= a.n_tiles) break;
+      if (threadIdx.x == 0) s_next_tile = atomicAdd(a.tq + (it & 1), 1);
+      err += blocked_tile<PV>(a, cin, cout, t, s_acc, s_runs, &s_next, &s_last, pol);
+    }
+    // chunks of the long rows, the hottest contributions from shared memory
+    float *s_hot = reinterpret_cast<float *>(s_acc);
+    const int n16 = a.hot / 4;
+    const float4 *src = reinterpret_cast<const float4 *>(cin);
+    for (int i = threadIdx.x; i < n16; i += blockDim.x)
+      reinterpret_cast<float4 *>(s_hot)[i] = ld_contrib4(src + i, pol.keep);
+    __syncthreads();
+    const HotGatherGeneric<float> gat{cin, s_hot, a.hot, pol.keep};
+    for (;;) {
+      int u0 = 0;
+      if (lane == 0) u0 = atomicAdd(a.wq + (it & 1), a.batch);
+      u0 = __shfl_sync(kFull, u0, 0);
+      if (u0 >= a.n_chunks) break;
+      const int u1 = min(u0 + a.batch, a.n_chunks);
+      for (int u = u0; u < u1; ++u) err += do_chunk<4>(a, gat, cout, u, lane, pol);
+    }
+    if (it < 2)
+      for (long long z = gw; z < a.n_zblk; z += nw) err += do_zero(a, cout, (int)z, lane, it, pol);
+    const double tot = block_sum(err);
+    if (!barrier_reduce(a, it, tot)) return;
+    const double total = __ldcg(a.err_hist + it);
+    ++it;
+    if (total < a.tol) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.status[1] = it;
+    a.status[2] = 1;
+  }
+}
+
+// Largest |score| (bits of a non-negative float order like the float; a NaN
+// sorts above every finite value and infinity).
+__global__ void k_max_abs(int m, const float *__restrict__ s, unsigned *out) {
+  unsigned mx = 0u;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
+       i += (long long)gridDim.x * blockDim.x)
+    mx = max(mx, __float_as_uint(s[i]) & 0x7FFFFFFFu);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
 }
 
 // One sweep per launch (graph mode).  The sweep index and the done flag live
@@ -583,6 +843,9 @@ void destroy(gpr_graph *g) {
   gpr::dfree(g->push_src);
   gpr::dfree(g->push_dst);
   gpr::dfree(g->push_sum);
+  gpr::free_blocked_layout(&g->B);
+  gpr::dfree(g->tq);
+  gpr::dfree(g->fx_max);
   if (g->e0) cudaEventDestroy(g->e0);
   if (g->e1) cudaEventDestroy(g->e1);
   if (g->e2) cudaEventDestroy(g->e2);
@@ -593,7 +856,7 @@ void destroy(gpr_graph *g) {
 
 int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
                 const int *any_outdeg, int lane_max, int chunk_min, int chunk, int hot_max,
-                bool keep_csr, gpr_graph *g) {
+                bool keep_csr, bool blocked, int block_rows, int tile_words, gpr_graph *g) {
   GPR_CUDA(cudaGetDevice(&g->device));
   GPR_CUDA(cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking));
   g->own_stream = true;
@@ -652,6 +915,11 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
     if (ev_rows) cudaEventDestroy(ev_rows);
     if (ev_col) cudaEventDestroy(ev_col);
   }
+  if (rc == GPR_OK && blocked) {
+    rc = gpr::build_blocked_layout(m, nnz, (const int *)rp, (const int *)cp, g->L, block_rows,
+                                   tile_words, &g->B, st);
+    g->has_blocked = rc == GPR_OK;
+  }
   if (orp) gpr::dfree(rp);
   if (ocp) gpr::dfree(cp);
   if (odp) gpr::dfree(dp);
@@ -700,6 +968,21 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
   g->grid_step = (int)step;
   g->max_grid = g->grid_step;
   for (int v = 0; v < kNumKernels; ++v) g->max_grid = std::max(g->max_grid, g->grid_hot[v]);
+  if (g->has_blocked) {
+    // one 1024-thread CTA per SM; shared memory: the accumulators (dynamic)
+    // and the tile's run table (static)
+    const int smem = 8 * gpr::kBlockedMaxRows;
+    int per_sm = 0;
+    GPR_CUDA(cudaFuncSetAttribute((const void *)k_pr_blocked<4>,
+                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_pr_blocked<4>,
+                                                           1024, smem));
+    g->blocked_ok = g->coop && per_sm >= 1;
+    g->grid_blocked = sms;
+    g->max_grid = std::max(g->max_grid, g->grid_blocked);
+    GPR_TRY(gpr::dalloc(&g->tq, 2, "tile queue"));
+    GPR_TRY(gpr::dalloc(&g->fx_max, 1, "largest score"));
+  }
   GPR_TRY(gpr::dalloc(&g->cta_err, 2 * (size_t)g->max_grid, "cta residuals"));
   g->err_cap = 128;
   GPR_TRY(gpr::dalloc(&g->err_hist, (size_t)g->err_cap, "residual history"));
@@ -754,9 +1037,28 @@ int graph_loop(gpr_graph *g, const PrArgs &a, int ki, cudaStream_t st) {
   return GPR_OK;
 }
 
-// One solve with sweep kernel ki from the scores in d_scores (device, vertex
-// order); the result is written back to d_scores.
-int solve_impl(gpr_graph *g, float *d_scores, const gpr_pr_opts &o, int ki, gpr_pr_stats *out) {
+// solve_impl status: the blocked form cannot represent these scores (a
+// non-finite score); the caller solves with the exact-order form instead.
+constexpr int kBlockedFallback = 100;
+
+// Fixed-point exponent S of the blocked form for a solve from scores whose
+// largest magnitude is mx.  Every sweep's total |score| is at most
+// B0 = max(1, m * mx) (a sweep maps total mass M to at most (1-d) + d*M), and
+// a row's sum is at most that, so |sum| * 2^S < 2^63 needs S <= 62 - log2(B0).
+// Within that, S puts a typical contribution (about B0 / nnz) near 2^28, so
+// most fit the low 32-bit word of the accumulator; S >= 31 unless B0 > 2^31.
+int blocked_shift(int m, long long nnz, float mx) {
+  const double b0 = std::max(1.0, (double)m * (double)mx);
+  const int cap = 62 - (int)ceil(log2(b0));
+  const int pref = (int)floor(log2(std::max(1.0, (double)nnz) / b0)) + 28;
+  return std::min(cap, std::max(31, pref));
+}
+
+// One solve with sweep kernel ki (or, when `blocked`, the blocked form) from
+// the scores in d_scores (device, vertex order); the result is written back
+// to d_scores.
+int solve_impl(gpr_graph *g, float *d_scores, const gpr_pr_opts &o, int ki, gpr_pr_stats *out,
+               bool blocked = false) {
   const int m = g->L.m;
   cudaStream_t st = g->st;
   if (kKernels[ki].elem == 2 && !g->h0) {
@@ -770,7 +1072,31 @@ int solve_impl(gpr_graph *g, float *d_scores, const gpr_pr_opts &o, int ki, gpr_
   GPR_CUDA(cudaMemsetAsync(g->status, 0, 4 * sizeof(int), st));
   GPR_CUDA(cudaMemsetAsync(g->wq, 0, 2 * sizeof(int), st));
   if (g->L.n_long) GPR_CUDA(cudaMemsetAsync(g->cnt, 0, sizeof(int) * g->L.n_long, st));
+  const gpr::BlockedLayout &B = g->B;
+  if (blocked) {
+    GPR_CUDA(cudaMemsetAsync(g->tq, 0, 2 * sizeof(int), st));
+    GPR_CUDA(cudaMemsetAsync(g->fx_max, 0, sizeof(unsigned), st));
+    if (B.n_blocks) {
+      // clean after an abandoned solve; a completed sweep leaves them clean
+      GPR_CUDA(cudaMemsetAsync(B.bcnt, 0, sizeof(int) * B.n_blocks, st));
+      GPR_CUDA(cudaMemsetAsync(B.gacc, 0, 8 * (size_t)(g->L.n_nz - g->L.n_long), st));
+    }
+  }
   PrArgs a = make_args(g, o, ki);
+  if (blocked) {
+    a.n_tiles = B.n_tiles;
+    a.tiles = B.tiles;
+    a.blocks = B.blocks;
+    a.runs = B.runs;
+    a.entry = B.entry;
+    a.gacc = B.gacc;
+    a.bcnt = B.bcnt;
+    a.tq = g->tq;
+    a.bar_expect = g->grid_blocked;
+    a.hot = std::min(hot_entries(g, 0), 2 * gpr::kBlockedMaxRows) / 4 * 4;
+    a.batch = (int)std::max<long long>(
+        1, (long long)g->L.n_chunks / ((long long)g->grid_blocked * 32 * 4));
+  }
   if (o.reserved[0] > 0) a.bar_expect += o.reserved[0];  // test hook: a barrier nobody completes
   int launches = 0;
   bool graph_mode = false;
@@ -783,11 +1109,39 @@ int solve_impl(gpr_graph *g, float *d_scores, const gpr_pr_opts &o, int ki, gpr_
     k_pr_prologue<float><<<grid_for((long long)m + 1), 256, 0, st>>>(
         m, g->L.perm, g->L.outdeg, d_scores, g->s, g->c0, g->c1);
   ++launches;
+  if (blocked) {
+    k_max_abs<<<std::min<unsigned>(grid_for(m), 148 * 8), 256, 0, st>>>(m, g->s, g->fx_max);
+    ++launches;
+    GPR_CUDA(cudaGetLastError());
+    unsigned bits = 0;
+    GPR_CUDA(cudaMemcpyAsync(&bits, g->fx_max, sizeof(bits), cudaMemcpyDeviceToHost, st));
+    GPR_CUDA(cudaStreamSynchronize(st));
+    float mx;
+    memcpy(&mx, &bits, sizeof(mx));
+    if (!isfinite(mx)) return kBlockedFallback;
+    const int S = blocked_shift(m, g->L.nnz, mx);
+    a.fx_scale = ldexpf(1.f, S);
+    a.fx_inv = ldexp(1.0, -S);
+  }
   int loop = o.loop;
   if (loop == GPR_LOOP_AUTO) loop = GPR_LOOP_PERSISTENT;
   if (loop == GPR_LOOP_PERSISTENT && !g->hot_ok) loop = GPR_LOOP_GRAPH;
   GPR_CUDA(cudaEventRecord(g->e2, st));
-  if (o.max_iter > 0) {
+  if (o.max_iter > 0 && blocked) {
+    void *args[] = {&a};
+    cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_pr_blocked<4>,
+                                                dim3(g->grid_blocked), dim3(1024), args,
+                                                8 * (size_t)gpr::kBlockedMaxRows, st);
+    if (e == cudaErrorCooperativeLaunchTooLarge) {
+      cudaGetLastError();
+      return kBlockedFallback;
+    }
+    if (e != cudaSuccess) {
+      gpr::set_error("cooperative launch: %s", cudaGetErrorString(e));
+      return GPR_ECUDA;
+    }
+    ++launches;
+  } else if (o.max_iter > 0) {
     if (loop == GPR_LOOP_PERSISTENT) {
       void *args[] = {&a};
       cudaError_t e = cudaLaunchCooperativeKernel(kKernels[ki].persistent, dim3(g->grid_hot[ki]),
@@ -841,10 +1195,24 @@ int pagerank_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts_in,
   if (opts_in) o = *opts_in;
   else gpr_pr_opts_default(&o);
   if (!(o.damping >= 0.f && o.damping <= 1.f) || o.max_iter < 0 || !(o.tol >= 0.0) ||
-      !(o.timeout_s > 0.0) || o.variant < 0 || o.variant >= kNumVariants) {
+      !(o.timeout_s > 0.0) || o.variant < 0 || o.variant >= kNumVariants ||
+      o.form < GPR_FORM_AUTO || o.form > GPR_FORM_BLOCKED) {
     gpr::set_error("gpr_pagerank: invalid options (damping %g, tol %g, max_iter %d, timeout %g, "
-                   "variant %d)", (double)o.damping, o.tol, o.max_iter, o.timeout_s, o.variant);
+                   "variant %d, form %d)", (double)o.damping, o.tol, o.max_iter, o.timeout_s,
+                   o.variant, o.form);
     return GPR_EINVAL;
+  }
+  if (o.form == GPR_FORM_BLOCKED) {
+    if (!g->has_blocked) {
+      gpr::set_error("gpr_pagerank: GPR_FORM_BLOCKED on a graph created without "
+                     "GPR_LAYOUT_BLOCKED");
+      return GPR_EINVAL;
+    }
+    if (o.precision != GPR_PREC_FP32 || o.loop == GPR_LOOP_GRAPH || !g->blocked_ok) {
+      gpr::set_error("gpr_pagerank: GPR_FORM_BLOCKED needs GPR_PREC_FP32 and the persistent "
+                     "loop (cooperative launch of one CTA per SM)");
+      return GPR_EUNSUPPORTED;
+    }
   }
   if (o.precision != GPR_PREC_FP32 && o.precision != GPR_PREC_BF16) {
     gpr::set_error("gpr_pagerank: precision %d not supported (GPR_PREC_FP32 or GPR_PREC_BF16)",
@@ -881,7 +1249,21 @@ int pagerank_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts_in,
                              cudaMemcpyHostToDevice, st));
   }
   int rc = GPR_OK;
-  if (o.precision == GPR_PREC_FP32) {
+  const bool use_blocked =
+      o.precision == GPR_PREC_FP32 && g->has_blocked && g->blocked_ok &&
+      o.loop != GPR_LOOP_GRAPH && o.form != GPR_FORM_EXACT;
+  if (use_blocked) {
+    rc = solve_impl(g, d_scores, o, 0, &st_local, true);
+    if (rc == kBlockedFallback) {
+      if (o.form == GPR_FORM_BLOCKED) {
+        gpr::set_error("gpr_pagerank: GPR_FORM_BLOCKED needs finite scores and a "
+                       "co-resident grid");
+        rc = GPR_EINVAL;
+      } else {
+        rc = solve_impl(g, d_scores, o, o.variant, &st_local);
+      }
+    }
+  } else if (o.precision == GPR_PREC_FP32) {
     rc = solve_impl(g, d_scores, o, o.variant, &st_local);
   } else {
     // Mixed form: BF16 contributions (twice the entries in the shared-memory
@@ -928,10 +1310,15 @@ int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr, const int *
   if (lopts && lopts->chunk) chunk = lopts->chunk;
   if (lopts && lopts->chunk_min) chunk_min = lopts->chunk_min;
   if (lopts && lopts->hot_entries) hot_max = lopts->hot_entries;
+  int block_rows = gpr::kBlockedRows, tile_words = gpr::kTileWordsDefault;
+  if (lopts && lopts->block_rows) block_rows = lopts->block_rows;
+  if (lopts && lopts->tile_words) tile_words = lopts->tile_words;
   if (lane_max < 1 || lane_max > 1024 || chunk < 128 || chunk % 128 != 0 || chunk_min < 1 ||
-      hot_max < 4 || hot_max > gpr::kHotMax || hot_max % 4 != 0) {
+      hot_max < 4 || hot_max > gpr::kHotMax || hot_max % 4 != 0 || block_rows < 1 ||
+      block_rows > gpr::kBlockedMaxRows || tile_words < gpr::kRunWords) {
     gpr::set_error("gpr_graph_create_ex: invalid layout options (lane_max %d, chunk %d, "
-                   "chunk_min %d, hot_entries %d)", lane_max, chunk, chunk_min, hot_max);
+                   "chunk_min %d, hot_entries %d, block_rows %d, tile_words %d)", lane_max, chunk,
+                   chunk_min, hot_max, block_rows, tile_words);
     return GPR_EINVAL;
   }
   if (!out) {
@@ -952,8 +1339,9 @@ int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr, const int *
   }
   gpr_graph *g = new gpr_graph();
   const bool keep_csr = lopts && (lopts->flags & (GPR_LAYOUT_BATCHED | GPR_LAYOUT_PUSH));
+  const bool blocked = lopts && (lopts->flags & GPR_LAYOUT_BLOCKED);
   int rc = create_impl(m, nnz, any_rowptr, any_col, any_outdeg, lane_max, chunk_min, chunk,
-                       hot_max, keep_csr, g);
+                       hot_max, keep_csr, blocked, block_rows, tile_words, g);
   if (rc != GPR_OK) {
     destroy(g);
     return rc;

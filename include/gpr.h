@@ -65,10 +65,32 @@ typedef struct {
   double timeout_s;     /* bound on every device-side wait (grid barrier); default 5 s */
   int refine_max;       /* mixed precision: max FP32 refinement sweeps (default 64) */
   int variant;          /* sweep-kernel variant, 0..7 (0 = default; the autotuner's choices) */
-  int reserved[7];      /* reserved[0] > 0: the grid barrier also waits for that many CTAs
+  int reserved[1];      /* reserved[0] > 0: the grid barrier also waits for that many CTAs
                            that do not exist, so its bounded wait runs out (tests of the
                            GPR_ETIMEOUT path); keep 0 otherwise */
+  int form;             /* gpr_form: which sweep sums the rows (FP32 solves of gpr_pagerank) */
+  int pad[5];           /* keep 0 */
 } gpr_pr_opts;
+
+/* Sweep forms of gpr_pagerank (FP32).  Both compute the reference's
+ * recurrence (src/pr/omp_base.cc:23-44) and meet its parity bar (1e-6 per
+ * vertex, sweep count within one); they differ in the order of each row's sum.
+ *   EXACT    rows of <= 64 in-edges add their contributions one by one in CSR
+ *            order with rounded float adds, as the reference does: such rows
+ *            are bit-identical to the reference's.
+ *   BLOCKED  rows of <= chunk_min in-edges are summed block by block from
+ *            source-ordered edges (far fewer memory requests on large graphs),
+ *            in 64-bit fixed point: the exact sum of the FP32 contributions
+ *            rounded once to 2^-S (S >= 31, chosen per solve from the edge
+ *            count and the largest score), then to FP32.  Deterministic.  Needs
+ *            a graph created with GPR_LAYOUT_BLOCKED and the persistent loop.
+ *   AUTO     BLOCKED when the graph has its layout and the persistent loop
+ *            runs, else EXACT. */
+typedef enum {
+  GPR_FORM_AUTO = 0,
+  GPR_FORM_EXACT = 1,
+  GPR_FORM_BLOCKED = 2
+} gpr_form;
 
 typedef struct {
   int iterations;       /* sweeps executed (the reference prints the same number, gather.cu:83);
@@ -102,7 +124,9 @@ int gpr_graph_create(int m, long long nnz, const int *any_rowptr,
 /* Layout knobs (the autotuner's search space); zero fields take defaults. */
 enum {
   GPR_LAYOUT_BATCHED = 1, /* also keep a relabelled CSR: needed by gpr_ppr */
-  GPR_LAYOUT_PUSH = 2     /* also keep it for gpr_pagerank_push */
+  GPR_LAYOUT_PUSH = 2,    /* also keep it for gpr_pagerank_push */
+  GPR_LAYOUT_BLOCKED = 4  /* also build the blocked form's layout (one radix sort of the
+                             edges at creation; ~4 bytes per edge more on the device) */
 };
 typedef struct {
   int sell_max;   /* max edges per lane in a SELL slice: rows of in-degree <= sell_max get
@@ -112,7 +136,9 @@ typedef struct {
   int hot_entries;/* contributions of the highest in-degree vertices kept in shared memory
                      by the persistent kernel, multiple of 4, <= 56832 (default 32768) */
   int flags;      /* GPR_LAYOUT_* bits */
-  int reserved[3];
+  int block_rows; /* blocked form: rows per block, <= 12288 (default 12288) */
+  int tile_words; /* blocked form: most entry words per tile, >= 512 (default 262144) */
+  int reserved[1];
 } gpr_layout_opts;
 int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr,
                         const int *any_col, const int *any_outdeg,
