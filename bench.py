@@ -51,6 +51,11 @@ def pr_bytes_per_sweep(m, nnz):
     return 4 * nnz + 28 * m + 4
 
 
+# Random 4-byte gathers served by L2 on one B200, whole GPU (requests/s):
+# profiles/gather_rates.md, 289-296 G/s for L2-resident working sets.
+L2_GATHER_RATE = 290e9
+
+
 def spmv_bytes(m, nnz):
     """Aj + Ax (8 nnz) + row offsets (4 (m+1)) + x once (4 m) + y read/write (8 m)."""
     return 8 * nnz + 16 * m + 4
@@ -253,15 +258,19 @@ def run_ours(args):
     m, nnz = csr.m, csr.nnz
     # The project autotuner picks the bins, hot prefix and kernel variant for
     # this degree distribution (timed on the graph, outside the timed region).
+    # It also decides between the exact-order layout and the blocked one.
     tuned = None
-    layout = {}
+    layout = {"blocked": True}  # untuned: the blocked form
     variant = 0
     if not args.no_tune:
         tuned = G.tune_graph(csr.rowptr, csr.col, csr.third, m=m, nnz=nnz, cache=args.tune_cache,
                              sweeps=5)
-        layout = {k: tuned[k] for k in ("sell_max", "chunk", "chunk_min", "hot_entries")}
+        layout = {k: tuned[k] for k in ("sell_max", "chunk", "chunk_min", "hot_entries",
+                                        "blocked", "block_rows", "tile_words")}
         variant = tuned["variant"]
         log(f"[ours] tuned: {tuned}")
+    blocked = bool(layout.get("blocked"))
+    kernel = "k_pr_blocked" if blocked else "k_pr_hot"
     g = G.Graph(csr.rowptr, csr.col, csr.third, m=m, nnz=nnz, batched=not args.no_forms,
                 **layout)
     g.set_stream(stream.cuda_stream)
@@ -308,14 +317,23 @@ def run_ours(args):
     alg_bytes = per_sweep * sweeps_per_solve
     peak, peak_kind = load_peaks()
     achieved = alg_bytes / (loop_ms / 1e3) / 1e9
-    traffic = load_traffic().get(f"k_pr_hot_rmat{args.scale}")
-    roof = {"kernel": "k_pr_hot (persistent: all sweeps of one solve)", "bound": "hbm",
+    traffic = load_traffic().get(f"{kernel}_rmat{args.scale}")
+    roof = {"kernel": f"{kernel} (persistent: all sweeps of one solve)", "bound": "hbm",
             "achieved": achieved, "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
             "frac": achieved / peak,
             "traffic": (traffic["bytes_per_sweep"] * sweeps_per_solve) if traffic else None,
             "algorithmic_bytes_per_launch": alg_bytes,
             "bytes_per_sweep_formula": "4*nnz + 28*m + 4",
             "launch_ms": loop_ms}
+    if traffic and traffic.get("l2_requests_per_sweep"):
+        # The second ceiling of a gather: L1->L2 requests (one per scattered
+        # sector) at the measured random-gather rate of profiles/gather_rates.md.
+        req = traffic["l2_requests_per_sweep"]
+        rate = req * sweeps_per_solve / (loop_ms / 1e3)
+        roof["l2_requests"] = {"requests_per_sweep": req, "achieved": rate,
+                               "peak": L2_GATHER_RATE, "unit": "requests/s",
+                               "frac": rate / L2_GATHER_RATE,
+                               "source": traffic.get("source", "")}
     resid = g.residual_f64(scores, DAMPING)
     accuracy = {"fp64_residual_l1": resid,
                 "l1_error_bound_vs_fixed_point": resid / (1.0 - float(DAMPING)),
@@ -326,13 +344,27 @@ def run_ours(args):
                                            "solver's result", "iterations": fp_it,
                                     "last_l1_change": fp_delta}
 
+    # The same solve in the exact-order form (rows of <= 64 in-edges summed in
+    # the reference's order) on the same graph, for comparison.
+    exact = None
+    for _ in range(3):
+        scores.fill_(init)
+        _, st = g.pagerank(scores, G.options(tol=TOL, max_iter=MAX_ITER, damping=DAMPING,
+                                             variant=variant if not blocked else 0,
+                                             form=G.FORM_EXACT))
+        if exact is None or st.loop_ms < exact.loop_ms:
+            exact = st
+    exact_order = {"kernel": "k_pr_hot", "sweeps": exact.iterations, "loop_ms": exact.loop_ms,
+                   "gteps": nnz * exact.iterations / (exact.loop_ms / 1e3) / 1e9,
+                   "hbm_frac": per_sweep * exact.iterations / (exact.loop_ms / 1e3) / 1e9 / peak}
+
     line = {"metric": "pagerank_gteps_rmat24", "value": gteps, "unit": "GTEPS", "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded RMAT generated on the GPU)",
             "config": workload_config(args.scale, m, nnz), "roofline": roof,
             "gpu_launches": launches, "clocks": clocks, "accuracy": accuracy,
-            "tuning": tuned}
+            "tuning": tuned, "form": "blocked" if blocked else "exact", "exact_order": exact_order}
 
     # End to end through the reference-shaped C-ABI call with host buffers:
     # PageRank(m, nnz, row_offsets, column_indices, degree, scores) copies the
@@ -816,12 +848,14 @@ def profile_solve(args):
 
     import gardenia_ocl_b200 as G
     csr = G.gen_rmat(args.scale, EDGE_FACTOR, seed=SEED, abc=ABC)
-    g = G.Graph(csr.rowptr, csr.col, csr.third, m=csr.m, nnz=csr.nnz)
+    blocked = args.profile_form == "blocked"
+    g = G.Graph(csr.rowptr, csr.col, csr.third, m=csr.m, nnz=csr.nnz, blocked=blocked)
     scores = torch.full((csr.m,), float(np.float32(1.0) / np.float32(csr.m)),
                         dtype=torch.float32, device="cuda")
     loop = G.LOOP_PERSISTENT if args.profile_loop == "persistent" else G.LOOP_GRAPH
     _, st = g.pagerank(scores, G.options(tol=0.0, max_iter=args.profile_solve, damping=DAMPING,
-                                         loop=loop))
+                                         loop=loop,
+                                         form=G.FORM_BLOCKED if blocked else G.FORM_EXACT))
     log(json.dumps({"m": csr.m, "nnz": csr.nnz, "layout": g.layout(), **st.as_dict()}))
     g.close()
     csr.close()
@@ -919,6 +953,8 @@ def main():
                          "nothing else (the case profiled with ncu)")
     ap.add_argument("--profile-loop", choices=["persistent", "graph"], default="persistent",
                     help="sweep loop of --profile-solve")
+    ap.add_argument("--profile-form", choices=["exact", "blocked"], default="exact",
+                    help="sweep form of --profile-solve (k_pr_hot / k_pr_step or k_pr_blocked)")
     ap.add_argument("--profile-multigraph", type=int, default=0, metavar="GRAPHS",
                     help="build the first GRAPHS graphs of the multi-graph batch and run one "
                          "solve of --profile-solve sweeps (the case profiled with ncu)")

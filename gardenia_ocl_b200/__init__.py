@@ -69,7 +69,9 @@ class TuneResult(C.Structure):
     def as_dict(self):
         lo = self.layout
         return {"sell_max": lo.sell_max, "chunk": lo.chunk, "chunk_min": lo.chunk_min,
-                "hot_entries": lo.hot_entries, "variant": self.variant,
+                "hot_entries": lo.hot_entries, "blocked": bool(lo.flags & LAYOUT_BLOCKED),
+                "block_rows": lo.block_rows, "tile_words": lo.tile_words,
+                "variant": self.variant,
                 "from_cache": bool(self.from_cache), "candidates": self.candidates,
                 "ms_per_sweep": self.ms_per_sweep,
                 "default_ms_per_sweep": self.default_ms_per_sweep,
@@ -728,9 +730,11 @@ def gen_uniform(n, seed, d_out) -> None:
 # Autotuner
 # ---------------------------------------------------------------------------
 def tune_graph(rowptr, col, outdeg, m=None, nnz=None, cache=None, sweeps=5) -> dict:
-    """Layout bins, hot prefix and kernel variant for this graph's in-degree
-    distribution (gpr_tune_graph).  Pass the result to ``Graph(**layout)`` and
-    ``pagerank(variant=...)``; ``cache``: path of the text cache (or None)."""
+    """Layout (exact order or blocked, bins, hot prefix) and kernel variant for
+    this graph's in-degree distribution (gpr_tune_graph).  Pass the layout
+    keys (sell_max, chunk, chunk_min, hot_entries, blocked, block_rows,
+    tile_words) to ``Graph(...)`` and ``variant`` to ``pagerank``; ``cache``:
+    path of the text cache (or None)."""
     m = int(len(rowptr) - 1) if m is None else int(m)
     nnz = int(len(col)) if nnz is None else int(nnz)
     pr, k0 = _ptr(rowptr, np.int32)

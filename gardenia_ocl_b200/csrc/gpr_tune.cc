@@ -9,16 +9,22 @@
 // time (BLOCK_SIZE, include/common.h:30; warp-per-row or thread-per-row
 // chosen by the Makefile, src/pr/Makefile:17-47).
 //
-// Search: coordinate descent from the defaults -- kernel variant, then hot
-// prefix, then lanes-per-row bound, then chunk threshold / size -- each
-// candidate timed as the best of `reps` solves of exactly `sweeps` sweeps
-// (tol 0), device time of the sweep loop (gpr_pr_stats.loop_ms), and taken
-// only when at least 3% faster than the current pick.  The batch
-// tuner groups graphs by signature and tunes one group at a time on the whole
-// batch, the other groups keeping their current picks.
+// Search (single graph): first the form -- the default exact-order layout
+// against the blocked layout (GPR_LAYOUT_BLOCKED, which costs a sort of the
+// edges at creation and pays on large graphs); then coordinate descent over
+// the chosen form's knobs: for the exact order the kernel variant, hot
+// prefix, lanes-per-row bound and chunk threshold / size; for the blocked
+// form the rows per block, words per tile, chunk threshold / size and hot
+// prefix.  Each candidate is timed as the best of kReps solves of exactly
+// `sweeps` sweeps (tol 0), device time of the sweep loop
+// (gpr_pr_stats.loop_ms), and taken only when at least kMargin faster than the
+// current pick.  The batch tuner groups graphs by signature and tunes one
+// group at a time on the whole batch, the other groups keeping their current
+// picks (exact order only).
 //
 // Cache file: one line per entry, later lines override earlier ones:
 //   <signature> <sell_max> <chunk> <chunk_min> <hot_entries> <variant> <ms_per_sweep>
+//       [<flags> <block_rows> <tile_words>]
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
@@ -34,15 +40,17 @@
 
 namespace {
 
-constexpr int kReps = 2;
+constexpr int kReps = 3;
 constexpr int kDefSell = 64, kDefChunk = 4096, kDefChunkMin = 4096, kDefHot = 32768;
 
 struct Cfg {
   int sell_max = kDefSell, chunk = kDefChunk, chunk_min = kDefChunkMin, hot = kDefHot,
       variant = 0;
+  int flags = 0, block_rows = 0, tile_words = 0;  // blocked form (0: library defaults)
   bool operator==(const Cfg &o) const {
     return sell_max == o.sell_max && chunk == o.chunk && chunk_min == o.chunk_min &&
-           hot == o.hot && variant == o.variant;
+           hot == o.hot && variant == o.variant && flags == o.flags &&
+           block_rows == o.block_rows && tile_words == o.tile_words;
   }
 };
 
@@ -69,12 +77,16 @@ std::map<std::string, std::pair<Cfg, double>> load_cache(const char *path) {
   if (!path) return c;
   FILE *f = fopen(path, "r");
   if (!f) return c;
-  char key[128];
-  Cfg x;
-  double ms = 0;
-  while (fscanf(f, "%127s %d %d %d %d %d %lf", key, &x.sell_max, &x.chunk, &x.chunk_min, &x.hot,
-                &x.variant, &ms) == 7)
-    c[key] = {x, ms};
+  char line[512];
+  while (fgets(line, sizeof(line), f)) {
+    char key[128];
+    Cfg x;
+    double ms = 0;
+    const int n = sscanf(line, "%127s %d %d %d %d %d %lf %d %d %d", key, &x.sell_max, &x.chunk,
+                         &x.chunk_min, &x.hot, &x.variant, &ms, &x.flags, &x.block_rows,
+                         &x.tile_words);
+    if (n == 7 || n == 10) c[key] = {x, ms};
+  }
   fclose(f);
   return c;
 }
@@ -83,8 +95,8 @@ void save_cache(const char *path, const std::string &key, const Cfg &x, double m
   if (!path) return;
   FILE *f = fopen(path, "a");
   if (!f) return;
-  fprintf(f, "%s %d %d %d %d %d %.6f\n", key.c_str(), x.sell_max, x.chunk, x.chunk_min, x.hot,
-          x.variant, ms);
+  fprintf(f, "%s %d %d %d %d %d %.6f %d %d %d\n", key.c_str(), x.sell_max, x.chunk, x.chunk_min,
+          x.hot, x.variant, ms, x.flags, x.block_rows, x.tile_words);
   fclose(f);
 }
 
@@ -95,6 +107,9 @@ gpr_layout_opts to_layout(const Cfg &x) {
   l.chunk = x.chunk;
   l.chunk_min = x.chunk_min;
   l.hot_entries = x.hot;
+  l.flags = x.flags;
+  l.block_rows = x.block_rows;
+  l.tile_words = x.tile_words;
   return l;
 }
 
@@ -222,17 +237,41 @@ int gpr_tune_graph(int m, long long nnz, const int *any_rowptr, const int *any_c
   const double t0 = time(x);
   if (!isfinite(t0)) return GPR_ECUDA;
   double best = t0;
-  descend(&x, &best, std::vector<int>{1, 2, 3, 4, 5, 6, 7},
-          [](Cfg *y, int v) { y->variant = v; }, time);
-  descend(&x, &best, std::vector<int>{8192, 16384, 56832},
-          [](Cfg *y, int v) { y->hot = v; }, time);
-  descend(&x, &best, std::vector<int>{16, 32, 128}, [](Cfg *y, int v) { y->sell_max = v; }, time);
-  descend(&x, &best, std::vector<std::pair<int, int>>{{1024, 1024}, {16384, 4096}, {4096, 1024}},
-          [](Cfg *y, std::pair<int, int> v) {
-            y->chunk_min = v.first;
-            y->chunk = v.second;
-          },
-          time);
+  Cfg xb;
+  xb.flags = GPR_LAYOUT_BLOCKED;
+  const double tb = time(xb);
+  if (tb < best * (1.0 - kMargin)) {
+    // the blocked form: its knobs, then the chunked rows' and the hot prefix
+    x = xb;
+    best = tb;
+    descend(&x, &best, std::vector<int>{6144, 8192},
+            [](Cfg *y, int v) { y->block_rows = v; }, time);
+    descend(&x, &best, std::vector<int>{131072, 524288},
+            [](Cfg *y, int v) { y->tile_words = v; }, time);
+    descend(&x, &best,
+            std::vector<std::pair<int, int>>{{16384, 4096}, {1 << 30, 4096}, {1024, 1024}},
+            [](Cfg *y, std::pair<int, int> v) {
+              y->chunk_min = v.first;
+              y->chunk = v.second;
+            },
+            time);
+    descend(&x, &best, std::vector<int>{8192, 16384},
+            [](Cfg *y, int v) { y->hot = v; }, time);
+  } else {
+    descend(&x, &best, std::vector<int>{1, 2, 3, 4, 5, 6, 7},
+            [](Cfg *y, int v) { y->variant = v; }, time);
+    descend(&x, &best, std::vector<int>{8192, 16384, 56832},
+            [](Cfg *y, int v) { y->hot = v; }, time);
+    descend(&x, &best, std::vector<int>{16, 32, 128}, [](Cfg *y, int v) { y->sell_max = v; },
+            time);
+    descend(&x, &best,
+            std::vector<std::pair<int, int>>{{1024, 1024}, {16384, 4096}, {4096, 1024}},
+            [](Cfg *y, std::pair<int, int> v) {
+              y->chunk_min = v.first;
+              y->chunk = v.second;
+            },
+            time);
+  }
   save_cache(cache_path, sig, x, best);
   fill_result(out, sig, x, best, t0, B.cands, 0);
   return GPR_OK;

@@ -7,6 +7,9 @@ import pytest
 
 from graphs import erdos_renyi, star
 
+LAYOUT_KEYS = ("sell_max", "chunk", "chunk_min", "hot_entries", "blocked", "block_rows",
+               "tile_words")
+
 
 def test_signature_classes(G, O):
     rp, _, _ = erdos_renyi(10000, 8, 1)
@@ -29,6 +32,16 @@ def test_cache_lookup_later_lines_win(G, tmp_path):
     assert r["hot_entries"] == 8192 and r["from_cache"] and r["ms_per_sweep"] == 0.25
     assert G.tune_cache_lookup(p, "batch:d3:s0")["sell_max"] == 128
     assert G.tune_cache_lookup(p, "pr:m1:d1:s1") is None
+    assert not G.tune_cache_lookup(p, "pr:m14:d4:s2")["blocked"]
+
+
+def test_cache_entries_of_the_blocked_form(G, tmp_path):
+    p = str(tmp_path / "tune.txt")
+    with open(p, "w") as f:
+        f.write("pr:m24:d4:s2 64 4096 1073741824 32768 0 0.59 4 8192 131072\n")
+    r = G.tune_cache_lookup(p, "pr:m24:d4:s2")
+    assert r["blocked"] and r["block_rows"] == 8192 and r["tile_words"] == 131072
+    assert r["chunk_min"] == 1 << 30 and r["ms_per_sweep"] == 0.59
 
 
 @pytest.mark.gpu
@@ -41,11 +54,10 @@ def test_tune_graph_and_cache(G, O, tmp_path):
     assert os.path.exists(cache)
     r2 = G.tune_graph(rp, col, od, cache=cache, sweeps=4)
     assert r2["from_cache"] and r2["signature"] == r["signature"]
-    for k in ("sell_max", "chunk", "chunk_min", "hot_entries", "variant"):
+    for k in LAYOUT_KEYS + ("variant",):
         assert r2[k] == r[k]
     ref, ref_it, _ = O.pr_plain_f32(rp, col, od, tol=1e-6, max_iter=100)
-    with G.Graph(rp, col, od, sell_max=r["sell_max"], chunk=r["chunk"],
-                 chunk_min=r["chunk_min"], hot_entries=r["hot_entries"]) as g:
+    with G.Graph(rp, col, od, **{k: r[k] for k in LAYOUT_KEYS}) as g:
         s, st = g.pagerank(tol=1e-6, max_iter=100, variant=r["variant"])
     assert abs(st.iterations - ref_it) <= 1
     s64, _, _ = O.pr_f64(rp, col, od, tol=0.0, max_iter=st.iterations)
