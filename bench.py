@@ -51,6 +51,15 @@ def pr_bytes_per_sweep(m, nnz):
     return 4 * nnz + 28 * m + 4
 
 
+# The BF16 + FP32-refinement results are reported as a study, not as a form
+# of the metric: a sweep here is bound by the latency and count of its gather
+# requests, not by their bytes, so a BF16 sweep costs what an FP32 sweep
+# costs, and the refinement back to the FP32 error needs as many FP32 sweeps
+# as the plain solve would have taken from the BF16 start.
+BF16_NOTE = ("measured, not a gain: BF16 halves gather bytes but the sweep is bound by "
+             "request latency and count, so a BF16 sweep costs what an FP32 sweep costs; "
+             "refining to the FP32 error then adds sweeps (time to solution >= plain)")
+
 # Random 4-byte gathers served by L2 on one B200, whole GPU (requests/s):
 # profiles/gather_rates.md, 289-296 G/s for L2-resident working sets.
 L2_GATHER_RATE = 290e9
@@ -399,16 +408,30 @@ def run_ours(args):
                                "via gpr_page_rank, pinned host buffers"}
 
     if not args.no_forms:
-        line["forms"] = forms_leg(G, torch, dev, g, m, nnz, gteps / world, args, x_star)
-        line["forms"]["pr_bf16_refined"]["time_to_solution_vs_plain"] = (
-            (ms / args.steps) / line["forms"]["pr_bf16_refined"]["loop_ms"])
+        line["forms"] = forms_leg(G, torch, dev, g, m, nnz, gteps / world, args, x_star,
+                                  (csr.rowptr.to_numpy(), csr.third.to_numpy()))
+        line["forms"]["bf16_study"]["pr_bf16_refined"]["time_to_solution_vs_plain"] = (
+            (ms / args.steps) / line["forms"]["bf16_study"]["pr_bf16_refined"]["loop_ms"])
     if not args.no_multigraph:
         line["multigraph"] = multigraph_leg(G, torch, dev, stream, gteps / world, args)
     if not args.no_forms:
         line["ppr"] = ppr_leg(G, torch, dev, stream, args)
 
+    if not args.no_s16:
+        line["s16"] = s16_leg(G, torch, dev, stream, args)
+    if rank == 0 and not args.no_ref_cuda:
+        line["reference_cuda"] = reference_cuda_leg(G, torch, dev, csr, args)
+        line["reference_cuda"]["gpr_pr_gteps"] = gteps / world
+        if "pr_gather_warp" in line["reference_cuda"]:
+            line["reference_cuda"]["gpr_vs_gather_warp"] = (
+                gteps / world / line["reference_cuda"]["pr_gather_warp"]["gteps"])
+            line["reference_cuda"]["gpr_vs_gather"] = (
+                gteps / world / line["reference_cuda"]["pr_gather"]["gteps"])
     if not args.no_spmv:
         line["spmv"] = spmv_leg(G, torch, dev, stream, args)
+        if "spmv_base" in line.get("reference_cuda", {}):
+            line["reference_cuda"]["gpr_spmv_vs_base"] = (
+                line["reference_cuda"]["spmv_base"]["ms"] / line["spmv"]["ms"])
     if not args.no_spmv:
         line["symgs"] = symgs_leg(G, torch, dev, args)
     if args.io and rank == 0:
@@ -500,7 +523,7 @@ def errors_vs(x_star, s):
             "max_error_vs_fp64_fixed_point": float(e.max())}
 
 
-def forms_leg(G, torch, dev, g, m, nnz, plain_gteps, args, x_star=None):
+def forms_leg(G, torch, dev, g, m, nnz, plain_gteps, args, x_star=None, g_host_degrees=None):
     """The forms the metric compares with the plain FP32 path, on the same
     graph: batched personalized PageRank (k seed vectors, one persistent
     launch) in FP32 and in BF16 with FP32 refinement.  Rates are edge-vector
@@ -518,12 +541,14 @@ def forms_leg(G, torch, dev, g, m, nnz, plain_gteps, args, x_star=None):
         if best is None or st.loop_ms < best.loop_ms:
             best = st
     resid = g.residual_f64(scores, DAMPING)
-    out["pr_bf16_refined"] = {
+    study = {"note": BF16_NOTE}
+    study["pr_bf16_refined"] = {
         "sweeps": best.iterations, "refine_sweeps": best.refine_iterations,
         "loop_ms": best.loop_ms, "gteps": nnz * best.iterations / (best.loop_ms / 1e3) / 1e9,
         "time_to_solution_vs_plain": None, "l1_error_bound_vs_fixed_point": resid / (1 - 0.85)}
     if x_star is not None:
-        out["pr_bf16_refined"].update(errors_vs(x_star, scores))
+        study["pr_bf16_refined"].update(errors_vs(x_star, scores))
+    out["bf16_study"] = study
     # push direction (atomic scatter) on the same graph, FP32
     best = None
     for _ in range(3):
@@ -538,9 +563,12 @@ def forms_leg(G, torch, dev, g, m, nnz, plain_gteps, args, x_star=None):
     if x_star is not None:
         out["pr_push_fp32"].update(errors_vs(x_star, scores))
     rng = np.random.default_rng(5)
+    rp_h, od_h = g_host_degrees
+    pool = np.flatnonzero((np.diff(rp_h) > 0) & (od_h > 0)).astype(np.int32)
     for k, prec, name in ((8, G.PREC_FP32, "ppr_k8_fp32"), (32, G.PREC_FP32, "ppr_k32_fp32"),
                           (32, G.PREC_BF16, "ppr_k32_bf16_refined")):
-        seeds = rng.integers(0, m, k).astype(np.int32)
+        dest = study if prec == G.PREC_BF16 else out
+        seeds = rng.choice(pool, k).astype(np.int32)
         buf = torch.empty(m * k, dtype=torch.float32, device=dev)
         best = None
         for _ in range(2):
@@ -549,7 +577,7 @@ def forms_leg(G, torch, dev, g, m, nnz, plain_gteps, args, x_star=None):
                 best = (st, it)
         st, it = best
         rate = nnz * k * st.iterations / (st.loop_ms / 1e3) / 1e9
-        out[name] = {"k": k,
+        dest[name] = {"k": k,
                      "precision": "bf16+fp32 refinement" if prec == G.PREC_BF16 else "fp32",
                      "sweeps": st.iterations, "refine_sweeps": st.refine_iterations,
                      "loop_ms": st.loop_ms, "edge_vector_gteps": rate,
@@ -572,23 +600,37 @@ def ppr_leg(G, torch, dev, stream, args):
     the plain FP32 single-vector GTEPS on the same graph is the comparison."""
     csr = G.gen_rmat(PPR_SCALE, EDGE_FACTOR, seed=SEED, abc=ABC)
     m, nnz = csr.m, csr.nnz
-    g = G.Graph(csr.rowptr, csr.col, csr.third, m=m, nnz=nnz, batched=True)
+    g = G.Graph(csr.rowptr, csr.col, csr.third, m=m, nnz=nnz, batched=True, blocked=True)
     g.set_stream(stream.cuda_stream)
     scores = torch.empty(m, dtype=torch.float32, device=dev)
-    best = None
-    for _ in range(4):
-        scores.fill_(float(np.float32(1.0) / np.float32(m)))
-        _, st = g.pagerank(scores, G.options(tol=TOL, max_iter=MAX_ITER, damping=DAMPING))
-        if best is None or st.loop_ms < best.loop_ms:
-            best = st
-    plain = nnz * best.iterations / (best.loop_ms / 1e3) / 1e9
+    plains = {}
+    for form, name in ((G.FORM_EXACT, "exact"), (G.FORM_BLOCKED, "blocked")):
+        best = None
+        for _ in range(4):
+            scores.fill_(float(np.float32(1.0) / np.float32(m)))
+            _, st = g.pagerank(scores, G.options(tol=TOL, max_iter=MAX_ITER, damping=DAMPING,
+                                                 form=form))
+            if best is None or st.loop_ms < best.loop_ms:
+                best = st
+        plains[name] = {"sweeps": best.iterations, "loop_ms": best.loop_ms,
+                        "gteps": nnz * best.iterations / (best.loop_ms / 1e3) / 1e9}
+    # the comparison: the faster single-vector FP32 form on the same graph
+    plain = max(p["gteps"] for p in plains.values())
     out = {"workload": f"ppr_rmat{PPR_SCALE}_ef{EDGE_FACTOR}_tol1e-6", "m": m, "nnz": nnz,
-           "plain_fp32": {"sweeps": best.iterations, "loop_ms": best.loop_ms, "gteps": plain}}
+           "seed_rule": "seeds drawn uniformly (seeded) from the vertices with in- and "
+                        "out-edges (a seed without out-edges keeps its mass and stops after "
+                        "one sweep)",
+           "plain_fp32": dict(gteps=plain, forms=plains),
+           "useful_rate": "nnz x (sum over vectors of the sweeps in which the vector still "
+                          "updated) per second of the sweep loop"}
+    rp_h, od_h = csr.rowptr.to_numpy(), csr.third.to_numpy()
+    pool = np.flatnonzero((np.diff(rp_h) > 0) & (od_h > 0)).astype(np.int32)
     rng = np.random.default_rng(22)
     for k in PPR_KS:
-        seeds = rng.integers(0, m, k).astype(np.int32)
+        seeds = rng.choice(pool, k).astype(np.int32)
         buf = torch.empty(m * k, dtype=torch.float32, device=dev)
         for prec, tag in ((G.PREC_FP32, "fp32"), (G.PREC_BF16, "bf16_refined")):
+            dest = out if prec == G.PREC_FP32 else out.setdefault("bf16_study", {"note": BF16_NOTE})
             bst = None
             for _ in range(2):
                 _, it, st = g.ppr(seeds, out=buf, tol=TOL, max_iter=MAX_ITER, precision=prec)
@@ -596,16 +638,20 @@ def ppr_leg(G, torch, dev, stream, args):
                     bst = (st, it)
             st, it = bst
             rate = nnz * k * st.iterations / (st.loop_ms / 1e3) / 1e9
-            out[f"k{k}_{tag}"] = {"sweeps": st.iterations, "refine_sweeps": st.refine_iterations,
-                                  "vector_sweeps_min": int(it.min()), "loop_ms": st.loop_ms,
+            useful = nnz * float(it.sum()) / (st.loop_ms / 1e3) / 1e9
+            dest[f"k{k}_{tag}"] = {"sweeps": st.iterations, "refine_sweeps": st.refine_iterations,
+                                  "vector_sweeps_min": int(it.min()),
+                                  "vector_sweeps_mean": float(it.mean()), "loop_ms": st.loop_ms,
                                   "edge_vector_gteps": rate, "vs_plain_fp32": rate / plain,
+                                  "useful_edge_vector_gteps": useful,
+                                  "useful_vs_plain_fp32": useful / plain,
                                   "max_final_residual": st.residual}
             # errors of the last solve's vectors against the FP64 fixed point
             xk = buf.view(m, k)
             x_star = ppr_fp64_fixed_point(torch, csr, m, seeds, xk)
             e = (xk.double() - x_star).abs()
-            out[f"k{k}_{tag}"]["max_l1_error_vs_fp64_fixed_point"] = float(e.sum(0).max())
-            out[f"k{k}_{tag}"]["max_error_vs_fp64_fixed_point"] = float(e.max())
+            dest[f"k{k}_{tag}"]["max_l1_error_vs_fp64_fixed_point"] = float(e.sum(0).max())
+            dest[f"k{k}_{tag}"]["max_error_vs_fp64_fixed_point"] = float(e.max())
             del x_star, e
         # the same FP32 solve as a CUDA-graph loop (one launch per sweep)
         bst = None
@@ -620,6 +666,105 @@ def ppr_leg(G, torch, dev, stream, args):
         del buf
     g.close()
     csr.close()
+    return out
+
+
+S16_SCALE, S16_TOL, S16_MAX_ITER = 16, 1e-4, 100
+
+
+def s16_leg(G, torch, dev, stream, args):
+    """plain PageRank on RMAT scale 16 (edge factor 16, same
+    RMAT parameters), tol 1e-4, at most 100 sweeps, from 1/m.  On the GPU
+    through the graph handle (device-resident graph: exact-order and blocked
+    forms, device time of the solve) and end to end through PageRank() with
+    host buffers; beside it the reference's own OpenMP PRSolver
+    (src/pr/omp_base.cc, compiled into oracle/_ref) solving the same graph on
+    the host cores (its full solve, wall time)."""
+    import oracle as O  # checker / baseline only
+    csr = G.gen_rmat(S16_SCALE, EDGE_FACTOR, seed=SEED, abc=ABC)
+    m, nnz = csr.m, csr.nnz
+    rp, col, od = csr.rowptr.to_numpy(), csr.col.to_numpy(), csr.third.to_numpy()
+    out = {"workload": f"pagerank_rmat{S16_SCALE}_ef{EDGE_FACTOR}_tol1e-4", "m": m, "nnz": nnz}
+    g = G.Graph(csr.rowptr, csr.col, csr.third, m=m, nnz=nnz, blocked=True)
+    g.set_stream(stream.cuda_stream)
+    scores = torch.empty(m, dtype=torch.float32, device=dev)
+    for form, name in ((G.FORM_EXACT, "gpu_exact"), (G.FORM_BLOCKED, "gpu_blocked")):
+        best = None
+        for _ in range(5):
+            scores.fill_(float(np.float32(1.0) / np.float32(m)))
+            _, st = g.pagerank(scores, G.options(tol=S16_TOL, max_iter=S16_MAX_ITER,
+                                                 damping=DAMPING, form=form))
+            if best is None or st.solve_ms < best.solve_ms:
+                best = st
+        out[name] = {"sweeps": best.iterations, "solve_ms": best.solve_ms,
+                     "loop_ms": best.loop_ms,
+                     "gteps": nnz * best.iterations / (best.solve_ms / 1e3) / 1e9}
+        if form == G.FORM_EXACT:
+            s_gpu = scores.cpu().numpy()
+    g.close()
+    # end to end: PageRank() on host arrays (copies, layout build, solve, copy back)
+    times, sweeps = [], 0
+    for i in range(4):
+        s_h = np.full(m, np.float32(1.0) / np.float32(m), dtype=np.float32)
+        t0 = time.perf_counter()
+        st = G.PageRank(m, nnz, rp, col, od, s_h, tol=S16_TOL, max_iter=S16_MAX_ITER,
+                        damping=DAMPING)
+        if i > 0:
+            times.append(time.perf_counter() - t0)
+            sweeps = st.iterations
+    e2e = min(times)
+    out["gpu_e2e"] = {"sweeps": sweeps, "ms": 1e3 * e2e, "gteps": nnz * sweeps / e2e / 1e9,
+                      "call": "PageRank(m, nnz, row_offsets, column_indices, degree, scores)"}
+    kind = "reference" if O.ref_available() else "port"
+    times = []
+    for i in range(4):
+        t0 = time.perf_counter()
+        if kind == "reference":
+            ref, printed, _ = O.ref_pr_solver(rp, col, od, tol=S16_TOL, max_iter=S16_MAX_ITER)
+            ref_sweeps = printed
+        else:
+            ref, ref_sweeps, _ = O.pr_plain_f32(rp, col, od, tol=S16_TOL, max_iter=S16_MAX_ITER)
+        if i > 0:
+            times.append(time.perf_counter() - t0)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    t = min(times)
+    out["cpu_reference"] = {"kind": kind, "cores": cores, "sweeps": ref_sweeps, "ms": 1e3 * t,
+                            "gteps": nnz * ref_sweeps / t / 1e9,
+                            "note": "wall time of the full solve (its per-sweep printf included)"}
+    out["max_abs_diff_gpu_vs_reference"] = float(np.abs(s_gpu - ref).max())
+    out["gpu_device_vs_cpu_reference"] = out["gpu_exact"]["gteps"] / out["cpu_reference"]["gteps"]
+    out["gpu_e2e_vs_cpu_reference"] = out["gpu_e2e"]["gteps"] / out["cpu_reference"]["gteps"]
+    csr.close()
+    return out
+
+
+REF_CUDA_SWEEPS = 10
+
+
+def reference_cuda_leg(G, torch, dev, csr24, args):
+    """The reference's own CUDA solvers (src/pr/gather.cu thread per row,
+    gather_warp.cu warp per row, src/spmv/base.cu thread per row), compiled
+    unmodified for sm_100a into oracle/_ref, on this benchmark's graph and on
+    the 27-point 128^3 stencil; times from their own Timer (the sweep loop,
+    including its per-sweep device-to-host residual copy).  gpr's numbers on
+    the same inputs beside them."""
+    import oracle as O  # baseline only
+    out = {}
+    if not O.ref_gpu_available("gather"):
+        return {"unavailable": "oracle/_ref CUDA solvers not built (needs the reference tree)"}
+    rp, col, od = csr24.rowptr.to_numpy(), csr24.col.to_numpy(), csr24.third.to_numpy()
+    nnz = len(col)
+    for name in ("gather", "gather_warp"):
+        _, it, ms, _ = O.ref_gpu_pr_solver(name, rp, col, od, tol=0.0, max_iter=REF_CUDA_SWEEPS)
+        out[f"pr_{name}"] = {"sweeps": it, "ms": ms, "gteps": nnz * it / (ms / 1e3) / 1e9,
+                             "workload": f"RMAT s{args.scale}, {REF_CUDA_SWEEPS} sweeps (tol 0)"}
+    Ap, Aj, Ax = O.stencil27(128)
+    m = len(Ap) - 1
+    x, y0 = O.uniform_f32(m, 3), np.zeros(m, np.float32)
+    O.ref_gpu_spmv_solver(Ap, Aj, Ax, x, y0)  # warm
+    _, ms = O.ref_gpu_spmv_solver(Ap, Aj, Ax, x, y0)
+    out["spmv_base"] = {"ms": ms, "gb_s": spmv_bytes(m, len(Aj)) / (ms / 1e3) / 1e9,
+                        "workload": "27-point 128^3 stencil, one SpMV"}
     return out
 
 
@@ -659,6 +804,7 @@ def multigraph_leg(G, torch, dev, stream, plain_gteps, args):
            if layouts else "defaults"}
     x_star = None
     for prec, name in ((G.PREC_FP32, "fp32"), (G.PREC_BF16, "bf16_refined")):
+        dest = out if prec == G.PREC_FP32 else out.setdefault("bf16_study", {"note": BF16_NOTE})
         best = None
         for _ in range(3):
             scores.copy_(init)
@@ -669,7 +815,7 @@ def multigraph_leg(G, torch, dev, stream, plain_gteps, args):
         st, it, res = best
         edges = float((nnz_g * it).sum())
         byts = float(((4 * nnz_g + 28 * m_g + 4) * it).sum())
-        out[name] = {"launch_sweeps": st.iterations, "refine_sweeps": st.refine_iterations,
+        dest[name] = {"launch_sweeps": st.iterations, "refine_sweeps": st.refine_iterations,
                      "graph_sweeps_min": int(it.min()), "graph_sweeps_max": int(it.max()),
                      "converged": int((res < TOL).sum()), "loop_ms": st.loop_ms,
                      "solve_ms": st.solve_ms, "gteps": edges / (st.loop_ms / 1e3) / 1e9,
@@ -684,8 +830,8 @@ def multigraph_leg(G, torch, dev, stream, plain_gteps, args):
             x_star, _, _ = fp64_fixed_point(torch, A, A.m, scores,
                                             base=torch.from_numpy(base).to(dev))
         e = (scores.double() - x_star).abs().cpu().numpy()
-        out[name]["max_l1_error_vs_fp64_fixed_point"] = float(np.add.reduceat(e, voff[:-1]).max())
-        out[name]["max_error_vs_fp64_fixed_point"] = float(e.max())
+        dest[name]["max_l1_error_vs_fp64_fixed_point"] = float(np.add.reduceat(e, voff[:-1]).max())
+        dest[name]["max_error_vs_fp64_fixed_point"] = float(e.max())
     del x_star
     # the FP32 solve again as a CUDA-graph loop (one launch per sweep)
     best = None
@@ -943,6 +1089,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-multigraph", action="store_true")
     ap.add_argument("--no-tune", action="store_true", help="default bins and kernel variant")
+    ap.add_argument("--no-s16", action="store_true", help="skip the RMAT s16 (tol 1e-4) leg")
+    ap.add_argument("--no-ref-cuda", action="store_true",
+                    help="skip the reference's own CUDA solvers on the benchmark inputs")
     ap.add_argument("--io", action="store_true",
                     help="also time graph loading: the reference's two read_graph calls vs "
                          "one parse with the CSRs built on the GPU")

@@ -916,6 +916,19 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
     if (ev_col) cudaEventDestroy(ev_col);
   }
   if (rc == GPR_OK && blocked) {
+    // Defaults sized to the graph: about two blocks and six tiles per SM
+    // (a multi-tile block adds one 8-byte atomic per row and tile).
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g->device);
+    const long long rows = (long long)g->L.n_nz - g->L.n_long;
+    const long long words = std::max(0LL, nnz - g->L.long_elems);
+    if (block_rows == 0)
+      block_rows = (int)std::min<long long>(
+          gpr::kBlockedRows, std::max<long long>(256, gpr::ceil_div(rows, 2LL * nsm)));
+    if (tile_words == 0)
+      tile_words = (int)std::min<long long>(
+          gpr::kTileWordsDefault,
+          std::max<long long>(4096, gpr::ceil_div(words, 6LL * nsm) / 512 * 512));
     rc = gpr::build_blocked_layout(m, nnz, (const int *)rp, (const int *)cp, g->L, block_rows,
                                    tile_words, &g->B, st);
     g->has_blocked = rc == GPR_OK;
@@ -1310,12 +1323,13 @@ int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr, const int *
   if (lopts && lopts->chunk) chunk = lopts->chunk;
   if (lopts && lopts->chunk_min) chunk_min = lopts->chunk_min;
   if (lopts && lopts->hot_entries) hot_max = lopts->hot_entries;
-  int block_rows = gpr::kBlockedRows, tile_words = gpr::kTileWordsDefault;
-  if (lopts && lopts->block_rows) block_rows = lopts->block_rows;
-  if (lopts && lopts->tile_words) tile_words = lopts->tile_words;
+  int block_rows = 0, tile_words = 0;  // 0: sized to the graph at creation
+  if (lopts) block_rows = lopts->block_rows;
+  if (lopts) tile_words = lopts->tile_words;
   if (lane_max < 1 || lane_max > 1024 || chunk < 128 || chunk % 128 != 0 || chunk_min < 1 ||
-      hot_max < 4 || hot_max > gpr::kHotMax || hot_max % 4 != 0 || block_rows < 1 ||
-      block_rows > gpr::kBlockedMaxRows || tile_words < gpr::kRunWords) {
+      hot_max < 4 || hot_max > gpr::kHotMax || hot_max % 4 != 0 || block_rows < 0 ||
+      block_rows > gpr::kBlockedMaxRows || tile_words < 0 ||
+      (tile_words > 0 && tile_words < gpr::kRunWords)) {
     gpr::set_error("gpr_graph_create_ex: invalid layout options (lane_max %d, chunk %d, "
                    "chunk_min %d, hot_entries %d, block_rows %d, tile_words %d)", lane_max, chunk,
                    chunk_min, hot_max, block_rows, tile_words);

@@ -249,7 +249,7 @@ int gpr_tune_graph(int m, long long nnz, const int *any_rowptr, const int *any_c
     descend(&x, &best, std::vector<int>{131072, 524288},
             [](Cfg *y, int v) { y->tile_words = v; }, time);
     descend(&x, &best,
-            std::vector<std::pair<int, int>>{{16384, 4096}, {1 << 30, 4096}, {1024, 1024}},
+            std::vector<std::pair<int, int>>{{16384, 4096}, {1024, 1024}},
             [](Cfg *y, std::pair<int, int> v) {
               y->chunk_min = v.first;
               y->chunk = v.second;

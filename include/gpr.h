@@ -136,8 +136,10 @@ typedef struct {
   int hot_entries;/* contributions of the highest in-degree vertices kept in shared memory
                      by the persistent kernel, multiple of 4, <= 56832 (default 32768) */
   int flags;      /* GPR_LAYOUT_* bits */
-  int block_rows; /* blocked form: rows per block, <= 12288 (default 12288) */
-  int tile_words; /* blocked form: most entry words per tile, >= 512 (default 262144) */
+  int block_rows; /* blocked form: rows per block, <= 12288 (default: about rows / (2 SMs),
+                     256 .. 12288) */
+  int tile_words; /* blocked form: most entry words per tile, >= 512 (default: about
+                     edges / (6 SMs), 4096 .. 262144) */
   int reserved[1];
 } gpr_layout_opts;
 int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr,
