@@ -622,7 +622,11 @@ def ppr_leg(G, torch, dev, stream, args):
                         "one sweep)",
            "plain_fp32": dict(gteps=plain, forms=plains),
            "useful_rate": "nnz x (sum over vectors of the sweeps in which the vector still "
-                          "updated) per second of the sweep loop"}
+                          "updated) per second of the sweep loop",
+           "edge_vector_rate": "nominal: nnz x k x the batch's sweeps per second; once half "
+                               "of the vectors stop, the rest continue packed into a narrower "
+                               "layout (gpr_pr_opts.ppr_repack), so later sweeps do less than "
+                               "k vectors' work"}
     rp_h, od_h = csr.rowptr.to_numpy(), csr.third.to_numpy()
     pool = np.flatnonzero((np.diff(rp_h) > 0) & (od_h > 0)).astype(np.int32)
     rng = np.random.default_rng(22)

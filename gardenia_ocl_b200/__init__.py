@@ -41,7 +41,7 @@ class PrOptions(C.Structure):
     _fields_ = [("damping", C.c_float), ("tol", C.c_double), ("max_iter", C.c_int),
                 ("precision", C.c_int), ("loop", C.c_int), ("timeout_s", C.c_double),
                 ("refine_max", C.c_int), ("variant", C.c_int), ("reserved", C.c_int * 1),
-                ("form", C.c_int), ("pad", C.c_int * 5)]
+                ("form", C.c_int), ("ppr_repack", C.c_int), ("pad", C.c_int * 4)]
 
 
 class LayoutOptions(C.Structure):
@@ -202,12 +202,13 @@ def _ptr(a, dtype=None):
 
 
 def options(tol=EPSILON, max_iter=MAX_ITER, damping=KDAMP, precision=PREC_FP32,
-            loop=LOOP_AUTO, timeout_s=5.0, refine_max=64, variant=0, form=FORM_AUTO) -> PrOptions:
+            loop=LOOP_AUTO, timeout_s=5.0, refine_max=64, variant=0, form=FORM_AUTO,
+            ppr_repack=True) -> PrOptions:
     o = PrOptions()
     _check(lib().gpr_pr_opts_default(C.byref(o)))
     o.tol, o.max_iter, o.damping = float(tol), int(max_iter), float(damping)
     o.precision, o.loop, o.timeout_s, o.refine_max = int(precision), int(loop), float(timeout_s), int(refine_max)
-    o.variant, o.form = int(variant), int(form)
+    o.variant, o.form, o.ppr_repack = int(variant), int(form), 1 if ppr_repack else 0
     return o
 
 

@@ -298,6 +298,7 @@ int gpr_pr_opts_default(gpr_pr_opts *o) {
   o->loop = GPR_LOOP_AUTO;
   o->timeout_s = 5.0;
   o->refine_max = 64;
+  o->ppr_repack = 1;
   return GPR_OK;
 }
 

@@ -253,6 +253,11 @@ struct gpr_graph {
   int *b_pk = nullptr;
   int b_npk = -1;
   long long b_pk_want = 0;
+  // Packet tables of the narrower layouts a batched solve packs its
+  // still-updating vectors into, by log2 of the rows per row group.
+  int *b_pkr[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+  int b_npkr[6] = {-1, -1, -1, -1, -1, -1};
+  long long b_pkwr[6] = {0, 0, 0, 0, 0, 0};
   // Push solver: edges sorted by source and the per-vertex accumulators,
   // built on first use.
   int *push_src = nullptr, *push_dst = nullptr;

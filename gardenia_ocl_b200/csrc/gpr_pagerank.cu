@@ -840,6 +840,7 @@ void destroy(gpr_graph *g) {
   gpr::dfree(g->b_crow);
   gpr::dfree(g->b_cdesc);
   gpr::dfree(g->b_pk);
+  for (int i = 0; i < 6; ++i) gpr::dfree(g->b_pkr[i]);
   gpr::dfree(g->push_src);
   gpr::dfree(g->push_dst);
   gpr::dfree(g->push_sum);

@@ -60,11 +60,13 @@ struct PprArgs {
   unsigned *active;      // [2][4] bit q: vector q still updating, by parity
   int *iters;            // [K]
   unsigned *bar;         // [2] arrivals, generation
-  int *status;           // [0] error flags, [1] sweeps, [2] any active
+  int *status;           // [0] error flags, [1] sweeps, [2] 1: vectors still updating,
+                         // 2: stopped for packing (at most repack_below still updating)
   int *wq;               // [2] packet-queue heads by sweep parity
   float damp;
   double tol;
   int max_iter, bar_expect;
+  int repack_below;      // > 0: stop once at most this many vectors are still updating
   long long timeout_ns;
   unsigned long long cond;  // graph mode: while-node condition handle (0: none)
 };
@@ -437,11 +439,13 @@ __device__ __forceinline__ void ppr_close(const PprArgs &a, int it, unsigned *s_
   __syncthreads();
   if (threadIdx.x == 0) {
     unsigned any = 0;
+    int n = 0;
     for (int i = 0; i < 4; ++i) {
       a.active[((it + 1) & 1) * 4 + i] = s_act[i];
       any |= s_act[i];
+      n += __popc(s_act[i]);
     }
-    a.status[2] = any != 0;
+    a.status[2] = any == 0 ? 0 : (n <= a.repack_below ? 2 : 1);
     atomicExch(a.wq + (it & 1), 0);
   }
   __syncthreads();
@@ -509,7 +513,7 @@ __global__ void __launch_bounds__(kPprBlock, Shape<K>::min_ctas) k_ppr(PprArgs a
     __syncthreads();
     if (s_state == 2) return;
     ++it;
-    if (!__ldcg(a.status + 2)) break;
+    if (__ldcg(a.status + 2) != 1) break;
   }
   if (blockIdx.x == 0 && threadIdx.x == 0) a.status[1] = it;
 }
@@ -529,7 +533,7 @@ __global__ void __launch_bounds__(kPprBlock, Shape<K>::min_ctas) k_ppr_step(PprA
   __shared__ int s_it, s_last;
   if (threadIdx.x == 0) {
     const int n_done = *(volatile int *)(a.status + 1);
-    const bool live = n_done == 0 || *(volatile int *)(a.status + 2) != 0;
+    const bool live = n_done == 0 || *(volatile int *)(a.status + 2) == 1;
     s_it = live && n_done < a.max_iter ? n_done : -1;
     if (a.cond && blockIdx.x == 0) {
       const int n = atomicAdd(a.status + 3, 1) + 1;
@@ -556,7 +560,7 @@ __global__ void __launch_bounds__(kPprBlock, Shape<K>::min_ctas) k_ppr_step(PprA
     atomicExch(a.bar, 0u);
     a.status[1] = it + 1;
     __threadfence();
-    if (a.cond && (!a.status[2] || it + 1 >= a.max_iter)) cudaGraphSetConditional(a.cond, 0u);
+    if (a.cond && (a.status[2] != 1 || it + 1 >= a.max_iter)) cudaGraphSetConditional(a.cond, 0u);
   }
 }
 
@@ -617,6 +621,58 @@ __global__ void k_ppr_scatter(int m, int k, const int *__restrict__ perm,
   out[(size_t)perm[v] * k + q] = x[(size_t)v * K + q];
 }
 
+// Packing of the still-updating vectors into a narrower layout of Kn slots:
+// slot j of the new layout takes slot sel[j] of the old one (x, the
+// contributions the next sweep reads, including the zero sentinel row m, the
+// dangling mass of the current iterate and the seed); slots past n_sel are
+// padding (seed -1, zeros).
+__global__ void k_ppr_pack(int m, int K, int Kn, int n_sel, const int *__restrict__ sel,
+                           const float *__restrict__ x, const float *__restrict__ c,
+                           const double *__restrict__ dang, const int *__restrict__ seed,
+                           float *xn, float *cn, double *dangn, int *seedn) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t < ((long long)m + 1) * Kn) {
+    const long long v = t / Kn;
+    const int j = (int)(t % Kn);
+    const bool in = j < n_sel;
+    const int q = in ? sel[j] : 0;
+    if (v < m) xn[t] = in ? x[v * K + q] : 0.f;
+    cn[t] = in ? c[v * K + q] : 0.f;
+  }
+  if (t < Kn) {
+    const bool in = t < n_sel;
+    dangn[t] = in ? dang[sel[t]] : 0.0;
+    dangn[Kn + t] = 0.0;
+    seedn[t] = in ? seed[sel[t]] : -1;
+  }
+}
+
+// Results of a packed layout back into the layout of K slots: slot j of the
+// packed layout is slot slot_of[j] there (-1: padding).
+__global__ void k_ppr_unpack(int m, int K, int Kn, const int *__restrict__ slot_of,
+                             const float *__restrict__ xn, float *x) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (t >= (long long)m * Kn) return;
+  const long long v = t / Kn;
+  const int j = (int)(t % Kn);
+  const int q = slot_of[j];
+  if (q >= 0) x[v * K + q] = xn[t];
+}
+
+// Masks of a fresh packed layout of Kn slots: the first n vectors updating,
+// sweep counts 0.
+__global__ void k_ppr_masks(int n, int Kn, int *iters, unsigned *active) {
+  const int t = threadIdx.x;
+  if (t < Kn) iters[t] = 0;
+  if (t < 4) {
+    unsigned w = 0;
+    for (int b = 0; b < 32; ++b)
+      if (t * 32 + b < n) w |= 1u << b;
+    active[t] = w;
+    active[4 + t] = w;
+  }
+}
+
 __global__ void k_invert_for_seeds(int m, const int *__restrict__ perm, int k,
                                    const int *__restrict__ seeds_old, int *seed_new) {
   const int v = blockIdx.x * blockDim.x + threadIdx.x;
@@ -670,6 +726,11 @@ int build_chunk_table(gpr_graph *g, int dmax, int chunk, cudaStream_t st) {
   g->b_cdesc = nullptr;
   g->b_nlong = -1;
   g->b_npk = -1;
+  for (int i = 0; i < 6; ++i) {
+    gpr::dfree(g->b_pkr[i]);
+    g->b_pkr[i] = nullptr;
+    g->b_npkr[i] = -1;
+  }
   const gpr::PrLayout &L = g->L;
   int *cnt = nullptr;
   GPR_TRY(gpr::dalloc(&cnt, 1, "chunk count"));
@@ -777,6 +838,39 @@ int build_packets(gpr_graph *g, int R, long long want, cudaStream_t st) {
   return GPR_OK;
 }
 
+// Packets for row groups of R rows over the current chunk table, cached per
+// R (the layouts of a solve's packed levels); the packet array stays owned by
+// the graph.
+int packets_for(gpr_graph *g, int R, long long want, cudaStream_t st, int **pk, int *npk) {
+  int slot = 0;
+  while ((1 << slot) < R) ++slot;
+  if (g->b_npkr[slot] < 0 || g->b_pkwr[slot] != want) {
+    gpr::dfree(g->b_pkr[slot]);
+    g->b_pkr[slot] = nullptr;
+    g->b_npkr[slot] = -1;
+    const gpr::PrLayout &L = g->L;
+    const int n_units = g->b_nchunks + (int)gpr::ceil_div((long long)L.n_nz - g->b_nlong, R);
+    long long *cost = nullptr;
+    GPR_TRY(gpr::dalloc(&cost, (size_t)std::max(1, n_units), "packet costs"));
+    int rc = GPR_OK;
+    if (n_units > 0) {
+      k_pk_cost<<<(unsigned)gpr::ceil_div(n_units, 256), 256, 0, st>>>(
+          g->b_nchunks, n_units, R, g->b_nlong, L.n_nz,
+          reinterpret_cast<const int4 *>(g->b_cdesc), L.csr_ptr, cost);
+      rc = GPR_CUDA_RC(cudaGetLastError());
+    }
+    int n = 0;
+    if (rc == GPR_OK) rc = gpr::make_packets(cost, n_units, want, &g->b_pkr[slot], &n, st);
+    gpr::dfree(cost);
+    GPR_TRY(rc);
+    g->b_npkr[slot] = n;
+    g->b_pkwr[slot] = want;
+  }
+  *pk = g->b_pkr[slot];
+  *npk = g->b_npkr[slot];
+  return GPR_OK;
+}
+
 struct PprKernels {
   const void *solve;  // persistent: all sweeps in one cooperative launch
   const void *step;   // one sweep per launch (graph mode)
@@ -808,11 +902,11 @@ PprKernels select(int K, bool bf16) {
 }
 
 struct Bufs {
-  void *p[32] = {nullptr};
+  void *p[64] = {nullptr};
   int n = 0;
   template <typename X>
   int get(X **out, size_t count, const char *what) {
-    if (n >= 32) {
+    if (n >= 64) {
       gpr::set_error("gpr_ppr: too many scratch buffers");
       return GPR_ENOMEM;
     }
@@ -888,21 +982,23 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
   GPR_TRY(build_chunk_table(g, b_dmax, b_chunk, st));
   const long long units =
       (long long)g->b_nchunks + gpr::ceil_div((long long)L.n_nz - g->b_nlong, R);
-  auto grid_of = [&](const PprKernels &kk, int *grid) -> int {
+  auto grid_of = [&](const PprKernels &kk, int Kx, long long units_x, int *grid) -> int {
+    const size_t smem_x = sizeof(double) * 2 * (kPprBlock / 32) * Kx;
     int per_sm = 0;
-    GPR_CUDA(cudaFuncSetAttribute(kk.solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kk.solve, kPprBlock, smem));
+    GPR_CUDA(cudaFuncSetAttribute(kk.solve, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem_x));
+    GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kk.solve, kPprBlock, smem_x));
     if (per_sm < 1) {
       gpr::set_error("gpr_ppr: kernel cannot be resident");
       return GPR_ECUDA;
     }
     *grid = (int)std::max<long long>(1, std::min<long long>((long long)sms * per_sm,
-                                                          gpr::ceil_div(units, kPprBlock / 32)));
+                                                          gpr::ceil_div(units_x, kPprBlock / 32)));
     return GPR_OK;
   };
   int G32 = 0, G16 = 0;
-  GPR_TRY(grid_of(k32, &G32));
-  if (bf16) GPR_TRY(grid_of(k16, &G16));
+  GPR_TRY(grid_of(k32, K, units, &G32));
+  if (bf16) GPR_TRY(grid_of(k16, K, units, &G16));
   const int Gmax = std::max(G32, G16);
   // About 32 packets per warp of the larger grid: fine enough that the end
   // of a sweep is not held by one warp's last packet (measured on RMAT s22:
@@ -932,7 +1028,9 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
   GPR_TRY(B.get(&iters, (size_t)K, "ppr iterations"));
   GPR_TRY(B.get(&status, 4, "ppr status"));
   GPR_TRY(B.get(&wq, 4, "ppr queues"));
-  GPR_TRY(B.get(&cta_red, (size_t)2 * Gmax * K, "ppr cta sums"));
+  // per-CTA sums of the widest layout; a packed layout (K/2 or narrower) runs
+  // at most 4 CTAs per SM and fits
+  GPR_TRY(B.get(&cta_red, (size_t)2 * std::max(Gmax, 4 * sms) * K, "ppr cta sums"));
   GPR_TRY(B.get(&seed_red, (size_t)2 * K, "ppr seed sums"));
   GPR_TRY(B.get(&res_hist, (size_t)std::max(1, max_iter) * K, "ppr residuals"));
   GPR_TRY(B.get(&dang, (size_t)2 * K, "ppr dangling"));
@@ -983,7 +1081,7 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
   // one k_ppr_step launch (the kernel clears the condition when the phase is
   // done).  Built, run and released per phase; `mark` records the loop's
   // start event after the graph is built, right before its launch.
-  auto step_loop = [&](const PprKernels &kk, int G, bool mark) -> int {
+  auto step_loop = [&](const PprKernels &kk, int G, size_t smem, bool mark) -> int {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     cudaGraphConditionalHandle h = 0;
@@ -1026,8 +1124,9 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
   // cooperative launch, or (GPR_LOOP_GRAPH, or when the grid cannot be
   // co-resident) in the graph loop.  The first phase (`mark`) records the
   // start event of the sweep loop right before its launch.
-  auto phase = [&](const PprKernels &kk, int G, double tol, bool mark, int *sweeps,
-                   std::vector<int> *it_out) -> int {
+  auto phase = [&](const PprKernels &kk, int G, int Kx, double tol, bool mark, int *sweeps,
+                   std::vector<int> *it_out, int *stop) -> int {
+    const size_t smem = sizeof(double) * 2 * (kPprBlock / 32) * Kx;
     a.tol = tol;
     a.bar_expect = G + (o.reserved[0] > 0 ? o.reserved[0] : 0);
     GPR_CUDA(cudaMemsetAsync(status, 0, sizeof(int) * 4, st));
@@ -1047,13 +1146,14 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
         ++launches;
       }
     }
-    if (max_iter > 0 && graph_mode) GPR_TRY(step_loop(kk, G, mark && o.loop == GPR_LOOP_GRAPH));
+    if (max_iter > 0 && graph_mode) GPR_TRY(step_loop(kk, G, smem, mark && o.loop == GPR_LOOP_GRAPH));
     int hs[4];
     GPR_CUDA(cudaMemcpyAsync(hs, status, sizeof(hs), cudaMemcpyDeviceToHost, st));
-    it_out->assign(K, 0);
-    GPR_CUDA(cudaMemcpyAsync(it_out->data(), iters, sizeof(int) * K, cudaMemcpyDeviceToHost, st));
+    it_out->assign(Kx, 0);
+    GPR_CUDA(cudaMemcpyAsync(it_out->data(), iters, sizeof(int) * Kx, cudaMemcpyDeviceToHost, st));
     GPR_CUDA(cudaStreamSynchronize(st));
     *sweeps = hs[1];
+    *stop = hs[2];
     if (max_iter > 0 && graph_mode) launches += hs[3];
     if (hs[0] & 1) {
       gpr::set_error("gpr_ppr: grid barrier wait exceeded %.3f s", o.timeout_s);
@@ -1061,15 +1161,122 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
     }
     return GPR_OK;
   };
+  // FP32 sweeps to `tol` with packing: the widest layout first; whenever at
+  // most half of its vectors are still updating (and it is wider than 8), the
+  // kernel stops, those vectors' x, next contributions, dangling mass and
+  // seeds are packed into the next narrower layout, and the sweeps go on
+  // there with the remaining sweep budget.  Vectors that stopped keep their
+  // final x in the widest layout (the master), where every packed layout is
+  // written back.  sweeps: launches' sweeps in total; it_total: per vector.
+  int last_sw = 0, last_K = K;  // sweeps and width of the last layout (its residuals)
+  auto fp32_phase = [&](double tol, bool mark, int *sweeps, std::vector<int> *it_total) -> int {
+    it_total->assign(K, 0);
+    *sweeps = 0;
+    int Kc = K, Gc = G32;
+    PprKernels kc = k32;
+    float *xc = x;
+    void *cc0 = c0, *cc1 = c1;
+    double *dc = dang;
+    int *sc = seed;
+    std::vector<int> slot_of(K);  // master slot of each slot of the current layout
+    for (int q = 0; q < K; ++q) slot_of[q] = q < k ? q : -1;
+    int *d_slot_of = nullptr;
+    bool first = true;
+    for (;;) {
+      a.repack_below = (o.ppr_repack && Kc > 8) ? Kc / 2 : 0;
+      a.max_iter = max_iter - *sweeps;
+      int sw = 0, stop = 0;
+      std::vector<int> itc;
+      GPR_TRY(phase(kc, Gc, Kc, tol, mark && first, &sw, &itc, &stop));
+      first = false;
+      *sweeps += sw;
+      last_sw = sw;
+      last_K = Kc;
+      for (int q = 0; q < Kc; ++q)
+        if (slot_of[q] >= 0) (*it_total)[slot_of[q]] += itc[q];
+      const bool packed = Kc != K;
+      if (stop != 2 || *sweeps >= max_iter) {
+        if (packed) {  // the packed layout's results back into the master
+          k_ppr_unpack<<<(unsigned)gpr::ceil_div((long long)m * Kc, 256), 256, 0, st>>>(
+              m, K, Kc, d_slot_of, xc, x);
+          ++launches;
+          GPR_CUDA(cudaGetLastError());
+        }
+        break;
+      }
+      // the slots still updating after the last sweep
+      unsigned act[4];
+      GPR_CUDA(cudaMemcpyAsync(act, active + (sw & 1) * 4, sizeof(act), cudaMemcpyDeviceToHost,
+                               st));
+      GPR_CUDA(cudaStreamSynchronize(st));
+      std::vector<int> sel;
+      for (int q = 0; q < Kc; ++q)
+        if ((act[q >> 5] >> (q & 31)) & 1u) sel.push_back(q);
+      const int Kn = pick_k((int)sel.size());
+      if (packed) {
+        k_ppr_unpack<<<(unsigned)gpr::ceil_div((long long)m * Kc, 256), 256, 0, st>>>(
+            m, K, Kc, d_slot_of, xc, x);
+        ++launches;
+      }
+      float *xn = nullptr, *cn0 = nullptr, *cn1 = nullptr;
+      double *dn = nullptr;
+      int *sn = nullptr, *d_sel = nullptr, *d_so = nullptr;
+      GPR_TRY(B.get(&xn, (size_t)m * Kn, "ppr packed x"));
+      GPR_TRY(B.get(&cn0, ((size_t)m + 1) * Kn, "ppr packed contrib0"));
+      GPR_TRY(B.get(&cn1, ((size_t)m + 1) * Kn, "ppr packed contrib1"));
+      GPR_TRY(B.get(&dn, (size_t)2 * Kn, "ppr packed dangling"));
+      GPR_TRY(B.get(&sn, (size_t)Kn, "ppr packed seeds"));
+      GPR_TRY(B.get(&d_sel, sel.size(), "ppr packed selection"));
+      GPR_TRY(B.get(&d_so, (size_t)Kn, "ppr packed slots"));
+      std::vector<int> so(Kn, -1);
+      for (size_t j = 0; j < sel.size(); ++j) so[j] = slot_of[sel[j]];
+      GPR_CUDA(cudaMemcpyAsync(d_sel, sel.data(), sizeof(int) * sel.size(), cudaMemcpyHostToDevice,
+                               st));
+      GPR_CUDA(cudaMemcpyAsync(d_so, so.data(), sizeof(int) * Kn, cudaMemcpyHostToDevice, st));
+      GPR_CUDA(cudaMemsetAsync(cn1, 0, sizeof(float) * ((size_t)m + 1) * Kn, st));
+      const float *ccur = static_cast<const float *>((sw & 1) ? cc1 : cc0);
+      k_ppr_pack<<<(unsigned)gpr::ceil_div(((long long)m + 1) * Kn, 256), 256, 0, st>>>(
+          m, Kc, Kn, (int)sel.size(), d_sel, xc, ccur, dc + (sw & 1) * Kc, sc, xn, cn0, dn, sn);
+      k_ppr_masks<<<1, 128, 0, st>>>((int)sel.size(), Kn, iters, active);
+      launches += 2;
+      GPR_CUDA(cudaGetLastError());
+      // the narrower layout's kernels, grid and packets
+      Kc = Kn;
+      kc = select(Kc, false);
+      const int Rn = 32 / (Kc / 4);
+      const long long units_n =
+          (long long)g->b_nchunks + gpr::ceil_div((long long)L.n_nz - g->b_nlong, Rn);
+      GPR_TRY(grid_of(kc, Kc, units_n, &Gc));
+      int *pk = nullptr, npk = 0;
+      GPR_TRY(packets_for(g, Rn, (long long)Gc * (kPprBlock / 32) * 32, st, &pk, &npk));
+      a.pk = pk;
+      a.n_pk = npk;
+      a.k = (int)sel.size();
+      a.x = xn;
+      a.c0 = cn0;
+      a.c1 = cn1;
+      a.dang = dn;
+      a.seed = sn;
+      xc = xn;
+      cc0 = cn0;
+      cc1 = cn1;
+      dc = dn;
+      sc = sn;
+      d_slot_of = d_so;
+      slot_of = so;
+    }
+    return GPR_OK;
+  };
   GPR_CUDA(cudaEventRecord(g->e0, st));
-  int s1 = 0, s2 = 0;
+  int s1 = 0, s2 = 0, stop1 = 0;
   std::vector<int> it1(K, 0), it2(K, 0);
   if (bf16) {
     a.c0 = h0;
     a.c1 = h1;
     k16.init<<<1, 128, 0, st>>>(a);
     ++launches;
-    GPR_TRY(phase(k16, G16, tol_lo, true, &s1, &it1));
+    a.repack_below = 0;
+    GPR_TRY(phase(k16, G16, K, tol_lo, true, &s1, &it1, &stop1));
     a.c0 = c0;
     a.c1 = c1;
     k32.refine_init<<<(unsigned)gpr::ceil_div((long long)m * K, 256), 256, 0, st>>>(
@@ -1081,7 +1288,7 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
     k32.init<<<1, 128, 0, st>>>(a);
     ++launches;
   }
-  GPR_TRY(phase(k32, G32, bf16 ? tol_fix : o.tol, !bf16, &s2, &it2));
+  GPR_TRY(fp32_phase(bf16 ? tol_fix : o.tol, !bf16, &s2, &it2));
   GPR_CUDA(cudaEventRecord(g->e3, st));
   const bool host_out = !gpr::is_device_ptr(any_x);
   float *dout = any_x;
@@ -1109,12 +1316,13 @@ extern "C" int gpr_ppr(gpr_graph *g, int k, const int *h_seeds, float *any_x,
     stats->solve_ms = ms;
     stats->loop_ms = lms;
     stats->gpu_launches = launches;
-    if (s2 > 0) {
-      std::vector<double> last(K);
-      GPR_CUDA(cudaMemcpy(last.data(), res_hist + (size_t)(s2 - 1) * K, sizeof(double) * K,
-                          cudaMemcpyDeviceToHost));
+    if (last_sw > 0) {
+      // the last sweep of the last layout: the vectors that updated longest
+      std::vector<double> last(last_K);
+      GPR_CUDA(cudaMemcpy(last.data(), res_hist + (size_t)(last_sw - 1) * last_K,
+                          sizeof(double) * last_K, cudaMemcpyDeviceToHost));
       double mx = 0;
-      for (int q = 0; q < k; ++q) mx = std::max(mx, last[q]);
+      for (int q = 0; q < std::min(k, last_K); ++q) mx = std::max(mx, last[q]);
       stats->residual = mx;
     }
   }

@@ -69,7 +69,10 @@ typedef struct {
                            that do not exist, so its bounded wait runs out (tests of the
                            GPR_ETIMEOUT path); keep 0 otherwise */
   int form;             /* gpr_form: which sweep sums the rows (FP32 solves of gpr_pagerank) */
-  int pad[5];           /* keep 0 */
+  int ppr_repack;       /* gpr_ppr, FP32 sweeps: once at most half of the vectors are still
+                           updating, continue with those packed into the next narrower
+                           layout (1, the default) or keep the layout (0) */
+  int pad[4];           /* keep 0 */
 } gpr_pr_opts;
 
 /* Sweep forms of gpr_pagerank (FP32).  Both compute the reference's

@@ -142,3 +142,67 @@ def test_ppr_barrier_wait_is_bounded(G, O):
     ref, ref_it = O.ppr_f64(rp, col, od, seeds, tol=1e-6, max_iter=100)
     assert np.all(l1_per_vector(x, ref) <= 1e-5)
     assert np.all(np.abs(it - ref_it) <= 1)
+
+
+def mixed_seeds(O, rp, od, k, seed):
+    """k seeds, about half on vertices without out-edges (their vector keeps
+    its mass at the seed and stops after one sweep), the rest on vertices with
+    in- and out-edges: the active set halves after the first sweep."""
+    rng = np.random.default_rng(seed)
+    dang = np.flatnonzero(od == 0)
+    live = np.flatnonzero((np.diff(rp) > 0) & (od > 0))
+    n_dead = k // 2 + 1 if k >= 16 else 0
+    return np.concatenate([rng.choice(dang, n_dead), rng.choice(live, k - n_dead)]).astype(np.int32)
+
+
+@pytest.mark.parametrize("k", [16, 32, 128])
+@pytest.mark.parametrize("loop", ["persistent", "graph"])
+def test_ppr_packing_matches_unpacked(G, O, k, loop):
+    """Once at most half of the vectors are still updating, the solve goes on
+    with those packed into the next narrower layout (gpr_pr_opts.ppr_repack,
+    on by default).  The narrower layout sums each row in another order, so
+    against the unpacked solve the results agree within rounding (1e-6 per
+    entry, sweeps within one); both meet the FP64 oracle's bar."""
+    lp = G.LOOP_GRAPH if loop == "graph" else G.LOOP_PERSISTENT
+    rp, col, od = O.rmat_graph(13, 8, seed=41)
+    seeds = mixed_seeds(O, rp, od, k, 5)
+    ref, ref_it = O.ppr_f64(rp, col, od, seeds, tol=1e-6, max_iter=100)
+    with G.Graph(rp, col, od, batched=True) as g:
+        xa, ita, sta = g.ppr(seeds, tol=1e-6, max_iter=100, loop=lp)
+        xb, itb, stb = g.ppr(seeds, tol=1e-6, max_iter=100, loop=lp, ppr_repack=False)
+        xc, itc, stc = g.ppr(seeds, tol=1e-6, max_iter=100, loop=lp)
+    for x, it in ((xa, ita), (xb, itb)):
+        assert np.all(l1_per_vector(x, ref) <= 1e-5)
+        assert np.all(np.abs(it - ref_it) <= 1)
+    assert np.all(np.abs(ita - itb) <= 1)
+    assert np.abs(xa - xb).max() <= 1e-6
+    # packing launched its pack / unpack kernels; repeated solves are identical
+    assert sta.gpu_launches > stb.gpu_launches
+    np.testing.assert_array_equal(xa, xc)
+    np.testing.assert_array_equal(ita, itc)
+
+
+def test_ppr_packing_in_the_bf16_refinement(G, O):
+    rp, col, od = O.rmat_graph(12, 8, seed=42)
+    seeds = mixed_seeds(O, rp, od, 32, 6)
+    fixed, _ = O.ppr_f64(rp, col, od, seeds, tol=1e-15, max_iter=3000)
+    with G.Graph(rp, col, od, batched=True) as g:
+        xa, ita, sta = g.ppr(seeds, tol=1e-6, max_iter=200, precision=G.PREC_BF16)
+        xb, itb, stb = g.ppr(seeds, tol=1e-6, max_iter=200, precision=G.PREC_BF16,
+                             ppr_repack=False)
+    assert sta.refine_iterations > 0
+    assert np.all(l1_per_vector(xa, fixed) <= 1e-5)
+    assert np.abs(xa - xb).max() <= 1e-6 and np.all(np.abs(ita - itb) <= 1)
+
+
+def test_ppr_packing_with_a_sweep_cap(G, O):
+    """The sweep budget is shared by the layouts: a capped solve stops at
+    max_iter sweeps in total, as the unpacked one does."""
+    rp, col, od = O.rmat_graph(12, 8, seed=43)
+    seeds = mixed_seeds(O, rp, od, 32, 7)
+    with G.Graph(rp, col, od, batched=True) as g:
+        xa, ita, sta = g.ppr(seeds, tol=1e-9, max_iter=9)
+        xb, itb, stb = g.ppr(seeds, tol=1e-9, max_iter=9, ppr_repack=False)
+    assert sta.iterations == stb.iterations == 9
+    np.testing.assert_array_equal(ita, itb)
+    assert np.abs(xa - xb).max() <= 1e-6
