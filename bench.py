@@ -275,7 +275,8 @@ def run_ours(args):
         tuned = G.tune_graph(csr.rowptr, csr.col, csr.third, m=m, nnz=nnz, cache=args.tune_cache,
                              sweeps=5)
         layout = {k: tuned[k] for k in ("sell_max", "chunk", "chunk_min", "hot_entries",
-                                        "blocked", "block_rows", "tile_words")}
+                                        "blocked", "block_rows", "tile_words",
+                                        "blocked_long")}
         variant = tuned["variant"]
         log(f"[ours] tuned: {tuned}")
     blocked = bool(layout.get("blocked"))

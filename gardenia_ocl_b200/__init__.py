@@ -47,7 +47,7 @@ class PrOptions(C.Structure):
 class LayoutOptions(C.Structure):
     _fields_ = [("sell_max", C.c_int), ("chunk", C.c_int), ("chunk_min", C.c_int),
                 ("hot_entries", C.c_int), ("flags", C.c_int), ("block_rows", C.c_int),
-                ("tile_words", C.c_int), ("reserved", C.c_int * 1)]
+                ("tile_words", C.c_int), ("blocked_long", C.c_int)]
 
 
 class PrStats(C.Structure):
@@ -71,7 +71,7 @@ class TuneResult(C.Structure):
         return {"sell_max": lo.sell_max, "chunk": lo.chunk, "chunk_min": lo.chunk_min,
                 "hot_entries": lo.hot_entries, "blocked": bool(lo.flags & LAYOUT_BLOCKED),
                 "block_rows": lo.block_rows, "tile_words": lo.tile_words,
-                "variant": self.variant,
+                "blocked_long": lo.blocked_long, "variant": self.variant,
                 "from_cache": bool(self.from_cache), "candidates": self.candidates,
                 "ms_per_sweep": self.ms_per_sweep,
                 "default_ms_per_sweep": self.default_ms_per_sweep,
@@ -255,7 +255,7 @@ class Graph:
 
     def __init__(self, rowptr, col, outdeg, m=None, nnz=None, sell_max=0, chunk=0, chunk_min=0,
                  hot_entries=0, batched=False, push=False, blocked=False, block_rows=0,
-                 tile_words=0):
+                 tile_words=0, blocked_long=0):
         L = lib()
         m = int(len(rowptr) - 1) if m is None else int(m)
         nnz = int(len(col)) if nnz is None else int(nnz)
@@ -265,7 +265,8 @@ class Graph:
         h = C.c_void_p()
         lo = LayoutOptions(int(sell_max), int(chunk), int(chunk_min), int(hot_entries),
                            (LAYOUT_BATCHED if batched else 0) | (LAYOUT_PUSH if push else 0) |
-                           (LAYOUT_BLOCKED if blocked else 0), int(block_rows), int(tile_words))
+                           (LAYOUT_BLOCKED if blocked else 0), int(block_rows), int(tile_words),
+                           int(blocked_long))
         _check(L.gpr_graph_create_ex(m, nnz, pr, pc, pd, C.byref(lo), C.byref(h)))
         self._h, self.m, self.nnz = h, m, nnz
         self.last_stats = None
@@ -734,7 +735,7 @@ def tune_graph(rowptr, col, outdeg, m=None, nnz=None, cache=None, sweeps=5) -> d
     """Layout (exact order or blocked, bins, hot prefix) and kernel variant for
     this graph's in-degree distribution (gpr_tune_graph).  Pass the layout
     keys (sell_max, chunk, chunk_min, hot_entries, blocked, block_rows,
-    tile_words) to ``Graph(...)`` and ``variant`` to ``pagerank``; ``cache``:
+    tile_words, blocked_long) to ``Graph(...)`` and ``variant`` to ``pagerank``; ``cache``:
     path of the text cache (or None)."""
     m = int(len(rowptr) - 1) if m is None else int(m)
     nnz = int(len(col)) if nnz is None else int(nnz)

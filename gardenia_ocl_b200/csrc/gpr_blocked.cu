@@ -5,9 +5,9 @@
 // sources of consecutive gathers are unrelated, so on a large power-law graph
 // nearly every gather outside the shared-memory hot prefix is its own L2
 // request (one request per edge is the bound of the exact-order kernel).
-// Here the rows with at most chunk_min in-edges (the rows the exact-order
-// kernel puts in SELL slices) are cut into blocks of R consecutive rows of
-// the relabelled order, and the edges of each block are sorted by SOURCE: a
+// Here the rows with at most long_min in-edges (long_min >= chunk_min: every
+// row the exact-order kernel puts in SELL slices, and the chunked rows up to
+// long_min) are cut into blocks of R consecutive rows of the relabelled order, and the edges of each block are sorted by SOURCE: a
 // warp's 32 gathers then fall on one or two 128-byte lines, and a block's
 // edges fetch each contribution line about once (RMAT scale 24, R = 12288:
 // ~0.16 sectors per edge instead of ~0.64 requests).  The sums are formed in
@@ -24,8 +24,9 @@
 //            at most tile_slots words and kTileRuns runs (one CTA's unit), in
 //            descending size (the CTA queue hands out the heaviest first)
 //   blocks   {row0, nrows, tiles, 0}
-// Rows of heavier in-degree (chunked) and rows without in-edges keep the
-// exact-order layout's work units.
+// Rows of heavier in-degree (the first row0 rows, chunked) and rows without
+// in-edges keep the exact-order layout's work units: the chunks of rows
+// [0, row0) are the first row_cbeg[row0] chunks of the exact-order layout.
 //
 // Construction: every in-edge of a blocked row gets the key (block << 32 |
 // source) and the value (row - row0); one radix sort orders them; the group
@@ -42,13 +43,23 @@ namespace gpr {
 
 namespace {
 
+// In-degrees of the rows [0, n) of the relabelled order.
+__global__ void k_new_degrees(int n, const int *__restrict__ perm, const int *__restrict__ rowptr,
+                              int *deg) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < n) {
+    const int o = perm[r];
+    deg[r] = rowptr[o + 1] - rowptr[o];
+  }
+}
+
 __global__ void k_inverse(int m, const int *__restrict__ perm, int *inv) {
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < m) inv[perm[i]] = i;
 }
 
 // One warp per original row: the keys and values of its in-edges when its
-// new label falls in [n_long, n_nz); other edges get the key ~0 (sorted last).
+// new label falls in [row0, n_nz); other edges get the key ~0 (sorted last).
 __global__ void k_block_keys(int m, const int *__restrict__ rowptr, const int *__restrict__ col,
                              const int *__restrict__ inv, int n_long, int n_nz, int R,
                              unsigned long long *key, unsigned *val) {
@@ -124,14 +135,67 @@ void free_blocked_layout(BlockedLayout *B) {
   *B = BlockedLayout();
 }
 
+int blocked_split(const PrLayout &L, const int *d_rowptr, int long_min, int R, int *row0,
+                  int *n_chunks, long long *long_words, cudaStream_t st) {
+  *row0 = 0;
+  *n_chunks = 0;
+  *long_words = 0;
+  if (L.n_long == 0) return GPR_OK;
+  // in-degrees of the chunkable rows and of the R rows after them
+  const int n = (int)std::min<long long>(L.n_nz, (long long)L.n_long + R);
+  int *d_deg = nullptr;
+  int rc = dalloc(&d_deg, (size_t)n, "blocked: heavy rows");
+  if (rc != GPR_OK) return rc;
+  std::vector<int> deg((size_t)n);
+  k_new_degrees<<<grid_of(n), 256, 0, st>>>(n, L.perm, d_rowptr, d_deg);
+  rc = GPR_CUDA_RC(cudaGetLastError());
+  if (rc == GPR_OK)
+    rc = GPR_CUDA_RC(cudaMemcpyAsync(deg.data(), d_deg, sizeof(int) * (size_t)n,
+                                     cudaMemcpyDeviceToHost, st));
+  if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaStreamSynchronize(st));
+  dfree(d_deg);
+  if (rc != GPR_OK) return rc;
+  // The chunked rows are a prefix (the order is by descending in-degree).
+  // With long_min > 0: the rows above long_min in-edges.  Otherwise the rows
+  // that would hold more than 1/8 of the edges of a block starting at them:
+  // their additions would queue on one shared-memory word (a star's hub),
+  // which chunks sum without contention.
+  int cnt = 0;
+  if (long_min > 0) {
+    while (cnt < L.n_long && deg[cnt] > long_min) ++cnt;
+  } else {
+    long long win = 0;  // in-edges of rows [cnt, cnt + R)
+    for (int j = 0; j < std::min(n, R); ++j) win += deg[j];
+    while (cnt < L.n_long && 8LL * deg[cnt] > win) {
+      win -= deg[cnt];
+      if (cnt + R < n) win += deg[cnt + R];
+      ++cnt;
+    }
+  }
+  int cb = 0;
+  long long lw = 0;
+  rc = GPR_CUDA_RC(cudaMemcpyAsync(&cb, L.row_cbeg + cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
+  if (rc == GPR_OK)
+    rc = GPR_CUDA_RC(cudaMemcpyAsync(&lw, L.long_ptr + cnt, sizeof(long long),
+                                     cudaMemcpyDeviceToHost, st));
+  if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaStreamSynchronize(st));
+  if (rc != GPR_OK) return rc;
+  *row0 = cnt;
+  *n_chunks = cb;
+  *long_words = lw;
+  return GPR_OK;
+}
+
 int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
-                         const PrLayout &L, int R, int tile_slots, BlockedLayout *B,
-                         cudaStream_t st) {
+                         const PrLayout &L, int row0, int n_chunks, int R, int tile_slots,
+                         BlockedLayout *B, cudaStream_t st) {
   *B = BlockedLayout();
   B->R = R;
   B->tile_slots = tile_slots;
-  const int n_rows = L.n_nz - L.n_long;
-  if (R < 1 || R > kBlockedMaxRows || tile_slots < kRunWords) {
+  B->row0 = row0;
+  B->n_chunks = n_chunks;
+  const int n_rows = L.n_nz - row0;
+  if (R < 1 || R > kBlockedMaxRows || tile_slots < kRunWords || row0 < 0 || row0 > L.n_long) {
     set_error("blocked layout: block rows %d must be in [1, %d], tile words %d >= %d", R,
               kBlockedMaxRows, tile_slots, kRunWords);
     return GPR_EINVAL;
@@ -159,7 +223,7 @@ int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d
       (rc = dalloc(&v1, (size_t)nnz, "blocked: rows")) != GPR_OK)
     return fail(rc);
   k_inverse<<<grid_of(m), 256, 0, st>>>(m, L.perm, inv);
-  k_block_keys<<<grid_of((long long)m * 32), 256, 0, st>>>(m, d_rowptr, d_col, inv, L.n_long,
+  k_block_keys<<<grid_of((long long)m * 32), 256, 0, st>>>(m, d_rowptr, d_col, inv, row0,
                                                            L.n_nz, R, k0, v0);
   if ((rc = GPR_CUDA_RC(cudaGetLastError())) != GPR_OK) return fail(rc);
   // Sort on (block, source): bits of the source ids, then of the block ids
@@ -267,8 +331,8 @@ int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d
   std::vector<int4> tiles;
   std::vector<int4> blocks(B->n_blocks);
   for (int b = 0; b < B->n_blocks; ++b) {
-    const int row0 = L.n_long + b * R;
-    blocks[b] = make_int4(row0, std::min(R, L.n_nz - row0), 0, 0);
+    const int r0 = row0 + b * R;
+    blocks[b] = make_int4(r0, std::min(R, L.n_nz - r0), 0, 0);
   }
   runs.reserve((size_t)(n_edges / kRunWords) + ng + 1);
   long long pos = 0;

@@ -132,20 +132,29 @@ constexpr int kTileWordsDefault = 1 << 18;
 
 struct BlockedLayout {
   int R = 0, tile_slots = 0;
+  int row0 = 0;      // first blocked row; rows [0, row0) are summed in chunks
+  int n_chunks = 0;  // chunks of rows [0, row0): a prefix of the exact-order chunks
   int n_blocks = 0, n_tiles = 0;
   long long n_runs = 0, slots = 0, edges = 0;
   unsigned *entry = nullptr;             // [slots]
   uint2 *runs = nullptr;                 // [n_runs] {first word, segment << 16 | words}
   int4 *tiles = nullptr;                 // [n_tiles] {block, run0, run1, words}
   int4 *blocks = nullptr;                // [n_blocks] {row0, nrows, tiles, 0}
-  unsigned long long *gacc = nullptr;    // [n_nz - n_long] sums of multi-tile blocks
+  unsigned long long *gacc = nullptr;    // [n_nz - row0] sums of multi-tile blocks
   int *bcnt = nullptr;                   // [n_blocks] tiles done in the current sweep
   long long device_bytes = 0;
 };
 
+// Rows of the blocked form that stay chunked: the first *row0 rows of the
+// exact-order layout's chunked rows [0, L.n_long), either those with more than
+// long_min in-edges or, when long_min is 0, those holding more than 1/8 of the
+// in-edges of the R rows that start at them; their *n_chunks chunks and the
+// *long_words padded entries of those rows.  Synchronizes st.
+int blocked_split(const PrLayout &L, const int *d_rowptr, int long_min, int R, int *row0,
+                  int *n_chunks, long long *long_words, cudaStream_t st);
 int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
-                         const PrLayout &L, int R, int tile_slots, BlockedLayout *B,
-                         cudaStream_t st);
+                         const PrLayout &L, int row0, int n_chunks, int R, int tile_slots,
+                         BlockedLayout *B, cudaStream_t st);
 void free_blocked_layout(BlockedLayout *B);
 
 // Validates a device CSR (rowptr[0] = 0, monotone, rowptr[m] = nnz, every
@@ -271,7 +280,7 @@ struct gpr_graph {
   // grid and co-residency, the tile-queue heads and the largest |score|.
   gpr::BlockedLayout B;
   bool has_blocked = false, blocked_ok = false;
-  int grid_blocked = 0;
+  int grid_blocked = 0, blocked_ctas = 1;  // blocked-form CTAs: total, per SM
   int *tq = nullptr;
   unsigned *fx_max = nullptr;
   alignas(8) unsigned char loop_args[512] = {0};

@@ -66,7 +66,8 @@ struct PrArgs {
   int batch;              // units per work-queue grab
   unsigned long long cond;  // graph mode: while-node condition handle (0: none)
   // blocked form (gpr_blocked.cu): tiles of source-ordered entries per block
-  int n_tiles;
+  int n_tiles, acc_rows;  // acc_rows: high words of the shared accumulators start here
+  int blk_row0;           // first blocked row (rows before it are chunked)
   const int4 *tiles;
   const int4 *blocks;
   const uint2 *runs;
@@ -387,35 +388,36 @@ __device__ __forceinline__ float gather_entry(const float *cin, unsigned segbase
 
 // Rows row0 + i, i < nrows, from their fixed-point sums (shared accumulators
 // or, when `global`, the cross-tile accumulators, which are cleared); eight
-// rows per thread are loaded before any is updated.
+// rows per thread are loaded before any is updated.  NT threads per CTA.
+template <int NT>
 __device__ __forceinline__ double blocked_finalize(const PrArgs &a, float *cout, int row0,
                                                    int nrows, const unsigned *acc, bool global,
                                                    const Policies &pol) {
   double err = 0.0;
-  for (int i0 = threadIdx.x; i0 < nrows; i0 += 8 * 1024) {
+  for (int i0 = threadIdx.x; i0 < nrows; i0 += 8 * NT) {
     long long x[8];
     float so[8];
     int od[8];
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const int i = i0 + 1024 * k;
+      const int i = i0 + NT * k;
       x[k] = 0;
       so[k] = 0.f;
       od[k] = 1;
       if (i < nrows) {
         const int r = row0 + i;
-        x[k] = global ? (long long)__ldcg(a.gacc + (r - a.n_long))
-                      : (long long)(((unsigned long long)acc[kBlockedMaxRows + i] << 32) | acc[i]);
+        x[k] = global ? (long long)__ldcg(a.gacc + (r - a.blk_row0))
+                      : (long long)(((unsigned long long)acc[a.acc_rows + i] << 32) | acc[i]);
         so[k] = ld_f32_stream(a.s + r, pol.stream);
         od[k] = ld_s32_stream(a.outdeg + r, pol.stream);
       }
     }
 #pragma unroll
     for (int k = 0; k < 8; ++k) {
-      const int i = i0 + 1024 * k;
+      const int i = i0 + NT * k;
       if (i < nrows) {
         const int r = row0 + i;
-        if (global) a.gacc[r - a.n_long] = 0ull;
+        if (global) a.gacc[r - a.blk_row0] = 0ull;
         const float sum = (float)((double)x[k] * a.fx_inv);
         err += row_update(a, r, sum, so[k], od[k], cout, pol);
       }
@@ -426,24 +428,24 @@ __device__ __forceinline__ double blocked_finalize(const PrArgs &a, float *cout,
 
 // One tile: zero the block's accumulators, add the tile's runs, then finalize
 // the block (single tile) or add into the cross-tile accumulators.
-template <int PV>
+template <int PV, int NT>
 __device__ __forceinline__ double blocked_tile(const PrArgs &a, const float *cin, float *cout,
-                                               int t, unsigned *acc, uint2 *s_runs, int *s_next,
-                                               int *s_last, const Policies &pol) {
+                                               int t, unsigned *acc, int *s_next, int *s_last,
+                                               const Policies &pol) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int4 td = a.tiles[t];
   const int4 bd = a.blocks[td.x];
   const int nr = td.z - td.y;
-  for (int i = threadIdx.x; i < nr; i += 1024) s_runs[i] = a.runs[td.y + i];
-  for (int i = threadIdx.x; i < bd.y; i += 1024) {
+  for (int i = threadIdx.x; i < bd.y; i += NT) {
     acc[i] = 0u;
-    acc[kBlockedMaxRows + i] = 0u;
+    acc[a.acc_rows + i] = 0u;
   }
-  if (threadIdx.x == 0) *s_next = 32;
+  if (threadIdx.x == 0) *s_next = NT / 32;
   __syncthreads();
   int r = warp;
+  uint2 rd = make_uint2(0u, 0u);
+  if (r < nr) rd = __ldg(a.runs + td.y + r);
   while (r < nr) {
-    const uint2 rd = s_runs[r];
     int rn = 0;
     if (lane == 0) rn = atomicAdd(s_next, 1);
     const unsigned segbase = (rd.y >> 16) << 16;
@@ -453,6 +455,10 @@ __device__ __forceinline__ double blocked_tile(const PrArgs &a, const float *cin
 #pragma unroll
     for (int i = 0; i < PV; ++i)
       q[i] = ld_entry4(a.entry + rd.x + 128 * i + 4 * lane, 128 * i + 4 * lane < len, pol.stream);
+    // the next run's descriptor is fetched while this run's loads are in flight
+    rn = __shfl_sync(kFull, rn, 0);
+    uint2 nd = make_uint2(0u, 0u);
+    if (rn < nr) nd = __ldg(a.runs + td.y + rn);
 #pragma unroll
     for (int i = 0; i < PV; ++i) {
       use_u32(q[i].x); use_u32(q[i].y); use_u32(q[i].z); use_u32(q[i].w);
@@ -486,19 +492,20 @@ __device__ __forceinline__ double blocked_tile(const PrArgs &a, const float *cin
 #pragma unroll
       for (int i = 0; i < 8; ++i) {
         const unsigned hc = hw[i] + (old[i] + lo[i] < old[i] ? 1u : 0u);
-        if (wv[h + i] != 0xFFFFFFFFu && hc) atomicAdd(acc + kBlockedMaxRows + (wv[h + i] & 0xFFFFu), hc);
+        if (wv[h + i] != 0xFFFFFFFFu && hc) atomicAdd(acc + a.acc_rows + (wv[h + i] & 0xFFFFu), hc);
       }
     }
-    r = __shfl_sync(kFull, rn, 0);
+    r = rn;
+    rd = nd;
   }
   __syncthreads();
   double err = 0.0;
   if (bd.z == 1) {
-    err = blocked_finalize(a, cout, bd.x, bd.y, acc, false, pol);
+    err = blocked_finalize<NT>(a, cout, bd.x, bd.y, acc, false, pol);
   } else {
-    for (int i = threadIdx.x; i < bd.y; i += 1024) {
-      const unsigned long long x = ((unsigned long long)acc[kBlockedMaxRows + i] << 32) | acc[i];
-      if (x) atomicAdd(a.gacc + (bd.x - a.n_long) + i, x);
+    for (int i = threadIdx.x; i < bd.y; i += NT) {
+      const unsigned long long x = ((unsigned long long)acc[a.acc_rows + i] << 32) | acc[i];
+      if (x) atomicAdd(a.gacc + (bd.x - a.blk_row0) + i, x);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -508,27 +515,28 @@ __device__ __forceinline__ double blocked_tile(const PrArgs &a, const float *cin
     __syncthreads();
     if (*s_last) {
       __threadfence();
-      err = blocked_finalize(a, cout, bd.x, bd.y, acc, true, pol);
+      err = blocked_finalize<NT>(a, cout, bd.x, bd.y, acc, true, pol);
       if (threadIdx.x == 0) a.bcnt[td.x] = 0;
     }
   }
   return err;
 }
 
-// All sweeps of the blocked form in one cooperative launch, one 1024-thread
-// CTA per SM.  Per sweep: CTAs take tiles from a queue (heaviest first; the
+// All sweeps of the blocked form in one cooperative launch, MINB CTAs of NT
+// threads per SM (one of 1024, or two of 512: then one CTA's warps keep
+// gathering while the other's wait at the barrier that closes a tile or
+// finalize its block).  Per sweep: CTAs take tiles from a queue (heaviest first; the
 // next tile is claimed while the current one runs), then warps take the
 // chunks of the rows above chunk_min in-edges, with the first contributions
 // staged in the shared memory the accumulators used, then the zero-in-degree
 // rows (sweeps 0 and 1), then the bounded grid barrier with the residual.
-template <int PV>
-__global__ void __launch_bounds__(1024, 1) k_pr_blocked(PrArgs a) {
-  extern __shared__ unsigned s_acc[];  // [2 * kBlockedMaxRows]: low / high words
-  __shared__ uint2 s_runs[kTileRuns];
+template <int PV, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_pr_blocked(PrArgs a) {
+  extern __shared__ unsigned s_acc[];  // [2 * acc_rows]: low / high words
   __shared__ int s_tile, s_next_tile, s_last, s_next;
   const int lane = threadIdx.x & 31;
-  const long long gw = (long long)blockIdx.x * 32 + (threadIdx.x >> 5);
-  const long long nw = (long long)gridDim.x * 32;
+  const long long gw = (long long)blockIdx.x * (NT / 32) + (threadIdx.x >> 5);
+  const long long nw = (long long)gridDim.x * (NT / 32);
   const Policies pol = make_policies();
   int it = 0;
   while (it < a.max_iter) {
@@ -543,23 +551,26 @@ __global__ void __launch_bounds__(1024, 1) k_pr_blocked(PrArgs a) {
       const int t = s_tile;
       if (t >= a.n_tiles) break;
       if (threadIdx.x == 0) s_next_tile = atomicAdd(a.tq + (it & 1), 1);
-      err += blocked_tile<PV>(a, cin, cout, t, s_acc, s_runs, &s_next, &s_last, pol);
+      err += blocked_tile<PV, NT>(a, cin, cout, t, s_acc, &s_next, &s_last, pol);
     }
-    // chunks of the long rows, the hottest contributions from shared memory
-    float *s_hot = reinterpret_cast<float *>(s_acc);
-    const int n16 = a.hot / 4;
-    const float4 *src = reinterpret_cast<const float4 *>(cin);
-    for (int i = threadIdx.x; i < n16; i += blockDim.x)
-      reinterpret_cast<float4 *>(s_hot)[i] = ld_contrib4(src + i, pol.keep);
-    __syncthreads();
-    const HotGatherGeneric<float> gat{cin, s_hot, a.hot, pol.keep};
-    for (;;) {
-      int u0 = 0;
-      if (lane == 0) u0 = atomicAdd(a.wq + (it & 1), a.batch);
-      u0 = __shfl_sync(kFull, u0, 0);
-      if (u0 >= a.n_chunks) break;
-      const int u1 = min(u0 + a.batch, a.n_chunks);
-      for (int u = u0; u < u1; ++u) err += do_chunk<4>(a, gat, cout, u, lane, pol);
+    // chunks of the heaviest rows, the hottest contributions from shared
+    // memory (none staged when the chunks are few)
+    if (a.n_chunks > 0) {
+      float *s_hot = reinterpret_cast<float *>(s_acc);
+      const int n16 = a.hot / 4;
+      const float4 *src = reinterpret_cast<const float4 *>(cin);
+      for (int i = threadIdx.x; i < n16; i += blockDim.x)
+        reinterpret_cast<float4 *>(s_hot)[i] = ld_contrib4(src + i, pol.keep);
+      __syncthreads();
+      const HotGatherGeneric<float> gat{cin, s_hot, a.hot, pol.keep};
+      for (;;) {
+        int u0 = 0;
+        if (lane == 0) u0 = atomicAdd(a.wq + (it & 1), a.batch);
+        u0 = __shfl_sync(kFull, u0, 0);
+        if (u0 >= a.n_chunks) break;
+        const int u1 = min(u0 + a.batch, a.n_chunks);
+        for (int u = u0; u < u1; ++u) err += do_chunk<4>(a, gat, cout, u, lane, pol);
+      }
     }
     if (it < 2)
       for (long long z = gw; z < a.n_zblk; z += nw) err += do_zero(a, cout, (int)z, lane, it, pol);
@@ -585,6 +596,11 @@ __global__ void k_max_abs(int m, const float *__restrict__ s, unsigned *out) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFull, mx, o));
   if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
+}
+
+// The blocked-form kernel with `ctas` CTAs per SM (1: 1024 threads, 2: 512).
+const void *blocked_kernel(int ctas) {
+  return ctas == 2 ? (const void *)k_pr_blocked<4, 512, 2> : (const void *)k_pr_blocked<4, 1024, 1>;
 }
 
 // One sweep per launch (graph mode).  The sweep index and the done flag live
@@ -857,7 +873,8 @@ void destroy(gpr_graph *g) {
 
 int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
                 const int *any_outdeg, int lane_max, int chunk_min, int chunk, int hot_max,
-                bool keep_csr, bool blocked, int block_rows, int tile_words, gpr_graph *g) {
+                bool keep_csr, bool blocked, int block_rows, int tile_words, int blocked_long,
+                gpr_graph *g) {
   GPR_CUDA(cudaGetDevice(&g->device));
   GPR_CUDA(cudaStreamCreateWithFlags(&g->st, cudaStreamNonBlocking));
   g->own_stream = true;
@@ -921,17 +938,23 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
     // (a multi-tile block adds one 8-byte atomic per row and tile).
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g->device);
-    const long long rows = (long long)g->L.n_nz - g->L.n_long;
-    const long long words = std::max(0LL, nnz - g->L.long_elems);
     if (block_rows == 0)
       block_rows = (int)std::min<long long>(
-          gpr::kBlockedRows, std::max<long long>(256, gpr::ceil_div(rows, 2LL * nsm)));
+          gpr::kBlockedRows,
+          std::max<long long>(256, gpr::ceil_div((long long)g->L.n_nz, 2LL * nsm)));
+    int row0 = 0, n_chunks = 0;
+    long long long_words = 0;
+    rc = gpr::blocked_split(g->L, (const int *)rp,
+                            blocked_long > 0 ? std::max(blocked_long, chunk_min) : 0, block_rows,
+                            &row0, &n_chunks, &long_words, st);
+    const long long words = std::max(0LL, nnz - long_words);
     if (tile_words == 0)
       tile_words = (int)std::min<long long>(
           gpr::kTileWordsDefault,
           std::max<long long>(4096, gpr::ceil_div(words, 6LL * nsm) / 512 * 512));
-    rc = gpr::build_blocked_layout(m, nnz, (const int *)rp, (const int *)cp, g->L, block_rows,
-                                   tile_words, &g->B, st);
+    if (rc == GPR_OK)
+      rc = gpr::build_blocked_layout(m, nnz, (const int *)rp, (const int *)cp, g->L, row0,
+                                     n_chunks, block_rows, tile_words, &g->B, st);
     g->has_blocked = rc == GPR_OK;
   }
   if (orp) gpr::dfree(rp);
@@ -983,16 +1006,36 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
   g->max_grid = g->grid_step;
   for (int v = 0; v < kNumKernels; ++v) g->max_grid = std::max(g->max_grid, g->grid_hot[v]);
   if (g->has_blocked) {
-    // one 1024-thread CTA per SM; shared memory: the accumulators (dynamic)
-    // and the tile's run table (static)
-    const int smem = 8 * gpr::kBlockedMaxRows;
+    // shared memory per CTA: the accumulators (dynamic) and the tile's run
+    // table (static)
+    const int smem = 8 * g->B.R;
+    int smem_sm = 0;
+    GPR_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor,
+                                    g->device));
+    // Two 512-thread CTAs per SM (one gathers while the other closes a tile)
+    // when both fit beside an L1 of about half the SM's 256 KB, else one
+    // 1024-thread CTA: the gathers' L1 line hits are worth more than the
+    // overlap (RMAT scale 24 with 12288-row blocks: 2x slower sweeps with
+    // two CTAs and a 28 KB L1).
+    g->blocked_ctas = g->B.R <= 8192 ? 2 : 1;
     int per_sm = 0;
-    GPR_CUDA(cudaFuncSetAttribute((const void *)k_pr_blocked<4>,
-                                  cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void *)k_pr_blocked<4>,
-                                                           1024, smem));
-    g->blocked_ok = g->coop && per_sm >= 1;
-    g->grid_blocked = sms;
+    for (;;) {
+      // the smallest shared-memory carveout that holds the CTAs: the rest of
+      // the SM's 256 KB stays L1
+      const void *k = blocked_kernel(g->blocked_ctas);
+      cudaFuncAttributes fa;
+      GPR_CUDA(cudaFuncGetAttributes(&fa, k));
+      const long long need = (long long)g->blocked_ctas * (smem + (long long)fa.sharedSizeBytes + 1024);
+      const int carve = (int)std::min<long long>(100, gpr::ceil_div(100 * need, smem_sm));
+      GPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      GPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+      GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+          &per_sm, k, 1024 / g->blocked_ctas, smem));
+      if (per_sm >= g->blocked_ctas || g->blocked_ctas == 1) break;
+      g->blocked_ctas = 1;
+    }
+    g->blocked_ok = g->coop && per_sm >= g->blocked_ctas;
+    g->grid_blocked = sms * g->blocked_ctas;
     g->max_grid = std::max(g->max_grid, g->grid_blocked);
     GPR_TRY(gpr::dalloc(&g->tq, 2, "tile queue"));
     GPR_TRY(gpr::dalloc(&g->fx_max, 1, "largest score"));
@@ -1093,7 +1136,7 @@ int solve_impl(gpr_graph *g, float *d_scores, const gpr_pr_opts &o, int ki, gpr_
     if (B.n_blocks) {
       // clean after an abandoned solve; a completed sweep leaves them clean
       GPR_CUDA(cudaMemsetAsync(B.bcnt, 0, sizeof(int) * B.n_blocks, st));
-      GPR_CUDA(cudaMemsetAsync(B.gacc, 0, 8 * (size_t)(g->L.n_nz - g->L.n_long), st));
+      GPR_CUDA(cudaMemsetAsync(B.gacc, 0, 8 * (size_t)(g->L.n_nz - B.row0), st));
     }
   }
   PrArgs a = make_args(g, o, ki);
@@ -1107,9 +1150,13 @@ int solve_impl(gpr_graph *g, float *d_scores, const gpr_pr_opts &o, int ki, gpr_
     a.bcnt = B.bcnt;
     a.tq = g->tq;
     a.bar_expect = g->grid_blocked;
-    a.hot = std::min(hot_entries(g, 0), 2 * gpr::kBlockedMaxRows) / 4 * 4;
-    a.batch = (int)std::max<long long>(
-        1, (long long)g->L.n_chunks / ((long long)g->grid_blocked * 32 * 4));
+    a.acc_rows = B.R;
+    a.blk_row0 = B.row0;
+    a.n_chunks = B.n_chunks;
+    // stage the hottest contributions only when every warp has chunks to take
+    const long long warps = (long long)g->grid_blocked * (32 / g->blocked_ctas);
+    a.hot = B.n_chunks >= 4 * warps ? std::min(hot_entries(g, 0), 2 * B.R) / 4 * 4 : 0;
+    a.batch = (int)std::max<long long>(1, (long long)B.n_chunks / (warps * 4));
   }
   if (o.reserved[0] > 0) a.bar_expect += o.reserved[0];  // test hook: a barrier nobody completes
   int launches = 0;
@@ -1143,9 +1190,10 @@ int solve_impl(gpr_graph *g, float *d_scores, const gpr_pr_opts &o, int ki, gpr_
   GPR_CUDA(cudaEventRecord(g->e2, st));
   if (o.max_iter > 0 && blocked) {
     void *args[] = {&a};
-    cudaError_t e = cudaLaunchCooperativeKernel((const void *)k_pr_blocked<4>,
-                                                dim3(g->grid_blocked), dim3(1024), args,
-                                                8 * (size_t)gpr::kBlockedMaxRows, st);
+    cudaError_t e = cudaLaunchCooperativeKernel(blocked_kernel(g->blocked_ctas),
+                                                dim3(g->grid_blocked),
+                                                dim3(1024 / g->blocked_ctas), args,
+                                                8 * (size_t)B.R, st);
     if (e == cudaErrorCooperativeLaunchTooLarge) {
       cudaGetLastError();
       return kBlockedFallback;
@@ -1325,15 +1373,17 @@ int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr, const int *
   if (lopts && lopts->chunk_min) chunk_min = lopts->chunk_min;
   if (lopts && lopts->hot_entries) hot_max = lopts->hot_entries;
   int block_rows = 0, tile_words = 0;  // 0: sized to the graph at creation
+  int blocked_long = 0;  // 0: rows that would crowd a block are chunked
   if (lopts) block_rows = lopts->block_rows;
   if (lopts) tile_words = lopts->tile_words;
+  if (lopts && lopts->blocked_long) blocked_long = lopts->blocked_long;
   if (lane_max < 1 || lane_max > 1024 || chunk < 128 || chunk % 128 != 0 || chunk_min < 1 ||
       hot_max < 4 || hot_max > gpr::kHotMax || hot_max % 4 != 0 || block_rows < 0 ||
       block_rows > gpr::kBlockedMaxRows || tile_words < 0 ||
-      (tile_words > 0 && tile_words < gpr::kRunWords)) {
+      (tile_words > 0 && tile_words < gpr::kRunWords) || blocked_long < 0) {
     gpr::set_error("gpr_graph_create_ex: invalid layout options (lane_max %d, chunk %d, "
-                   "chunk_min %d, hot_entries %d, block_rows %d, tile_words %d)", lane_max, chunk,
-                   chunk_min, hot_max, block_rows, tile_words);
+                   "chunk_min %d, hot_entries %d, block_rows %d, tile_words %d, blocked_long %d)",
+                   lane_max, chunk, chunk_min, hot_max, block_rows, tile_words, blocked_long);
     return GPR_EINVAL;
   }
   if (!out) {
@@ -1356,7 +1406,7 @@ int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr, const int *
   const bool keep_csr = lopts && (lopts->flags & (GPR_LAYOUT_BATCHED | GPR_LAYOUT_PUSH));
   const bool blocked = lopts && (lopts->flags & GPR_LAYOUT_BLOCKED);
   int rc = create_impl(m, nnz, any_rowptr, any_col, any_outdeg, lane_max, chunk_min, chunk,
-                       hot_max, keep_csr, blocked, block_rows, tile_words, g);
+                       hot_max, keep_csr, blocked, block_rows, tile_words, blocked_long, g);
   if (rc != GPR_OK) {
     destroy(g);
     return rc;

@@ -14,8 +14,8 @@
 // edges at creation and pays on large graphs); then coordinate descent over
 // the chosen form's knobs: for the exact order the kernel variant, hot
 // prefix, lanes-per-row bound and chunk threshold / size; for the blocked
-// form the rows per block, words per tile, chunk threshold / size and hot
-// prefix.  Each candidate is timed as the best of kReps solves of exactly
+// form the rows per block, words per tile and the in-degree above which
+// rows are summed in chunks rather than in blocks.  Each candidate is timed as the best of kReps solves of exactly
 // `sweeps` sweeps (tol 0), device time of the sweep loop
 // (gpr_pr_stats.loop_ms), and taken only when at least kMargin faster than the
 // current pick.  The batch tuner groups graphs by signature and tunes one
@@ -24,7 +24,7 @@
 //
 // Cache file: one line per entry, later lines override earlier ones:
 //   <signature> <sell_max> <chunk> <chunk_min> <hot_entries> <variant> <ms_per_sweep>
-//       [<flags> <block_rows> <tile_words>]
+//       [<flags> <block_rows> <tile_words> [<blocked_long>]]
 #include <math.h>
 #include <stdio.h>
 #include <string.h>
@@ -46,11 +46,13 @@ constexpr int kDefSell = 64, kDefChunk = 4096, kDefChunkMin = 4096, kDefHot = 32
 struct Cfg {
   int sell_max = kDefSell, chunk = kDefChunk, chunk_min = kDefChunkMin, hot = kDefHot,
       variant = 0;
-  int flags = 0, block_rows = 0, tile_words = 0;  // blocked form (0: library defaults)
+  // blocked form (0: library defaults)
+  int flags = 0, block_rows = 0, tile_words = 0, blocked_long = 0;
   bool operator==(const Cfg &o) const {
     return sell_max == o.sell_max && chunk == o.chunk && chunk_min == o.chunk_min &&
            hot == o.hot && variant == o.variant && flags == o.flags &&
-           block_rows == o.block_rows && tile_words == o.tile_words;
+           block_rows == o.block_rows && tile_words == o.tile_words &&
+           blocked_long == o.blocked_long;
   }
 };
 
@@ -82,10 +84,10 @@ std::map<std::string, std::pair<Cfg, double>> load_cache(const char *path) {
     char key[128];
     Cfg x;
     double ms = 0;
-    const int n = sscanf(line, "%127s %d %d %d %d %d %lf %d %d %d", key, &x.sell_max, &x.chunk,
+    const int n = sscanf(line, "%127s %d %d %d %d %d %lf %d %d %d %d", key, &x.sell_max, &x.chunk,
                          &x.chunk_min, &x.hot, &x.variant, &ms, &x.flags, &x.block_rows,
-                         &x.tile_words);
-    if (n == 7 || n == 10) c[key] = {x, ms};
+                         &x.tile_words, &x.blocked_long);
+    if (n == 7 || n == 10 || n == 11) c[key] = {x, ms};
   }
   fclose(f);
   return c;
@@ -95,8 +97,8 @@ void save_cache(const char *path, const std::string &key, const Cfg &x, double m
   if (!path) return;
   FILE *f = fopen(path, "a");
   if (!f) return;
-  fprintf(f, "%s %d %d %d %d %d %.6f %d %d %d\n", key.c_str(), x.sell_max, x.chunk, x.chunk_min,
-          x.hot, x.variant, ms, x.flags, x.block_rows, x.tile_words);
+  fprintf(f, "%s %d %d %d %d %d %.6f %d %d %d %d\n", key.c_str(), x.sell_max, x.chunk,
+          x.chunk_min, x.hot, x.variant, ms, x.flags, x.block_rows, x.tile_words, x.blocked_long);
   fclose(f);
 }
 
@@ -110,6 +112,7 @@ gpr_layout_opts to_layout(const Cfg &x) {
   l.flags = x.flags;
   l.block_rows = x.block_rows;
   l.tile_words = x.tile_words;
+  l.blocked_long = x.blocked_long;
   return l;
 }
 
@@ -241,22 +244,16 @@ int gpr_tune_graph(int m, long long nnz, const int *any_rowptr, const int *any_c
   xb.flags = GPR_LAYOUT_BLOCKED;
   const double tb = time(xb);
   if (tb < best * (1.0 - kMargin)) {
-    // the blocked form: its knobs, then the chunked rows' and the hot prefix
+    // the blocked form: its knobs (rows per block also decide one or two
+    // CTAs per SM), then which heavy rows are summed in chunks
     x = xb;
     best = tb;
     descend(&x, &best, std::vector<int>{6144, 8192},
             [](Cfg *y, int v) { y->block_rows = v; }, time);
     descend(&x, &best, std::vector<int>{131072, 524288},
             [](Cfg *y, int v) { y->tile_words = v; }, time);
-    descend(&x, &best,
-            std::vector<std::pair<int, int>>{{16384, 4096}, {1024, 1024}},
-            [](Cfg *y, std::pair<int, int> v) {
-              y->chunk_min = v.first;
-              y->chunk = v.second;
-            },
-            time);
-    descend(&x, &best, std::vector<int>{8192, 16384},
-            [](Cfg *y, int v) { y->hot = v; }, time);
+    descend(&x, &best, std::vector<int>{16384, 1 << 30},
+            [](Cfg *y, int v) { y->blocked_long = v; }, time);
   } else {
     descend(&x, &best, std::vector<int>{1, 2, 3, 4, 5, 6, 7},
             [](Cfg *y, int v) { y->variant = v; }, time);

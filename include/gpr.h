@@ -143,7 +143,11 @@ typedef struct {
                      256 .. 12288) */
   int tile_words; /* blocked form: most entry words per tile, >= 512 (default: about
                      edges / (6 SMs), 4096 .. 262144) */
-  int reserved[1];
+  int blocked_long; /* blocked form: rows with more in-edges than this are summed in chunks,
+                       the others in blocks; values below chunk_min act as chunk_min.
+                       0 (default): a row is chunked when it holds more than 1/8 of the
+                       in-edges of the block_rows rows that start at it (a hub whose
+                       additions would queue on one shared-memory word) */
 } gpr_layout_opts;
 int gpr_graph_create_ex(int m, long long nnz, const int *any_rowptr,
                         const int *any_col, const int *any_outdeg,

@@ -1,7 +1,9 @@
 """The blocked form of the PageRank sweep (GPR_LAYOUT_BLOCKED, GPR_FORM_BLOCKED).
 
-Rows with at most chunk_min in-edges are summed block by block from
-source-ordered edges in 64-bit fixed point: each contribution c (FP32) becomes
+Rows are summed block by block from source-ordered edges in 64-bit fixed
+point, except rows with more than chunk_min in-edges that either exceed
+blocked_long or (blocked_long 0, the default) would hold more than 1/8 of the
+edges of their block: each contribution c (FP32) becomes
 rint(c * 2^S), the row's integers are added exactly, and the sum is
 (float)(x * 2^-S).  The update is the reference's (src/pr/omp_base.cc:39, 26).
 So the form is pinned exactly: on graphs without chunked rows every sweep is
@@ -106,12 +108,50 @@ def test_blocked_matches_reference(G, O, scale, tol):
     assert l1_fix <= 1e-5 if tol <= 1e-6 else True
 
 
+@pytest.mark.parametrize("maker", [lambda: star(20000), degree_ladder], ids=["star", "ladder"])
+def test_heavy_rows_in_blocks_follow_the_fixed_point_recurrence(G, O, maker):
+    """Rows the exact-order layout cuts into chunks (chunk_min 1024) are summed
+    in blocks when they have at most blocked_long in-edges: every sweep is
+    still the fixed-point recurrence, bit for bit, hub rows included (a hub
+    that crowds its block only costs time)."""
+    rp, col, od = maker()
+    m = len(rp) - 1
+    assert np.diff(rp).max() > 1024
+    s0 = np.full(m, np.float32(1.0) / np.float32(m), dtype=np.float32)
+    for layout in (dict(block_rows=300, tile_words=1024), {}):
+        with G.Graph(rp, col, od, chunk=512, chunk_min=1024, blocked=True,
+                     blocked_long=1 << 30, **layout) as g:
+            assert g.layout()["n_long"] > 0
+            for sweeps in (1, 3):
+                s, st = g.pagerank(tol=0.0, max_iter=sweeps, form=G.FORM_BLOCKED)
+                ref, _ = fixed_point_sweeps(rp, col, od, s0, sweeps)
+                assert np.array_equal(s, ref), (layout, sweeps, np.abs(s - ref).max())
+
+
+@pytest.mark.parametrize("maker", [lambda: star(20000), degree_ladder], ids=["star", "ladder"])
+@pytest.mark.parametrize("blocked_long", [0, 64, 2048, 4096, 1 << 30])
+def test_heavy_row_threshold(G, O, maker, blocked_long):
+    """Rows above blocked_long in-edges (0: the rows that crowd their block)
+    are summed in chunks, the rest in blocks; any split meets the parity bar."""
+    rp, col, od = maker()
+    ref, ref_it, _ = O.pr_plain_f32(rp, col, od, tol=1e-6, max_iter=100)
+    with G.Graph(rp, col, od, chunk=256, chunk_min=64, blocked=True, block_rows=500,
+                 tile_words=2048, blocked_long=blocked_long) as g:
+        s, st = g.pagerank(tol=1e-6, max_iter=100, form=G.FORM_BLOCKED)
+    assert abs(st.iterations - ref_it) <= 1
+    s64, _, _ = O.pr_f64(rp, col, od, tol=0.0, max_iter=st.iterations)
+    assert np.all(np.abs(s - ref) <= ABS_TOL + np.abs(ref - s64))
+    with pytest.raises(G.GprError) as e:
+        G.Graph(rp, col, od, blocked=True, blocked_long=-1)
+    assert e.value.status == G.GPR_EINVAL
+
+
 @pytest.mark.parametrize("maker", [star, degree_ladder])
 def test_blocked_with_chunked_rows(G, O, maker):
     rp, col, od = maker()
     ref, ref_it, _ = O.pr_plain_f32(rp, col, od, tol=1e-5, max_iter=60)
     with G.Graph(rp, col, od, chunk=512, chunk_min=1024, blocked=True, block_rows=300,
-                 tile_words=1024) as g:
+                 tile_words=1024, blocked_long=1) as g:
         lay = g.layout()
         s, st = g.pagerank(tol=1e-5, max_iter=60, form=G.FORM_BLOCKED)
     assert lay["n_long"] > 0
@@ -184,7 +224,7 @@ def test_graphs_without_blocked_rows(G, O):
     assert st.iterations == it and np.array_equal(s, ref)
     # every row with in-edges chunked
     rp, col, od = star(20000)
-    with G.Graph(rp, col, od, chunk=128, chunk_min=1, blocked=True) as g:
+    with G.Graph(rp, col, od, chunk=128, chunk_min=1, blocked=True, blocked_long=1) as g:
         s, st = g.pagerank(tol=1e-6, max_iter=50, form=G.FORM_BLOCKED)
     ref, it, _ = O.pr_plain_f32(rp, col, od, tol=1e-6, max_iter=50)
     assert abs(st.iterations - it) <= 1

@@ -8,7 +8,7 @@ import pytest
 from graphs import erdos_renyi, star
 
 LAYOUT_KEYS = ("sell_max", "chunk", "chunk_min", "hot_entries", "blocked", "block_rows",
-               "tile_words")
+               "tile_words", "blocked_long")
 
 
 def test_signature_classes(G, O):
@@ -39,9 +39,13 @@ def test_cache_entries_of_the_blocked_form(G, tmp_path):
     p = str(tmp_path / "tune.txt")
     with open(p, "w") as f:
         f.write("pr:m24:d4:s2 64 4096 1073741824 32768 0 0.59 4 8192 131072\n")
+        f.write("pr:m22:d4:s2 64 4096 4096 32768 0 0.15 4 0 0 16384\n")
     r = G.tune_cache_lookup(p, "pr:m24:d4:s2")
     assert r["blocked"] and r["block_rows"] == 8192 and r["tile_words"] == 131072
     assert r["chunk_min"] == 1 << 30 and r["ms_per_sweep"] == 0.59
+    assert r["blocked_long"] == 0  # ten-field lines: the library default
+    r = G.tune_cache_lookup(p, "pr:m22:d4:s2")
+    assert r["blocked"] and r["blocked_long"] == 16384 and r["block_rows"] == 0
 
 
 @pytest.mark.gpu
@@ -49,7 +53,7 @@ def test_tune_graph_and_cache(G, O, tmp_path):
     rp, col, od = O.rmat_graph(15, 16, seed=2)
     cache = str(tmp_path / "tune.txt")
     r = G.tune_graph(rp, col, od, cache=cache, sweeps=4)
-    assert not r["from_cache"] and r["candidates"] >= 10
+    assert not r["from_cache"] and r["candidates"] >= 8
     assert r["ms_per_sweep"] <= r["default_ms_per_sweep"]  # a pick only replaces a slower one
     assert os.path.exists(cache)
     r2 = G.tune_graph(rp, col, od, cache=cache, sweeps=4)
