@@ -18,8 +18,8 @@
 //            grouped by the 65536-source segment (source >> 16) and, inside a
 //            group, by source; every group starts on a multiple of 4 words
 //            (padding words are 0xFFFFFFFF and read nothing)
-//   runs     {first word, segment << 16 | words}: at most kRunWords words of one
-//            group (one warp's unit of work)
+//   runs     {first word, segment << 16 | words}: at most run_words words (128
+//            per index load of a lane; 512) of one group (one warp's unit of work)
 //   tiles    {block, first run, end run, words}: consecutive runs of one block,
 //            at most tile_slots words and kTileRuns runs (one CTA's unit), in
 //            descending size (the CTA queue hands out the heaviest first)
@@ -32,9 +32,24 @@
 // source) and the value (row - row0); one radix sort orders them; the group
 // starts are selected on the device and the run / tile tables (a few hundred
 // thousand entries) are cut on the host.
+//
+// Tail of the sweep: CTAs take tiles heaviest first, each as it frees, so the
+// sweep ends when the last CTA finishes its last tile.  With tiles of nearly
+// one size, tiles / CTAs just above an integer leaves most CTAs idle for a
+// whole tile (RMAT scale 22: 890 tiles of 73K words on 296 CTAs, a quarter of
+// the sweep at the grid barrier).  The builder plays the queue on the host
+// (tile time = words + 2 per block row + 1024, for opening and closing it)
+// and halves, at a run boundary, every tile that would end after 1.02 x the
+// balanced time, until none does (or none can be halved).  A tile's real time
+// also grows with the sparsity of its block (RMAT scale 24: ~0.7 ns per word
+// in blocks of < 20 edges per row, ~0.19 in the densest), but ordering and
+// splitting by that estimate measured slower than by words: each extra split
+// adds a cross-tile flush of the block's rows.
 #include <cub/cub.cuh>
 
 #include <algorithm>
+#include <functional>
+#include <queue>
 #include <vector>
 
 #include "gpr_internal.cuh"
@@ -188,14 +203,16 @@ int blocked_split(const PrLayout &L, const int *d_rowptr, int long_min, int R, i
 
 int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
                          const PrLayout &L, int row0, int n_chunks, int R, int tile_slots,
-                         BlockedLayout *B, cudaStream_t st) {
+                         int run_words, int workers, BlockedLayout *B, cudaStream_t st) {
   *B = BlockedLayout();
   B->R = R;
+  B->run_words = run_words;
   B->tile_slots = tile_slots;
   B->row0 = row0;
   B->n_chunks = n_chunks;
   const int n_rows = L.n_nz - row0;
-  if (R < 1 || R > kBlockedMaxRows || tile_slots < kRunWords || row0 < 0 || row0 > L.n_long) {
+  if (R < 1 || R > kBlockedMaxRows || tile_slots < kRunWords || row0 < 0 || row0 > L.n_long ||
+      run_words < 128 || run_words > 512 || run_words % 128 != 0) {
     set_error("blocked layout: block rows %d must be in [1, %d], tile words %d >= %d", R,
               kBlockedMaxRows, tile_slots, kRunWords);
     return GPR_EINVAL;
@@ -334,7 +351,7 @@ int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d
     const int r0 = row0 + b * R;
     blocks[b] = make_int4(r0, std::min(R, L.n_nz - r0), 0, 0);
   }
-  runs.reserve((size_t)(n_edges / kRunWords) + ng + 1);
+  runs.reserve((size_t)(n_edges / run_words) + ng + 1);
   long long pos = 0;
   int g = 0;
   while (g < ng) {
@@ -357,8 +374,8 @@ int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d
       const long long size = (q + 1 < ng ? (long long)h_gstart[q + 1] : n_edges) - h_gstart[q];
       const long long padded = (size + 3) / 4 * 4;
       gpos[q] = pos;
-      for (long long off = 0; off < padded; off += kRunWords) {
-        const int len = (int)std::min<long long>(kRunWords, padded - off);
+      for (long long off = 0; off < padded; off += run_words) {
+        const int len = (int)std::min<long long>(run_words, padded - off);
         if (tile_runs > 0 && (tile_words + len > tile_slots || tile_runs == kTileRuns)) close_tile();
         runs.push_back(make_uint2((unsigned)(pos + off), ((unsigned)h_gseg[q] << 16) | (unsigned)len));
         ++tile_runs;
@@ -375,8 +392,44 @@ int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d
     dfree(gstart);
     return fail(GPR_EINVAL);
   }
-  std::stable_sort(tiles.begin(), tiles.end(),
-                   [](const int4 &x, const int4 &y) { return x.w > y.w; });
+  const double open_close = 2.0 * R + 1024.0;
+  auto cost = [&](const int4 &t) { return t.w + open_close; };
+  auto by_cost = [](const int4 &x, const int4 &y) { return x.w > y.w; };
+  for (int round = 0; round < 24 && workers > 0; ++round) {
+    std::stable_sort(tiles.begin(), tiles.end(), by_cost);
+    std::priority_queue<double, std::vector<double>, std::greater<double>> free_at;
+    for (int i = 0; i < workers; ++i) free_at.push(0.0);
+    std::vector<double> end(tiles.size());
+    double total = 0.0;
+    for (size_t i = 0; i < tiles.size(); ++i) {
+      end[i] = free_at.top() + cost(tiles[i]);
+      free_at.pop();
+      free_at.push(end[i]);
+      total += cost(tiles[i]);
+    }
+    const double share = total / workers;
+    std::vector<int4> next;
+    next.reserve(tiles.size() + workers);
+    bool split = false;
+    for (size_t i = 0; i < tiles.size(); ++i) {
+      const int4 t = tiles[i];
+      if (end[i] <= 1.02 * share || t.z - t.y < 2) {
+        next.push_back(t);
+        continue;
+      }
+      int mid = t.y, left = 0;
+      while (mid < t.z - 1 && left + (int)(runs[mid].y & 0xFFFFu) <= t.w / 2)
+        left += (int)(runs[mid++].y & 0xFFFFu);
+      if (mid == t.y) left += (int)(runs[mid++].y & 0xFFFFu);
+      next.push_back(make_int4(t.x, t.y, mid, left));
+      next.push_back(make_int4(t.x, mid, t.z, t.w - left));
+      blocks[t.x].z += 1;
+      split = true;
+    }
+    tiles.swap(next);
+    if (!split) break;
+  }
+  std::stable_sort(tiles.begin(), tiles.end(), by_cost);
   B->slots = pos;
   B->n_runs = (long long)runs.size();
   B->n_tiles = (int)tiles.size();

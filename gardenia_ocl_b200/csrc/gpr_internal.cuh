@@ -124,14 +124,17 @@ void free_pr_layout(PrLayout *L);
 
 // Destination-blocked, source-ordered layout of the rows [n_long, n_nz) of a
 // PrLayout (gpr_blocked.cu describes the storage).
-constexpr int kRunWords = 512;        // entry words of one run (a warp's unit)
-constexpr int kTileRuns = 1024;       // most runs in one tile (staged in shared memory)
+constexpr int kRunWords = 512;        // most entry words of one run (a warp's unit)
+constexpr int kTileRuns = 1 << 16;    // most runs in one tile
 constexpr int kBlockedRows = 12288;   // rows per block (accumulators in shared memory)
 constexpr int kBlockedMaxRows = 12288;
-constexpr int kTileWordsDefault = 1 << 18;
+constexpr int kTileWordsDefault = 1 << 20;
+// GPR_FORM_AUTO picks the blocked form from this many edges up
+constexpr long long kBlockedAutoMinEdges = 3LL << 24;
 
 struct BlockedLayout {
   int R = 0, tile_slots = 0;
+  int run_words = 0;  // most entry words per run: 128 x the kernel's index loads per lane
   int row0 = 0;      // first blocked row; rows [0, row0) are summed in chunks
   int n_chunks = 0;  // chunks of rows [0, row0): a prefix of the exact-order chunks
   int n_blocks = 0, n_tiles = 0;
@@ -154,7 +157,10 @@ int blocked_split(const PrLayout &L, const int *d_rowptr, int long_min, int R, i
                   int *n_chunks, long long *long_words, cudaStream_t st);
 int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
                          const PrLayout &L, int row0, int n_chunks, int R, int tile_slots,
-                         BlockedLayout *B, cudaStream_t st);
+                         int run_words, int workers, BlockedLayout *B, cudaStream_t st);
+// CTAs per SM of the blocked kernel for blocks of R rows: two 512-thread CTAs
+// when both fit beside an L1 of about half the SM's 256 KB, else one of 1024.
+inline int blocked_ctas_per_sm(int R) { return R <= 8192 ? 2 : 1; }
 void free_blocked_layout(BlockedLayout *B);
 
 // Validates a device CSR (rowptr[0] = 0, monotone, rowptr[m] = nnz, every

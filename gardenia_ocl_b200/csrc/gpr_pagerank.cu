@@ -426,16 +426,76 @@ __device__ __forceinline__ double blocked_finalize(const PrArgs &a, float *cout,
   return err;
 }
 
+// Index words of a run (lanes past its end get padding words).
+template <int PV>
+__device__ __forceinline__ void load_run(const PrArgs &a, uint2 rd, int lane, uint4 *q,
+                                         const Policies &pol) {
+  const int len = (int)(rd.y & 0xFFFFu);
+#pragma unroll
+  for (int i = 0; i < PV; ++i)
+    q[i] = ld_entry4(a.entry + rd.x + 128 * i + 4 * lane, 128 * i + 4 * lane < len, pol.stream);
+}
+
+// The run's contributions: wait for its index words, issue every gather, wait
+// for them, then add them to the rows' fixed-point accumulators (PV even:
+// the additions go eight at a time).
+template <int PV>
+__device__ __forceinline__ void add_run(const PrArgs &a, const float *cin, unsigned *acc,
+                                        uint2 rd, const uint4 *q, const Policies &pol) {
+  static_assert(PV % 2 == 0, "eight contributions per addition batch");
+  const unsigned segbase = (rd.y >> 16) << 16;
+#pragma unroll
+  for (int i = 0; i < PV; ++i) {
+    use_u32(q[i].x); use_u32(q[i].y); use_u32(q[i].z); use_u32(q[i].w);
+  }
+  float v[4 * PV];
+#pragma unroll
+  for (int i = 0; i < PV; ++i) {
+    v[4 * i + 0] = gather_entry(cin, segbase, q[i].x, pol.keep);
+    v[4 * i + 1] = gather_entry(cin, segbase, q[i].y, pol.keep);
+    v[4 * i + 2] = gather_entry(cin, segbase, q[i].z, pol.keep);
+    v[4 * i + 3] = gather_entry(cin, segbase, q[i].w, pol.keep);
+  }
+#pragma unroll
+  for (int i = 0; i < 4 * PV; ++i) use_f32(v[i]);
+  unsigned wv[4 * PV];
+#pragma unroll
+  for (int i = 0; i < PV; ++i) {
+    wv[4 * i + 0] = q[i].x; wv[4 * i + 1] = q[i].y; wv[4 * i + 2] = q[i].z; wv[4 * i + 3] = q[i].w;
+  }
+#pragma unroll
+  for (int h = 0; h < 4 * PV; h += 8) {
+    unsigned lo[8], hw[8], old[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const long long x = __float2ll_rn(v[h + i] * a.fx_scale);
+      lo[i] = (unsigned)x;
+      hw[i] = (unsigned)((unsigned long long)x >> 32);
+      old[i] = 0u;
+      if (wv[h + i] != 0xFFFFFFFFu) old[i] = atomicAdd(acc + (wv[h + i] & 0xFFFFu), lo[i]);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+      const unsigned hc = hw[i] + (old[i] + lo[i] < old[i] ? 1u : 0u);
+      if (wv[h + i] != 0xFFFFFFFFu && hc) atomicAdd(acc + a.acc_rows + (wv[h + i] & 0xFFFFu), hc);
+    }
+  }
+}
+
 // One tile: zero the block's accumulators, add the tile's runs, then finalize
-// the block (single tile) or add into the cross-tile accumulators.
+// the block (single tile) or add into the cross-tile accumulators.  Warps
+// take runs from a shared counter; the CTA claims its next tile from the
+// queue `tq` once its runs are done (the claim's latency hides behind the
+// close of this tile, and the tile goes to a CTA that is about to be free).
 template <int PV, int NT>
 __device__ __forceinline__ double blocked_tile(const PrArgs &a, const float *cin, float *cout,
                                                int t, unsigned *acc, int *s_next, int *s_last,
-                                               const Policies &pol) {
+                                               int *s_next_tile, int *tq, const Policies &pol) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int4 td = a.tiles[t];
   const int4 bd = a.blocks[td.x];
   const int nr = td.z - td.y;
+  const uint2 *runs = a.runs + td.y;
   for (int i = threadIdx.x; i < bd.y; i += NT) {
     acc[i] = 0u;
     acc[a.acc_rows + i] = 0u;
@@ -444,60 +504,21 @@ __device__ __forceinline__ double blocked_tile(const PrArgs &a, const float *cin
   __syncthreads();
   int r = warp;
   uint2 rd = make_uint2(0u, 0u);
-  if (r < nr) rd = __ldg(a.runs + td.y + r);
+  if (r < nr) rd = __ldg(runs + r);
   while (r < nr) {
     int rn = 0;
     if (lane == 0) rn = atomicAdd(s_next, 1);
-    const unsigned segbase = (rd.y >> 16) << 16;
-    const int len = (int)(rd.y & 0xFFFFu);
-    // all index loads of the run, then all gathers, then the additions
     uint4 q[PV];
-#pragma unroll
-    for (int i = 0; i < PV; ++i)
-      q[i] = ld_entry4(a.entry + rd.x + 128 * i + 4 * lane, 128 * i + 4 * lane < len, pol.stream);
+    load_run<PV>(a, rd, lane, q, pol);
     // the next run's descriptor is fetched while this run's loads are in flight
     rn = __shfl_sync(kFull, rn, 0);
     uint2 nd = make_uint2(0u, 0u);
-    if (rn < nr) nd = __ldg(a.runs + td.y + rn);
-#pragma unroll
-    for (int i = 0; i < PV; ++i) {
-      use_u32(q[i].x); use_u32(q[i].y); use_u32(q[i].z); use_u32(q[i].w);
-    }
-    float v[4 * PV];
-#pragma unroll
-    for (int i = 0; i < PV; ++i) {
-      v[4 * i + 0] = gather_entry(cin, segbase, q[i].x, pol.keep);
-      v[4 * i + 1] = gather_entry(cin, segbase, q[i].y, pol.keep);
-      v[4 * i + 2] = gather_entry(cin, segbase, q[i].z, pol.keep);
-      v[4 * i + 3] = gather_entry(cin, segbase, q[i].w, pol.keep);
-    }
-#pragma unroll
-    for (int i = 0; i < 4 * PV; ++i) use_f32(v[i]);
-    unsigned wv[4 * PV];
-#pragma unroll
-    for (int i = 0; i < PV; ++i) {
-      wv[4 * i + 0] = q[i].x; wv[4 * i + 1] = q[i].y; wv[4 * i + 2] = q[i].z; wv[4 * i + 3] = q[i].w;
-    }
-#pragma unroll
-    for (int h = 0; h < 4 * PV; h += 8) {
-      unsigned lo[8], hw[8], old[8];
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const long long x = __float2ll_rn(v[h + i] * a.fx_scale);
-        lo[i] = (unsigned)x;
-        hw[i] = (unsigned)((unsigned long long)x >> 32);
-        old[i] = 0u;
-        if (wv[h + i] != 0xFFFFFFFFu) old[i] = atomicAdd(acc + (wv[h + i] & 0xFFFFu), lo[i]);
-      }
-#pragma unroll
-      for (int i = 0; i < 8; ++i) {
-        const unsigned hc = hw[i] + (old[i] + lo[i] < old[i] ? 1u : 0u);
-        if (wv[h + i] != 0xFFFFFFFFu && hc) atomicAdd(acc + a.acc_rows + (wv[h + i] & 0xFFFFu), hc);
-      }
-    }
+    if (rn < nr) nd = __ldg(runs + rn);
+    add_run<PV>(a, cin, acc, rd, q, pol);
     r = rn;
     rd = nd;
   }
+  if (threadIdx.x == 0) *s_next_tile = atomicAdd(tq, 1);
   __syncthreads();
   double err = 0.0;
   if (bd.z == 1) {
@@ -526,7 +547,7 @@ __device__ __forceinline__ double blocked_tile(const PrArgs &a, const float *cin
 // threads per SM (one of 1024, or two of 512: then one CTA's warps keep
 // gathering while the other's wait at the barrier that closes a tile or
 // finalize its block).  Per sweep: CTAs take tiles from a queue (heaviest first; the
-// next tile is claimed while the current one runs), then warps take the
+// next tile is claimed while the current one closes), then warps take the
 // chunks of the rows above chunk_min in-edges, with the first contributions
 // staged in the shared memory the accumulators used, then the zero-in-degree
 // rows (sweeps 0 and 1), then the bounded grid barrier with the residual.
@@ -550,8 +571,8 @@ __global__ void __launch_bounds__(NT, MINB) k_pr_blocked(PrArgs a) {
       __syncthreads();
       const int t = s_tile;
       if (t >= a.n_tiles) break;
-      if (threadIdx.x == 0) s_next_tile = atomicAdd(a.tq + (it & 1), 1);
-      err += blocked_tile<PV, NT>(a, cin, cout, t, s_acc, &s_next, &s_last, pol);
+      err += blocked_tile<PV, NT>(a, cin, cout, t, s_acc, &s_next, &s_last, &s_next_tile,
+                                  a.tq + (it & 1), pol);
     }
     // chunks of the heaviest rows, the hottest contributions from shared
     // memory (none staged when the chunks are few)
@@ -934,8 +955,10 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
     if (ev_col) cudaEventDestroy(ev_col);
   }
   if (rc == GPR_OK && blocked) {
-    // Defaults sized to the graph: about two blocks and six tiles per SM
-    // (a multi-tile block adds one 8-byte atomic per row and tile).
+    // Default rows per block: about two blocks per SM.  Default tile size:
+    // whole blocks up to 1M words (a multi-tile block adds one 8-byte atomic
+    // per row and tile); the builder halves the tiles that would end the
+    // sweep late.
     int nsm = 148;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, g->device);
     if (block_rows == 0)
@@ -947,14 +970,11 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
     rc = gpr::blocked_split(g->L, (const int *)rp,
                             blocked_long > 0 ? std::max(blocked_long, chunk_min) : 0, block_rows,
                             &row0, &n_chunks, &long_words, st);
-    const long long words = std::max(0LL, nnz - long_words);
-    if (tile_words == 0)
-      tile_words = (int)std::min<long long>(
-          gpr::kTileWordsDefault,
-          std::max<long long>(4096, gpr::ceil_div(words, 6LL * nsm) / 512 * 512));
+    if (tile_words == 0) tile_words = gpr::kTileWordsDefault;
     if (rc == GPR_OK)
       rc = gpr::build_blocked_layout(m, nnz, (const int *)rp, (const int *)cp, g->L, row0,
-                                     n_chunks, block_rows, tile_words, &g->B, st);
+                                     n_chunks, block_rows, tile_words, gpr::kRunWords,
+                                     nsm * gpr::blocked_ctas_per_sm(block_rows), &g->B, st);
     g->has_blocked = rc == GPR_OK;
   }
   if (orp) gpr::dfree(rp);
@@ -1006,9 +1026,6 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
   g->max_grid = g->grid_step;
   for (int v = 0; v < kNumKernels; ++v) g->max_grid = std::max(g->max_grid, g->grid_hot[v]);
   if (g->has_blocked) {
-    // shared memory per CTA: the accumulators (dynamic) and the tile's run
-    // table (static)
-    const int smem = 8 * g->B.R;
     int smem_sm = 0;
     GPR_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor,
                                     g->device));
@@ -1017,12 +1034,13 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
     // 1024-thread CTA: the gathers' L1 line hits are worth more than the
     // overlap (RMAT scale 24 with 12288-row blocks: 2x slower sweeps with
     // two CTAs and a 28 KB L1).
-    g->blocked_ctas = g->B.R <= 8192 ? 2 : 1;
+    g->blocked_ctas = gpr::blocked_ctas_per_sm(g->B.R);
     int per_sm = 0;
     for (;;) {
       // the smallest shared-memory carveout that holds the CTAs: the rest of
       // the SM's 256 KB stays L1
       const void *k = blocked_kernel(g->blocked_ctas);
+      const int smem = 8 * g->B.R;
       cudaFuncAttributes fa;
       GPR_CUDA(cudaFuncGetAttributes(&fa, k));
       const long long need = (long long)g->blocked_ctas * (smem + (long long)fa.sharedSizeBytes + 1024);
@@ -1313,7 +1331,8 @@ int pagerank_impl(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts_in,
   int rc = GPR_OK;
   const bool use_blocked =
       o.precision == GPR_PREC_FP32 && g->has_blocked && g->blocked_ok &&
-      o.loop != GPR_LOOP_GRAPH && o.form != GPR_FORM_EXACT;
+      o.loop != GPR_LOOP_GRAPH && o.form != GPR_FORM_EXACT &&
+      (o.form == GPR_FORM_BLOCKED || g->L.nnz >= gpr::kBlockedAutoMinEdges);
   if (use_blocked) {
     rc = solve_impl(g, d_scores, o, 0, &st_local, true);
     if (rc == kBlockedFallback) {

@@ -250,7 +250,7 @@ int gpr_tune_graph(int m, long long nnz, const int *any_rowptr, const int *any_c
     best = tb;
     descend(&x, &best, std::vector<int>{6144, 8192},
             [](Cfg *y, int v) { y->block_rows = v; }, time);
-    descend(&x, &best, std::vector<int>{131072, 524288},
+    descend(&x, &best, std::vector<int>{2097152, 4194304},
             [](Cfg *y, int v) { y->tile_words = v; }, time);
     descend(&x, &best, std::vector<int>{16384, 1 << 30},
             [](Cfg *y, int v) { y->blocked_long = v; }, time);

@@ -81,14 +81,16 @@ typedef struct {
  *   EXACT    rows of <= 64 in-edges add their contributions one by one in CSR
  *            order with rounded float adds, as the reference does: such rows
  *            are bit-identical to the reference's.
- *   BLOCKED  rows of <= chunk_min in-edges are summed block by block from
- *            source-ordered edges (far fewer memory requests on large graphs),
- *            in 64-bit fixed point: the exact sum of the FP32 contributions
- *            rounded once to 2^-S (S >= 31, chosen per solve from the edge
- *            count and the largest score), then to FP32.  Deterministic.  Needs
- *            a graph created with GPR_LAYOUT_BLOCKED and the persistent loop.
- *   AUTO     BLOCKED when the graph has its layout and the persistent loop
- *            runs, else EXACT. */
+ *   BLOCKED  rows (all but the hubs, gpr_layout_opts.blocked_long) are summed
+ *            block by block from source-ordered edges (far fewer memory
+ *            requests on large graphs), in 64-bit fixed point: the exact sum
+ *            of the FP32 contributions rounded once to 2^-S (S >= 31, chosen
+ *            per solve from the edge count and the largest score), then to
+ *            FP32.  Deterministic.  Needs a graph created with
+ *            GPR_LAYOUT_BLOCKED and the persistent loop.
+ *   AUTO     BLOCKED when the graph has its layout, at least 50,331,648 edges
+ *            (below that EXACT measured faster: RMAT scale 21 3.6 vs 3.9 ms,
+ *            scale 22 7.6 vs 6.8 ms) and the persistent loop runs, else EXACT. */
 typedef enum {
   GPR_FORM_AUTO = 0,
   GPR_FORM_EXACT = 1,
@@ -141,8 +143,8 @@ typedef struct {
   int flags;      /* GPR_LAYOUT_* bits */
   int block_rows; /* blocked form: rows per block, <= 12288 (default: about rows / (2 SMs),
                      256 .. 12288) */
-  int tile_words; /* blocked form: most entry words per tile, >= 512 (default: about
-                     edges / (6 SMs), 4096 .. 262144) */
+  int tile_words; /* blocked form: most entry words per tile, >= 512 (default 1048576;
+                     the tiles that would end a sweep late are halved further) */
   int blocked_long; /* blocked form: rows with more in-edges than this are summed in chunks,
                        the others in blocks; values below chunk_min act as chunk_min.
                        0 (default): a row is chunked when it holds more than 1/8 of the

@@ -90,7 +90,7 @@ def test_any_tiling_gives_the_same_bits(G, O):
 def test_blocked_matches_reference(G, O, scale, tol):
     rp, col, od = O.rmat_graph(scale, 16, seed=1)
     ref, ref_it, _ = O.pr_plain_f32(rp, col, od, tol=tol, max_iter=100)
-    s, st = solve(G, rp, col, od, tol=tol, max_iter=100)  # AUTO picks the blocked form
+    s, st = solve(G, rp, col, od, tol=tol, max_iter=100, form=G.FORM_BLOCKED)
     assert abs(st.iterations - ref_it) <= 1
     assert np.abs(s - ref).max() <= ABS_TOL
     # Rounding: against an FP64 run of the same sweeps, the fixed-point sums

@@ -19,18 +19,32 @@ pytestmark = pytest.mark.gpu
 
 
 def test_rmat24_pagerank_full_size(G, O):
+    """Both sweep forms at full size: the exact-order layout, and the blocked
+    layout that AUTO solves in the blocked form at this size (and, from a
+    non-finite score, in the exact form)."""
     csr = G.gen_rmat(24, 16, seed=1)
     rp, col, od = csr.rowptr.to_numpy(), csr.col.to_numpy(), csr.third.to_numpy()
-    with G.Graph(csr.rowptr, csr.col, csr.third, m=csr.m, nnz=csr.nnz) as g:
+    m = csr.m
+    bad = np.full(m, np.float32(1.0) / np.float32(m), dtype=np.float32)
+    bad[7] = np.inf
+    with G.Graph(csr.rowptr, csr.col, csr.third, m=m, nnz=csr.nnz) as g:
         s, st = g.pagerank(tol=1e-6, max_iter=100)
+        s_bad, st_bad = g.pagerank(bad.copy(), tol=1e-6, max_iter=3)
+    with G.Graph(csr.rowptr, csr.col, csr.third, m=m, nnz=csr.nnz, blocked=True) as g:
+        sb, stb = g.pagerank(tol=1e-6, max_iter=100)
+        sb_bad, stb_bad = g.pagerank(bad.copy(), tol=1e-6, max_iter=3)
     csr.close()
+    assert stb_bad.iterations == st_bad.iterations
+    assert np.array_equal(np.isnan(sb_bad), np.isnan(s_bad))
+    assert np.array_equal(sb_bad[~np.isnan(sb_bad)], s_bad[~np.isnan(s_bad)])
     ref, ref_it, _ = O.pr_plain_f32(rp, col, od, tol=1e-6, max_iter=100)
-    assert abs(st.iterations - ref_it) <= 1
-    s64, _, _ = O.pr_f64(rp, col, od, tol=0.0, max_iter=st.iterations)
-    assert np.all(np.abs(s - ref) <= 1e-6 + np.abs(ref - s64))
     fix, _, _ = O.pr_f64(rp, col, od, tol=1e-13, max_iter=400)
-    _, l1 = O.err_vs_f64(s, fix)
-    assert l1 <= 1e-5
+    for got, n in ((s, st.iterations), (sb, stb.iterations)):
+        assert abs(n - ref_it) <= 1
+        s64, _, _ = O.pr_f64(rp, col, od, tol=0.0, max_iter=n)
+        assert np.all(np.abs(got - ref) <= 1e-6 + np.abs(ref - s64))
+        _, l1 = O.err_vs_f64(got, fix)
+        assert l1 <= 1e-5
 
 
 def test_multigraph_512_sample_full_size(G, O):
