@@ -65,3 +65,51 @@ def test_symgs_zero_diagonal_rows_unchanged(G, O):
     x = x0.copy()
     G.SymGSSolver(m, len(Aj), Ap, Aj, idx, Ax, x, b, co)
     assert np.array_equal(x, x0)
+
+
+def test_symgs_stencil128_parity_colouring_full_size(G, O):
+    """The benchmark's case: 27-point 128^3 stencil, 8-colour parity colouring,
+    296 row domains synchronised only with their neighbours; two sweeps,
+    bit-identical to the oracle's sequential colour order."""
+    n = 128
+    Ap, Aj, Ax = O.stencil27(n)
+    m = len(Ap) - 1
+    v = np.arange(m, dtype=np.int64)
+    color = (v % n % 2) + 2 * ((v // n) % n % 2) + 4 * ((v // (n * n)) % 2)
+    idx = np.argsort(color, kind="stable").astype(np.int32)
+    co = np.zeros(9, dtype=np.int32)
+    np.cumsum(np.bincount(color, minlength=8), out=co[1:])
+    x0, b = O.uniform_f32(m, 31), O.uniform_f32(m, 32)
+    with G.SymGS(Ap, Aj, Ax, idx, co) as S:
+        x = x0.copy()
+        S.apply(x, b, sweeps=2)
+    xr = O.symgs_f32(Ap, Aj, Ax, idx, co, O.symgs_f32(Ap, Aj, Ax, idx, co, x0, b), b)
+    assert np.array_equal(x, xr)
+
+
+@pytest.mark.parametrize("seed", [1, 2])
+def test_symgs_irregular_matrix(G, O, seed):
+    """A random symmetric sparsity pattern with a few dense rows and a greedy
+    colouring: domains of uneven row counts with many neighbours each."""
+    rng = np.random.default_rng(seed)
+    m = 60000
+    src = rng.integers(0, m, 4 * m)
+    dst = rng.integers(0, m, 4 * m)
+    hubs = rng.integers(0, m, 20)
+    src = np.concatenate([src, np.repeat(hubs, 3000), np.arange(m)])
+    dst = np.concatenate([dst, rng.integers(0, m, 20 * 3000), np.arange(m)])
+    a, c = np.concatenate([src, dst]), np.concatenate([dst, src])
+    key = np.unique(a.astype(np.int64) * m + c)
+    rows, cols = (key // m).astype(np.int32), (key % m).astype(np.int32)
+    Ap = np.zeros(m + 1, dtype=np.int32)
+    np.cumsum(np.bincount(rows, minlength=m), out=Ap[1:])
+    Aj = cols
+    Ax = np.where(rows == cols, np.float32(40.0),
+                  rng.random(len(cols), dtype=np.float32) - np.float32(0.5)).astype(np.float32)
+    idx, co = O.greedy_coloring(Ap, Aj)
+    x0, b = O.uniform_f32(m, 5), O.uniform_f32(m, 6)
+    with G.SymGS(Ap, Aj, Ax, idx, co) as S:
+        x = x0.copy()
+        S.apply(x, b, sweeps=2)
+    xr = O.symgs_f32(Ap, Aj, Ax, idx, co, O.symgs_f32(Ap, Aj, Ax, idx, co, x0, b), b)
+    assert np.array_equal(x, xr)
