@@ -780,10 +780,11 @@ def multigraph_leg(G, torch, dev, stream, plain_gteps, args):
     """Uneven multi-graph batch: 512 seeded graphs, m_g log-uniform in
     [1e3, 5e5], half Erdos-Renyi (8 draws per vertex), half Chung-Lu power
     law (exponent 2.1, 16 draws per vertex), each solved to tol 1e-6 as plain
-    PageRank of its own, all in one persistent launch, in FP32 and in the
-    BF16 + FP32 refinement form.  Rate: sum over graphs of nnz_g x sweeps_g
-    per second of the sweep loop; bytes: sum of (4 nnz_g + 28 m_g + 4) x
-    sweeps_g."""
+    PageRank of its own, all in one persistent launch, in FP32 (the blocked
+    form: every graph's rows in blocks of source-ordered edges, fixed-point
+    sums; the units form beside it) and in the BF16 + FP32 refinement form.
+    Rate: sum over graphs of nnz_g x sweeps_g per second of the sweep loop;
+    bytes: sum of (4 nnz_g + 28 m_g + 4) x sweeps_g."""
     t0 = time.time()
     A, voff = G.gen_multigraph(MG_GRAPHS, MG_MMIN, MG_MMAX, seed=MG_SEED)
     layouts, tuned = None, None
@@ -791,7 +792,7 @@ def multigraph_leg(G, torch, dev, stream, plain_gteps, args):
         layouts, tuned = G.tune_multigraph(A.rowptr, A.col, A.third, voff, nnz=A.nnz,
                                            cache=args.tune_cache, sweeps=5)
         log(f"[ours] multigraph tuned: {tuned}")
-    mg = G.MultiGraph(A.rowptr, A.col, A.third, voff, nnz=A.nnz, layouts=layouts)
+    mg = G.MultiGraph(A.rowptr, A.col, A.third, voff, nnz=A.nnz, layouts=layouts, blocked=True)
     mg.set_stream(stream.cuda_stream)
     info = mg.info()
     rp = A.rowptr.to_numpy()
@@ -808,13 +809,15 @@ def multigraph_leg(G, torch, dev, stream, plain_gteps, args):
            "bins": sorted({(d["sell_max"], d["chunk_min"], d["chunk"]) for d in layouts})
            if layouts else "defaults"}
     x_star = None
-    for prec, name in ((G.PREC_FP32, "fp32"), (G.PREC_BF16, "bf16_refined")):
+    for prec, name, form in ((G.PREC_FP32, "fp32", G.FORM_AUTO),
+                             (G.PREC_FP32, "fp32_units_form", G.FORM_EXACT),
+                             (G.PREC_BF16, "bf16_refined", G.FORM_AUTO)):
         dest = out if prec == G.PREC_FP32 else out.setdefault("bf16_study", {"note": BF16_NOTE})
         best = None
         for _ in range(3):
             scores.copy_(init)
             _, it, res, st = mg.pagerank(scores, tol=TOL, max_iter=MG_MAX_ITER, damping=DAMPING,
-                                         precision=prec)
+                                         precision=prec, form=form)
             if best is None or st.loop_ms < best[0].loop_ms:
                 best = (st, it.copy(), res.copy())
         st, it, res = best
@@ -827,7 +830,8 @@ def multigraph_leg(G, torch, dev, stream, plain_gteps, args):
                      "vs_plain_single_graph": edges / (st.loop_ms / 1e3) / 1e9 / plain_gteps,
                      "achieved_gbs": byts / (st.loop_ms / 1e3) / 1e9,
                      "frac": byts / (st.loop_ms / 1e3) / 1e9 / peak, "peak_kind": peak_kind,
-                     "gpu_launches": st.gpu_launches}
+                     "gpu_launches": st.gpu_launches,
+                     "form": "blocked" if name == "fp32" else "units"}
         # every graph's errors against the batch's FP64 fixed point (each
         # graph with its own teleport (1 - d) / m_g); all graphs have m_g > 0
         if x_star is None:

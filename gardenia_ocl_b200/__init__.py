@@ -363,23 +363,29 @@ class MultiGraph:
     rows come from that range (global vertex ids).  ``layouts``: None, or one
     dict per graph with any of sell_max / chunk / chunk_min (each graph's own
     bins).  Every graph is solved as ``Graph.pagerank`` solves it alone, all
-    in one persistent launch."""
+    in one persistent launch.  ``blocked``: also build the blocked form's
+    layout (each graph's rows in blocks; ``block_rows`` / ``tile_words`` as
+    for ``Graph``), which ``pagerank`` uses from 50.3M edges up (AUTO) or when
+    asked with ``form=FORM_BLOCKED``."""
 
-    def __init__(self, rowptr, col, outdeg, voff, nnz=None, layouts=None):
+    def __init__(self, rowptr, col, outdeg, voff, nnz=None, layouts=None, blocked=False,
+                 block_rows=0, tile_words=0):
         L = lib()
         self.voff = np.ascontiguousarray(voff, dtype=np.int32)
         self.n_graphs = len(self.voff) - 1
         self.m = int(self.voff[-1])
         nnz = int(len(col)) if nnz is None else int(nnz)
         lo = None
-        if layouts is not None:
-            if len(layouts) != self.n_graphs:
+        if layouts is not None or blocked:
+            if layouts is not None and len(layouts) != self.n_graphs:
                 raise ValueError("one layout per graph")
             lo = (LayoutOptions * self.n_graphs)()
-            for i, d in enumerate(layouts):
-                d = d or {}
+            for i in range(self.n_graphs):
+                d = (layouts[i] if layouts is not None else None) or {}
                 lo[i] = LayoutOptions(int(d.get("sell_max", 0)), int(d.get("chunk", 0)),
-                                      int(d.get("chunk_min", 0)), 0, 0)
+                                      int(d.get("chunk_min", 0)), 0,
+                                      LAYOUT_BLOCKED if blocked else 0, int(block_rows),
+                                      int(tile_words), 0)
         pr, k0 = _ptr(rowptr, np.int32)
         pc, k1 = _ptr(col, np.int32)
         pd, k2 = _ptr(outdeg, np.int32)

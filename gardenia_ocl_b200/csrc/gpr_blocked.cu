@@ -20,10 +20,10 @@
 //            (padding words are 0xFFFFFFFF and read nothing)
 //   runs     {first word, segment << 16 | words}: at most run_words words (128
 //            per index load of a lane; 512) of one group (one warp's unit of work)
-//   tiles    {block, first run, end run, words}: consecutive runs of one block,
+//   tiles    {block, first run, end run, residual slot}: consecutive runs of one block,
 //            at most tile_slots words and kTileRuns runs (one CTA's unit), in
 //            descending size (the CTA queue hands out the heaviest first)
-//   blocks   {row0, nrows, tiles, 0}
+//   blocks   {row0, nrows, tiles, row range}
 // Rows of heavier in-degree (the first row0 rows, chunked) and rows without
 // in-edges keep the exact-order layout's work units: the chunks of rows
 // [0, row0) are the first row_cbeg[row0] chunks of the exact-order layout.
@@ -74,18 +74,27 @@ __global__ void k_inverse(int m, const int *__restrict__ perm, int *inv) {
 }
 
 // One warp per original row: the keys and values of its in-edges when its
-// new label falls in [row0, n_nz); other edges get the key ~0 (sorted last).
+// new label falls in a blocked range [rb[i], re[i]) (ranges ascending and
+// disjoint, range i's blocks numbered from bb[i]); other edges get the key ~0
+// (sorted last).
 __global__ void k_block_keys(int m, const int *__restrict__ rowptr, const int *__restrict__ col,
-                             const int *__restrict__ inv, int n_long, int n_nz, int R,
+                             const int *__restrict__ inv, int n_ranges, const int *__restrict__ rb,
+                             const int *__restrict__ re, const int *__restrict__ bb, int R,
                              unsigned long long *key, unsigned *val) {
   const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= m) return;
   const int o = (int)w;
   const int r = inv[o];
-  const bool in = r >= n_long && r < n_nz;
-  const unsigned long long blk = in ? (unsigned long long)((r - n_long) / R) : 0ull;
-  const unsigned dl = in ? (unsigned)((r - n_long) % R) : 0u;
+  int lo = 0, hi = n_ranges - 1;  // the last range starting at or before r
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (rb[mid] <= r) lo = mid;
+    else hi = mid - 1;
+  }
+  const bool in = r >= rb[lo] && r < re[lo];
+  const unsigned long long blk = in ? (unsigned long long)(bb[lo] + (r - rb[lo]) / R) : 0ull;
+  const unsigned dl = in ? (unsigned)((r - rb[lo]) % R) : 0u;
   for (int e = rowptr[o] + lane; e < rowptr[o + 1]; e += 32) {
     key[e] = in ? (blk << 32) | (unsigned)inv[col[e]] : ~0ull;
     val[e] = dl;
@@ -204,44 +213,76 @@ int blocked_split(const PrLayout &L, const int *d_rowptr, int long_min, int R, i
 int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
                          const PrLayout &L, int row0, int n_chunks, int R, int tile_slots,
                          int run_words, int workers, BlockedLayout *B, cudaStream_t st) {
+  if (row0 < 0 || row0 > L.n_long) {
+    set_error("blocked layout: first blocked row %d outside [0, %d]", row0, L.n_long);
+    return GPR_EINVAL;
+  }
+  const std::vector<int> rb{row0}, re{L.n_nz};
+  const int rc = build_blocked_ranges(m, nnz, d_rowptr, d_col, L.perm, rb, re, R, tile_slots,
+                                      run_words, workers, B, st);
+  B->n_chunks = n_chunks;
+  return rc;
+}
+
+int build_blocked_ranges(int m, long long nnz, const int *d_rowptr, const int *d_col,
+                         const int *d_perm, const std::vector<int> &rb,
+                         const std::vector<int> &re, int R, int tile_slots, int run_words,
+                         int workers, BlockedLayout *B, cudaStream_t st) {
   *B = BlockedLayout();
   B->R = R;
   B->run_words = run_words;
   B->tile_slots = tile_slots;
-  B->row0 = row0;
-  B->n_chunks = n_chunks;
-  const int n_rows = L.n_nz - row0;
-  if (R < 1 || R > kBlockedMaxRows || tile_slots < kRunWords || row0 < 0 || row0 > L.n_long ||
-      run_words < 128 || run_words > 512 || run_words % 128 != 0) {
-    set_error("blocked layout: block rows %d must be in [1, %d], tile words %d >= %d", R,
-              kBlockedMaxRows, tile_slots, kRunWords);
+  const int n_ranges = (int)rb.size();
+  bool ranges_ok = n_ranges >= 1 && re.size() == rb.size();
+  for (int i = 0; ranges_ok && i < n_ranges; ++i)
+    ranges_ok = rb[i] >= 0 && re[i] >= rb[i] && re[i] <= m && (i == 0 || rb[i] >= re[i - 1]);
+  if (R < 1 || R > kBlockedMaxRows || tile_slots < kRunWords || !ranges_ok || run_words < 128 ||
+      run_words > 512 || run_words % 128 != 0) {
+    set_error("blocked layout: block rows %d must be in [1, %d], tile words %d >= %d, row "
+              "ranges ascending and disjoint", R, kBlockedMaxRows, tile_slots, kRunWords);
     return GPR_EINVAL;
   }
-  B->n_blocks = n_rows > 0 ? (int)ceil_div(n_rows, R) : 0;
-  if (n_rows <= 0 || nnz == 0) {
+  // Blocks: each range cut into blocks of R rows; accumulators of the rows
+  // [row0, row end of the last range).
+  std::vector<int> bb(n_ranges + 1, 0);
+  for (int i = 0; i < n_ranges; ++i) bb[i + 1] = bb[i] + (int)ceil_div(re[i] - rb[i], R);
+  B->n_blocks = bb[n_ranges];
+  B->row0 = rb[0];
+  B->range_tiles.assign(n_ranges + 1, 0);
+  const int n_rows = re[n_ranges - 1] - rb[0];
+  if (B->n_blocks == 0 || nnz == 0) {
     B->n_blocks = 0;
     return GPR_OK;
   }
   // Keys and values of every edge; blocked ones first after the sort.
-  int *inv = nullptr;
+  int *inv = nullptr, *d_rng = nullptr;
   unsigned long long *k0 = nullptr, *k1 = nullptr;
   unsigned *v0 = nullptr, *v1 = nullptr;
   void *tmp = nullptr;
   int rc = GPR_OK;
   auto fail = [&](int code) {
-    dfree(inv); dfree(k0); dfree(k1); dfree(v0); dfree(v1); dfree(tmp);
+    dfree(inv); dfree(d_rng); dfree(k0); dfree(k1); dfree(v0); dfree(v1); dfree(tmp);
     free_blocked_layout(B);
     return code;
   };
   if ((rc = dalloc(&inv, (size_t)m + 2, "blocked: inverse")) != GPR_OK ||
+      (rc = dalloc(&d_rng, 3 * (size_t)n_ranges, "blocked: row ranges")) != GPR_OK ||
       (rc = dalloc(&k0, (size_t)nnz, "blocked: keys")) != GPR_OK ||
       (rc = dalloc(&k1, (size_t)nnz, "blocked: keys")) != GPR_OK ||
       (rc = dalloc(&v0, (size_t)nnz, "blocked: rows")) != GPR_OK ||
       (rc = dalloc(&v1, (size_t)nnz, "blocked: rows")) != GPR_OK)
     return fail(rc);
-  k_inverse<<<grid_of(m), 256, 0, st>>>(m, L.perm, inv);
-  k_block_keys<<<grid_of((long long)m * 32), 256, 0, st>>>(m, d_rowptr, d_col, inv, row0,
-                                                           L.n_nz, R, k0, v0);
+  if ((rc = GPR_CUDA_RC(cudaMemcpyAsync(d_rng, rb.data(), sizeof(int) * n_ranges,
+                                        cudaMemcpyHostToDevice, st))) != GPR_OK ||
+      (rc = GPR_CUDA_RC(cudaMemcpyAsync(d_rng + n_ranges, re.data(), sizeof(int) * n_ranges,
+                                        cudaMemcpyHostToDevice, st))) != GPR_OK ||
+      (rc = GPR_CUDA_RC(cudaMemcpyAsync(d_rng + 2 * n_ranges, bb.data(), sizeof(int) * n_ranges,
+                                        cudaMemcpyHostToDevice, st))) != GPR_OK)
+    return fail(rc);
+  k_inverse<<<grid_of(m), 256, 0, st>>>(m, d_perm, inv);
+  k_block_keys<<<grid_of((long long)m * 32), 256, 0, st>>>(m, d_rowptr, d_col, inv, n_ranges,
+                                                           d_rng, d_rng + n_ranges,
+                                                           d_rng + 2 * n_ranges, R, k0, v0);
   if ((rc = GPR_CUDA_RC(cudaGetLastError())) != GPR_OK) return fail(rc);
   // Sort on (block, source): bits of the source ids, then of the block ids
   // (the ~0 keys of the excluded edges have every bit set and sort last).
@@ -277,7 +318,7 @@ int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d
   }
   B->edges = n_edges;
   if (n_edges == 0) {
-    dfree(inv); dfree(k0); dfree(k1); dfree(v0); dfree(v1);
+    dfree(inv); dfree(d_rng); dfree(k0); dfree(k1); dfree(v0); dfree(v1);
     B->n_blocks = 0;
     return GPR_OK;
   }
@@ -347,10 +388,11 @@ int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d
   std::vector<uint2> runs;
   std::vector<int4> tiles;
   std::vector<int4> blocks(B->n_blocks);
-  for (int b = 0; b < B->n_blocks; ++b) {
-    const int r0 = row0 + b * R;
-    blocks[b] = make_int4(r0, std::min(R, L.n_nz - r0), 0, 0);
-  }
+  for (int i = 0; i < n_ranges; ++i)
+    for (int b = bb[i]; b < bb[i + 1]; ++b) {
+      const int r0 = rb[i] + (b - bb[i]) * R;
+      blocks[b] = make_int4(r0, std::min(R, re[i] - r0), 0, i);
+    }
   runs.reserve((size_t)(n_edges / run_words) + ng + 1);
   long long pos = 0;
   int g = 0;
@@ -430,6 +472,14 @@ int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d
     if (!split) break;
   }
   std::stable_sort(tiles.begin(), tiles.end(), by_cost);
+  // Each tile's residual slot (its .w on the device; the words are host-only):
+  // tiles numbered range by range, so a range's slots are contiguous.
+  for (const int4 &t : tiles) B->range_tiles[blocks[t.x].w + 1] += 1;
+  for (int i = 0; i < n_ranges; ++i) B->range_tiles[i + 1] += B->range_tiles[i];
+  {
+    std::vector<int> next_slot(B->range_tiles.begin(), B->range_tiles.end() - 1);
+    for (int4 &t : tiles) t.w = next_slot[blocks[t.x].w]++;
+  }
   B->slots = pos;
   B->n_runs = (long long)runs.size();
   B->n_tiles = (int)tiles.size();
@@ -441,6 +491,7 @@ int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d
   if (rc == GPR_OK) rc = dalloc(&B->tiles, (size_t)B->n_tiles, "blocked: tiles");
   if (rc == GPR_OK) rc = dalloc(&B->blocks, (size_t)B->n_blocks, "blocked: blocks");
   if (rc == GPR_OK) rc = dalloc(&B->gacc, (size_t)n_rows, "blocked: cross-tile sums");
+  B->gacc_rows = n_rows;
   if (rc == GPR_OK) rc = dalloc(&B->bcnt, (size_t)B->n_blocks, "blocked: tile counters");
   if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemcpyAsync(d_gpos, gpos.data(), sizeof(long long) * ng,
                                                      cudaMemcpyHostToDevice, st));
@@ -461,7 +512,7 @@ int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d
   dfree(d_gpos);
   dfree(gstart);
   if (rc != GPR_OK) return fail(rc);
-  dfree(inv); dfree(k0); dfree(k1); dfree(v0); dfree(v1);
+  dfree(inv); dfree(d_rng); dfree(k0); dfree(k1); dfree(v0); dfree(v1);
   B->device_bytes = 4 * pos + 8 * B->n_runs + 16LL * B->n_tiles + 16LL * B->n_blocks +
                     8LL * n_rows + 4LL * B->n_blocks;
   return GPR_OK;

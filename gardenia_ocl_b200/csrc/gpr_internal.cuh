@@ -141,9 +141,11 @@ struct BlockedLayout {
   long long n_runs = 0, slots = 0, edges = 0;
   unsigned *entry = nullptr;             // [slots]
   uint2 *runs = nullptr;                 // [n_runs] {first word, segment << 16 | words}
-  int4 *tiles = nullptr;                 // [n_tiles] {block, run0, run1, words}
-  int4 *blocks = nullptr;                // [n_blocks] {row0, nrows, tiles, 0}
-  unsigned long long *gacc = nullptr;    // [n_nz - row0] sums of multi-tile blocks
+  int4 *tiles = nullptr;                 // [n_tiles] {block, run0, run1, residual slot}
+  int4 *blocks = nullptr;                // [n_blocks] {row0, nrows, tiles, row range}
+  std::vector<int> range_tiles;          // [ranges + 1] residual slots of each row range
+  unsigned long long *gacc = nullptr;    // [gacc_rows] sums of multi-tile blocks, rows row0 on
+  long long gacc_rows = 0;
   int *bcnt = nullptr;                   // [n_blocks] tiles done in the current sweep
   long long device_bytes = 0;
 };
@@ -158,6 +160,14 @@ int blocked_split(const PrLayout &L, const int *d_rowptr, int long_min, int R, i
 int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
                          const PrLayout &L, int row0, int n_chunks, int R, int tile_slots,
                          int run_words, int workers, BlockedLayout *B, cudaStream_t st);
+// The same for several row ranges of the relabelled order (perm: new -> old),
+// ascending and disjoint (one per graph of a batch): blocks never span two
+// ranges; blocks[b].w is the block's range, tiles[t].w the tile's residual
+// slot, numbered range by range (B->range_tiles).
+int build_blocked_ranges(int m, long long nnz, const int *d_rowptr, const int *d_col,
+                         const int *d_perm, const std::vector<int> &rb,
+                         const std::vector<int> &re, int R, int tile_slots, int run_words,
+                         int workers, BlockedLayout *B, cudaStream_t st);
 // CTAs per SM of the blocked kernel for blocks of R rows: two 512-thread CTAs
 // when both fit beside an L1 of about half the SM's 256 KB, else one of 1024.
 inline int blocked_ctas_per_sm(int R) { return R <= 8192 ? 2 : 1; }

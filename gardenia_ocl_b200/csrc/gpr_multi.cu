@@ -37,6 +37,7 @@
 #include <numeric>
 #include <vector>
 
+#include "gpr_blocked.cuh"
 #include "gpr_device.cuh"
 #include "gpr_internal.cuh"
 #include "gpr_guard.h"
@@ -85,6 +86,20 @@ struct MultiArgs {
   int max_iter, bar_expect;
   long long timeout_ns;
   unsigned long long cond;  // graph mode: while-node condition handle (0: none)
+  // blocked form (gpr_blocked.cuh): each graph's rows with in-edges in
+  // blocks, tiles of source-ordered entries; null tb: the units form
+  const int *tb;          // [G+1] residual slots (tiles) of each graph
+  double *terr;           // [tiles] residual of each tile, by slot
+  int n_tiles, acc_rows, blk_row0;
+  const int4 *tiles;
+  const int4 *blocks;     // .w: the block's graph
+  const uint2 *runs;
+  const unsigned *entry;
+  unsigned long long *gacc;
+  int *bcnt;
+  int *tq;                // [2] tile-queue heads by parity
+  float fx_scale;         // 2^S: contributions as 64-bit fixed point
+  double fx_inv;          // 2^-S
 };
 
 template <typename T>
@@ -216,21 +231,24 @@ __device__ __forceinline__ double range_sum(const double *v, int b, int e, int l
   return ((acc[0] + acc[1]) + (acc[2] + acc[3])) + ((acc[4] + acc[5]) + (acc[6] + acc[7]));
 }
 
-// `done` units of graph g finished by this warp in sweep it.  The warp that
-// completes the graph's last unit sums the graph's unit residuals in unit
-// order and decides whether the graph keeps updating.
+// `done` units of graph g finished by this warp in sweep it (in the blocked
+// form a tile counts as one unit).  The warp that completes the graph's last
+// unit sums the graph's unit (or tile) residuals in slot order and decides
+// whether the graph keeps updating.
 __device__ __forceinline__ void finish_units(const MultiArgs &a, int g, int done, int it,
                                              int lane) {
   int last = 0;
   if (lane == 0) {
-    const int expect = (a.hb[g + 1] - a.hb[g]) + (it < 2 ? a.zb[g + 1] - a.zb[g] : 0);
+    const int heavy = a.tb ? a.tb[g + 1] - a.tb[g] : a.hb[g + 1] - a.hb[g];
+    const int expect = heavy + (it < 2 ? a.zb[g + 1] - a.zb[g] : 0);
     __threadfence();
     last = atomicAdd(a.gdone + g, done) + done == expect;
   }
   last = __shfl_sync(kFull, last, 0);
   if (!last) return;
   __threadfence();
-  double t = range_sum(a.uerr, a.hb[g], a.hb[g + 1], lane);
+  double t = a.tb ? range_sum(a.terr, a.tb[g], a.tb[g + 1], lane)
+                  : range_sum(a.uerr, a.hb[g], a.hb[g + 1], lane);
   if (it < 2) t += range_sum(a.uerr, a.zb[g], a.zb[g + 1], lane);
   t = warp_sum(t);
   if (lane == 0) {
@@ -261,6 +279,7 @@ __device__ void multi_close(const MultiArgs &a, int it) {
       }
     }
   atomicExch(a.wq + (it & 1), 0);
+  if (a.tq) atomicExch(a.tq + (it & 1), 0);
   atomicExch(a.n_next + (it & 1), 0);
 }
 
@@ -368,6 +387,103 @@ __global__ void __launch_bounds__(kMultiBlock, 1) k_multi(MultiArgs a) {
     a.status[1] = it;
     a.status[2] = 1;
   }
+}
+
+// All sweeps of the blocked form in one cooperative launch (FP32), MINB CTAs
+// of NT threads per SM.  Per sweep: CTAs take tiles from a queue (heaviest
+// first), skipping the tiles of graphs that no longer update; a tile's
+// residual goes to its graph's slot and the CTA that finishes a graph's last
+// unit closes the graph (as the units form does).  Then, in sweeps 0 and 1,
+// warps take the packets of zero-in-degree rows.  One bounded grid barrier
+// per sweep.
+template <int PV, int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_multi_blocked(MultiArgs a) {
+  extern __shared__ unsigned s_acc[];  // [2 * acc_rows]: low / high words
+  __shared__ int s_tile, s_next_tile, s_last, s_next;
+  __shared__ double s_red[NT / 32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const Policies pol = make_policies();
+  int it = 0;
+  while (it < a.max_iter) {
+    const float *cin = static_cast<const float *>((it & 1) ? a.c1 : a.c0);
+    float *cout = static_cast<float *>((it & 1) ? a.c0 : a.c1);
+    int *tq = a.tq + (it & 1);
+    if (threadIdx.x == 0) s_next_tile = atomicAdd(tq, 1);
+    for (;;) {
+      __syncthreads();
+      if (threadIdx.x == 0) s_tile = s_next_tile;
+      __syncthreads();
+      const int t = s_tile;
+      if (t >= a.n_tiles) break;
+      const int4 td = __ldg(a.tiles + t);
+      const int g = __ldg(&a.blocks[td.x].w);
+      if (it >= __ldcg(a.stop + g)) {  // the graph no longer updates
+        if (threadIdx.x == 0) s_next_tile = atomicAdd(tq, 1);
+        continue;
+      }
+      const float base = __fdiv_rn(__fsub_rn(1.0f, a.damp), __int2float_rn(__ldg(a.gm + g)));
+      double err = gpr::blk::blocked_tile<PV, NT>(a, cin, cout, t, s_acc, &s_next, &s_last,
+                                                  &s_next_tile, tq, base, pol);
+      err = warp_sum(err);
+      if (lane == 0) s_red[warp] = err;
+      __syncthreads();
+      if (warp == 0) {
+        double e = lane < NT / 32 ? s_red[lane] : 0.0;
+        e = warp_sum(e);
+        if (lane == 0) a.terr[td.w] = e;
+        finish_units(a, g, 1, it, lane);
+      }
+    }
+    if (it < 2) {  // zero-in-degree rows: the zero packets of the units form
+      for (;;) {
+        int p = 0;
+        if (lane == 0) p = atomicAdd(a.wq + (it & 1), 1);
+        p = a.n_hpk + __shfl_sync(kFull, p, 0);
+        if (p >= a.n_pk) break;
+        const int u0 = __ldg(a.pk + p), u1 = __ldg(a.pk + p + 1);
+        int cur = -1, done = 0;
+        bool act = false;
+        float base = 0.f;
+        for (int u = u0; u < u1; ++u) {
+          const int4 md = __ldg(a.meta + u);
+          const int g = md.w >> 8;
+          if (g != cur) {
+            if (done) finish_units(a, cur, done, it, lane);
+            cur = g;
+            done = 0;
+            act = it < __ldcg(a.stop + g);
+            base = __fdiv_rn(__fsub_rn(1.0f, a.damp), __int2float_rn(__ldg(a.gm + g)));
+          }
+          if (!act) continue;
+          double err = m_zero(a, cout, md, base, lane, it, pol);
+          err = warp_sum(err);
+          if (lane == 0) a.uerr[u] = err;
+          ++done;
+        }
+        if (done) finish_units(a, cur, done, it, lane);
+      }
+    }
+    if (!multi_barrier(a, it)) return;
+    const int n = __ldcg(a.n_next + ((it + 1) & 1));
+    ++it;
+    if (n == 0) break;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) {
+    a.status[1] = it;
+    a.status[2] = 1;
+  }
+}
+
+// Largest |score| (bits of a non-negative float order like the float; a NaN
+// sorts above every finite value and infinity).
+__global__ void k_multi_max_abs(int m, const float *__restrict__ s, unsigned *out) {
+  unsigned mx = 0u;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < m;
+       i += (long long)gridDim.x * blockDim.x)
+    mx = max(mx, __float_as_uint(s[i]) & 0x7FFFFFFFu);
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(kFull, mx, o));
+  if ((threadIdx.x & 31) == 0) atomicMax(out, mx);
 }
 
 // One sweep per launch (graph mode): the body of a CUDA-graph while node.
@@ -605,6 +721,14 @@ struct gpr_multigraph {
   bool own_stream = false;
   cudaEvent_t e0 = nullptr, e1 = nullptr, e2 = nullptr, e3 = nullptr;
   long long device_bytes = 0;
+  // blocked form: each graph's rows with in-edges in blocks
+  gpr::BlockedLayout B;
+  bool has_blocked = false, blocked_ok = false;
+  int grid_blocked = 0, blocked_ctas = 1, max_gm = 0;
+  int *tq = nullptr, *tb = nullptr, *lazy_b = nullptr;
+  std::vector<int> lazy_bh;     // graphs with vertices but no tiles
+  double *terr = nullptr;
+  unsigned *fx_max = nullptr;
 };
 
 namespace {
@@ -617,14 +741,24 @@ const void *multi_step_kernel(bool bf) {
   return bf ? (const void *)k_multi_step<16, 4, bf16> : (const void *)k_multi_step<16, 4, float>;
 }
 
+// The blocked batch kernel with `ctas` CTAs per SM (1: 1024 threads, 2: 512).
+const void *multi_blocked_kernel(int ctas) {
+  return ctas == 2 ? (const void *)k_multi_blocked<4, 512, 2>
+                   : (const void *)k_multi_blocked<4, 1024, 1>;
+}
+
+// solve_phase status: the blocked form cannot represent these scores
+constexpr int kMultiBlockedFallback = 100;
+
 void destroy_multi(gpr_multigraph *g) {
   if (!g) return;
   void *ptrs[] = {g->perm,  g->outdeg, g->ecol,    g->meta,    g->uoff,   g->gm,
                   g->hb,    g->zb,     g->cap,     g->stop,    g->gdone,  g->lazy,
                   g->gres,  g->s,      g->c0,      g->c1,      g->h0,     g->h1,
                   g->partial, g->cnt,  g->uerr,    g->n_next,  g->bar,    g->status,
-                  g->wq,    g->scores_tmp, g->pk};
+                  g->wq,    g->scores_tmp, g->pk, g->tq, g->tb, g->lazy_b, g->terr, g->fx_max};
   for (void *p : ptrs) gpr::dfree(p);
+  gpr::free_blocked_layout(&g->B);
   if (g->e0) cudaEventDestroy(g->e0);
   if (g->e1) cudaEventDestroy(g->e1);
   if (g->e2) cudaEventDestroy(g->e2);
@@ -648,6 +782,9 @@ struct Tmp {
 
 int build_multi(gpr_multigraph *g, const int *h_voff, const int *d_rowptr, const int *d_col,
                 const int *d_outdeg, const gpr_layout_opts *lopts) {
+  const gpr_layout_opts *blo = nullptr;  // the first graph's options that ask for blocks
+  for (int ug = 0; lopts && ug < g->G && !blo; ++ug)
+    if (lopts[ug].flags & GPR_LAYOUT_BLOCKED) blo = lopts + ug;
   const int G = g->G, M = g->M;
   cudaStream_t st = g->st;
   Tmp T;
@@ -899,6 +1036,64 @@ int build_multi(gpr_multigraph *g, const int *h_voff, const int *d_rowptr, const
   }
   g->grid = (int)std::max<long long>(1, std::min<long long>(sms, gpr::ceil_div(U, 32)));
   GPR_CUDA(cudaStreamSynchronize(st));
+  for (int r = 0; r < G; ++r) g->max_gm = std::max(g->max_gm, gm[r]);
+  if (blo) {
+    // Blocked form: the rows with in-edges of each graph (the first rows of
+    // its range) in blocks of R rows, never spanning two graphs.
+    std::vector<int> rb(G), re(G);
+    long long rows = 0;
+    for (int r = 0; r < G; ++r) {
+      rb[r] = g->ivoff[r];
+      re[r] = g->ivoff[r] + bounds[8 * (size_t)r + 6];
+      rows += re[r] - rb[r];
+    }
+    const int R = blo->block_rows
+                      ? blo->block_rows
+                      : (int)std::min<long long>(gpr::kBlockedRows,
+                                                 std::max<long long>(256, gpr::ceil_div(rows, 2LL * sms)));
+    const int tile_words = blo->tile_words ? blo->tile_words : gpr::kTileWordsDefault;
+    GPR_TRY(gpr::build_blocked_ranges(M, g->nnz, d_rowptr, d_col, g->perm, rb, re, R, tile_words,
+                                      gpr::kRunWords, sms * gpr::blocked_ctas_per_sm(R), &g->B,
+                                      st));
+    const gpr::BlockedLayout &B = g->B;
+    g->lazy_bh.clear();
+    for (int r = 0; r < G; ++r)
+      if (g->ivoff[r + 1] > g->ivoff[r] && B.range_tiles[r + 1] == B.range_tiles[r])
+        g->lazy_bh.push_back(r);
+    GPR_TRY(gpr::dalloc(&g->tb, (size_t)G + 1, "graph tile slots"));
+    GPR_TRY(gpr::dalloc(&g->terr, (size_t)std::max(B.n_tiles, 1), "tile residuals"));
+    GPR_TRY(gpr::dalloc(&g->lazy_b, std::max<size_t>(g->lazy_bh.size(), 1), "graphs without tiles"));
+    GPR_TRY(gpr::dalloc(&g->tq, 2, "tile queue"));
+    GPR_TRY(gpr::dalloc(&g->fx_max, 1, "largest score"));
+    GPR_CUDA(cudaMemcpyAsync(g->tb, B.range_tiles.data(), sizeof(int) * ((size_t)G + 1),
+                             cudaMemcpyHostToDevice, st));
+    if (!g->lazy_bh.empty())
+      GPR_CUDA(cudaMemcpyAsync(g->lazy_b, g->lazy_bh.data(), sizeof(int) * g->lazy_bh.size(),
+                               cudaMemcpyHostToDevice, st));
+    // CTAs per SM and the smallest carveout that holds them (as the
+    // single-graph blocked kernel)
+    int smem_sm = 0, per_bsm = 0;
+    GPR_CUDA(cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, g->device));
+    g->blocked_ctas = gpr::blocked_ctas_per_sm(B.R > 0 ? B.R : R);
+    const int smem = 8 * std::max(B.R, 1);
+    for (;;) {
+      const void *k = multi_blocked_kernel(g->blocked_ctas);
+      cudaFuncAttributes fa;
+      GPR_CUDA(cudaFuncGetAttributes(&fa, k));
+      const long long need = (long long)g->blocked_ctas * (smem + (long long)fa.sharedSizeBytes + 1024);
+      const int carve = (int)std::min<long long>(100, gpr::ceil_div(100 * need, smem_sm));
+      GPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+      GPR_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, carve));
+      GPR_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_bsm, k, 1024 / g->blocked_ctas, smem));
+      if (per_bsm >= g->blocked_ctas || g->blocked_ctas == 1) break;
+      g->blocked_ctas = 1;
+    }
+    g->grid_blocked = sms * g->blocked_ctas;
+    g->blocked_ok = g->coop_ok && per_bsm >= g->blocked_ctas;
+    g->has_blocked = true;
+    g->device_bytes += B.device_bytes + 8LL * std::max(B.n_tiles, 1) + 4LL * (G + 1);
+    GPR_CUDA(cudaStreamSynchronize(st));
+  }
   return GPR_OK;
 }
 
@@ -906,7 +1101,7 @@ int build_multi(gpr_multigraph *g, const int *h_voff, const int *d_rowptr, const
 // graph.  Reads back the sweeps (stop) and last residual of every graph.
 int solve_phase(gpr_multigraph *g, float *d_scores, const gpr_pr_opts &o, bool bf,
                 const std::vector<int> &caps, std::vector<int> *iters, std::vector<double> *res,
-                gpr_pr_stats *out) {
+                gpr_pr_stats *out, bool blocked = false) {
   const int G = g->G, M = g->M;
   cudaStream_t st = g->st;
   if (bf && !g->h0) {
@@ -927,6 +1122,7 @@ int solve_phase(gpr_multigraph *g, float *d_scores, const gpr_pr_opts &o, bool b
   GPR_CUDA(cudaMemcpyAsync(g->cap, caps.data(), sizeof(int) * G, cudaMemcpyHostToDevice, st));
   GPR_CUDA(cudaMemcpyAsync(g->stop, caps.data(), sizeof(int) * G, cudaMemcpyHostToDevice, st));
   MultiArgs a;
+  memset(&a, 0, sizeof(a));
   a.M = M;
   a.G = G;
   a.n_heavy = g->n_heavy;
@@ -963,10 +1159,51 @@ int solve_phase(gpr_multigraph *g, float *d_scores, const gpr_pr_opts &o, bool b
   a.n_pk = g->n_pk;
   a.timeout_ns = (long long)(o.timeout_s * 1e9);
   a.cond = 0;
+  if (blocked) {
+    const gpr::BlockedLayout &B = g->B;
+    GPR_CUDA(cudaMemsetAsync(g->tq, 0, 2 * sizeof(int), st));
+    GPR_CUDA(cudaMemsetAsync(g->fx_max, 0, sizeof(unsigned), st));
+    if (B.n_blocks) {
+      // clean after an abandoned solve; a completed sweep leaves them clean
+      GPR_CUDA(cudaMemsetAsync(B.bcnt, 0, sizeof(int) * B.n_blocks, st));
+      GPR_CUDA(cudaMemsetAsync(B.gacc, 0, 8 * (size_t)B.gacc_rows, st));
+    }
+    // Fixed-point exponent from the largest initial score: every graph's
+    // total |score| stays at most max(1, m_g max|s0|) <= B0 (as gpr_pagerank).
+    k_multi_max_abs<<<std::min<long long>(grid_for(M), 148 * 8), 256, 0, st>>>(M, d_scores, g->fx_max);
+    GPR_CUDA(cudaGetLastError());
+    unsigned bits = 0;
+    GPR_CUDA(cudaMemcpyAsync(&bits, g->fx_max, sizeof(bits), cudaMemcpyDeviceToHost, st));
+    GPR_CUDA(cudaStreamSynchronize(st));
+    float mx;
+    memcpy(&mx, &bits, sizeof(mx));
+    if (!isfinite(mx)) return kMultiBlockedFallback;
+    const double b0 = std::max(1.0, (double)g->max_gm * (double)mx);
+    const int cap = 62 - (int)ceil(log2(b0));
+    const int pref = (int)floor(log2(std::max(1.0, (double)g->nnz) / b0)) + 28;
+    const int S = std::min(cap, std::max(31, pref));
+    a.fx_scale = ldexpf(1.f, S);
+    a.fx_inv = ldexp(1.0, -S);
+    a.tb = g->tb;
+    a.terr = g->terr;
+    a.n_tiles = B.n_tiles;
+    a.acc_rows = B.R;
+    a.blk_row0 = B.row0;
+    a.tiles = B.tiles;
+    a.blocks = B.blocks;
+    a.runs = B.runs;
+    a.entry = B.entry;
+    a.gacc = B.gacc;
+    a.bcnt = B.bcnt;
+    a.tq = g->tq;
+    a.lazy = g->lazy_b;
+    a.n_lazy = (int)g->lazy_bh.size();
+    a.bar_expect = g->grid_blocked + (o.reserved[0] > 0 ? o.reserved[0] : 0);
+  }
   // Graph mode when asked for, or when the persistent kernel cannot be
   // co-resident: the sweep loop as a CUDA-graph while node whose body is one
   // k_multi_step launch, built here and released after the phase.
-  const bool graph_mode = o.loop == GPR_LOOP_GRAPH || !g->coop_ok;
+  const bool graph_mode = !blocked && (o.loop == GPR_LOOP_GRAPH || !g->coop_ok);
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   if (max_cap > 0 && graph_mode) {
@@ -1020,6 +1257,20 @@ int solve_phase(gpr_multigraph *g, float *d_scores, const gpr_pr_opts &o, bool b
       gpr::set_error("multi-graph loop graph: %s", cudaGetErrorString(e));
       return GPR_ECUDA;
     }
+  } else if (max_cap > 0 && blocked) {
+    void *args[] = {&a};
+    cudaError_t e = cudaLaunchCooperativeKernel(
+        multi_blocked_kernel(g->blocked_ctas), dim3(g->grid_blocked),
+        dim3(1024 / g->blocked_ctas), args, 8 * (size_t)g->B.R, st);
+    if (e == cudaErrorCooperativeLaunchTooLarge) {
+      cudaGetLastError();
+      return kMultiBlockedFallback;
+    }
+    if (e != cudaSuccess) {
+      gpr::set_error("multi-graph cooperative launch: %s", cudaGetErrorString(e));
+      return GPR_ECUDA;
+    }
+    ++launches;
   } else if (max_cap > 0) {
     void *args[] = {&a};
     cudaError_t e = cudaLaunchCooperativeKernel(multi_kernel(bf), dim3(g->grid), dim3(kMultiBlock),
@@ -1049,7 +1300,7 @@ int solve_phase(gpr_multigraph *g, float *d_scores, const gpr_pr_opts &o, bool b
   out->iterations = max_cap > 0 ? hs[1] : 0;
   out->solve_ms = ms;
   out->loop_ms = lms;
-  out->gpu_launches = launches + (max_cap > 0 && graph_mode ? hs[3] : 0);
+  out->gpu_launches = launches + (max_cap > 0 && graph_mode ? hs[3] : 0) + (blocked ? 1 : 0);
   double rmax = 0.0;
   for (double r : *res) rmax = std::max(rmax, r);
   out->residual = rmax;
@@ -1074,6 +1325,25 @@ int multi_pagerank_impl(gpr_multigraph *g, float *any_scores, const gpr_pr_opts 
     gpr::set_error("gpr_multigraph_pagerank: precision %d not supported", o.precision);
     return GPR_EUNSUPPORTED;
   }
+  if (o.form != GPR_FORM_AUTO && o.form != GPR_FORM_EXACT && o.form != GPR_FORM_BLOCKED) {
+    gpr::set_error("gpr_multigraph_pagerank: unknown form %d", o.form);
+    return GPR_EINVAL;
+  }
+  if (o.form == GPR_FORM_BLOCKED) {
+    if (!g->has_blocked) {
+      gpr::set_error("gpr_multigraph_pagerank: GPR_FORM_BLOCKED needs a batch created with "
+                     "GPR_LAYOUT_BLOCKED");
+      return GPR_EINVAL;
+    }
+    if (o.precision != GPR_PREC_FP32 || o.loop == GPR_LOOP_GRAPH || !g->blocked_ok) {
+      gpr::set_error("gpr_multigraph_pagerank: GPR_FORM_BLOCKED runs FP32 in the persistent "
+                     "loop only");
+      return GPR_EUNSUPPORTED;
+    }
+  }
+  const bool use_blocked = o.precision == GPR_PREC_FP32 && g->has_blocked && g->blocked_ok &&
+                           o.loop != GPR_LOOP_GRAPH && o.form != GPR_FORM_EXACT &&
+                           (o.form == GPR_FORM_BLOCKED || g->nnz >= gpr::kBlockedAutoMinEdges);
   gpr_pr_stats sl;
   memset(&sl, 0, sizeof(sl));
   const int G = g->G, M = g->M;
@@ -1103,7 +1373,17 @@ int multi_pagerank_impl(gpr_multigraph *g, float *any_scores, const gpr_pr_opts 
   int rc;
   std::vector<int> refine(G, 0);
   if (o.precision == GPR_PREC_FP32) {
-    rc = solve_phase(g, d_scores, o, false, caps, &it1, &r1, &sl);
+    rc = use_blocked ? solve_phase(g, d_scores, o, false, caps, &it1, &r1, &sl, true)
+                     : kMultiBlockedFallback;
+    if (rc == kMultiBlockedFallback) {
+      if (o.form == GPR_FORM_BLOCKED) {
+        gpr::set_error("gpr_multigraph_pagerank: GPR_FORM_BLOCKED needs finite scores and a "
+                       "co-resident grid");
+        rc = GPR_EINVAL;
+      } else {
+        rc = solve_phase(g, d_scores, o, false, caps, &it1, &r1, &sl);
+      }
+    }
   } else {
     gpr_pr_opts o1 = o;
     o1.tol = std::max(o.tol, kBf16Tol);

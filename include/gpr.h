@@ -230,7 +230,15 @@ int gpr_pagerank_push(gpr_graph *g, float *any_scores, const gpr_pr_opts *opts,
  * GPR_EINVAL otherwise).  rowptr / col / outdeg are the usual in-CSR and
  * out-degrees over all h_voff[n_graphs] vertices.  h_lopts (n_graphs entries,
  * or NULL for the defaults) gives each graph its own bins: sell_max, chunk,
- * chunk_min as in gpr_graph_create_ex (hot_entries and flags are ignored).
+ * chunk_min as in gpr_graph_create_ex (hot_entries is ignored).  When any
+ * graph's flags hold GPR_LAYOUT_BLOCKED the batch also builds the blocked
+ * form's layout: every graph's rows with in-edges in blocks of block_rows
+ * rows that never span two graphs, tiles of up to tile_words words (the
+ * first such graph's values; 0: defaults as in gpr_graph_create_ex).
+ * opts->form then works as for gpr_pagerank: BLOCKED sums every graph's rows
+ * in 64-bit fixed point (one exponent S for the batch, from its edge count
+ * and the largest m_g x |initial score|), FP32 and the persistent loop only;
+ * AUTO picks it from 50,331,648 edges in the batch, else the units form.
  *
  * gpr_multigraph_pagerank solves every graph as gpr_pagerank would solve it
  * alone -- base (1 - kDamp) / m_g, its own L1 residual, stop after its first
