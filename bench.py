@@ -1024,10 +1024,12 @@ def profile_multigraph(args):
 
     import gardenia_ocl_b200 as G
     A, voff = G.gen_multigraph(args.profile_multigraph, MG_MMIN, MG_MMAX, seed=MG_SEED)
-    mg = G.MultiGraph(A.rowptr, A.col, A.third, voff, nnz=A.nnz)
+    blocked = args.profile_form == "blocked"
+    mg = G.MultiGraph(A.rowptr, A.col, A.third, voff, nnz=A.nnz, blocked=blocked)
     scores = torch.from_numpy(mg.initial_scores()).cuda()
     _, it, _, st = mg.pagerank(scores, tol=0.0, max_iter=args.profile_solve or 10,
-                               damping=DAMPING)
+                               damping=DAMPING,
+                               form=G.FORM_BLOCKED if blocked else G.FORM_EXACT)
     log(json.dumps({"info": mg.info(), **st.as_dict()}))
     mg.close()
     A.close()
@@ -1112,7 +1114,8 @@ def main():
     ap.add_argument("--profile-loop", choices=["persistent", "graph"], default="persistent",
                     help="sweep loop of --profile-solve")
     ap.add_argument("--profile-form", choices=["exact", "blocked"], default="exact",
-                    help="sweep form of --profile-solve (k_pr_hot / k_pr_step or k_pr_blocked)")
+                    help="sweep form of --profile-solve (k_pr_hot / k_pr_step or k_pr_blocked) "
+                         "and of --profile-multigraph (k_multi or k_multi_blocked)")
     ap.add_argument("--profile-multigraph", type=int, default=0, metavar="GRAPHS",
                     help="build the first GRAPHS graphs of the multi-graph batch and run one "
                          "solve of --profile-solve sweeps (the case profiled with ncu)")
