@@ -160,10 +160,9 @@ void free_blocked_layout(BlockedLayout *B) {
 }
 
 int blocked_split(const PrLayout &L, const int *d_rowptr, int long_min, int R, int *row0,
-                  int *n_chunks, long long *long_words, cudaStream_t st) {
+                  int *n_chunks, cudaStream_t st) {
   *row0 = 0;
   *n_chunks = 0;
-  *long_words = 0;
   if (L.n_long == 0) return GPR_OK;
   // in-degrees of the chunkable rows and of the R rows after them
   const int n = (int)std::min<long long>(L.n_nz, (long long)L.n_long + R);
@@ -197,16 +196,11 @@ int blocked_split(const PrLayout &L, const int *d_rowptr, int long_min, int R, i
     }
   }
   int cb = 0;
-  long long lw = 0;
   rc = GPR_CUDA_RC(cudaMemcpyAsync(&cb, L.row_cbeg + cnt, sizeof(int), cudaMemcpyDeviceToHost, st));
-  if (rc == GPR_OK)
-    rc = GPR_CUDA_RC(cudaMemcpyAsync(&lw, L.long_ptr + cnt, sizeof(long long),
-                                     cudaMemcpyDeviceToHost, st));
   if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaStreamSynchronize(st));
   if (rc != GPR_OK) return rc;
   *row0 = cnt;
   *n_chunks = cb;
-  *long_words = lw;
   return GPR_OK;
 }
 

@@ -3,7 +3,7 @@
 // batch (gpr_multi.cu).  Templated on the kernel's argument struct, which
 // provides: entry, runs, tiles, blocks (the layout), acc_rows, gacc, bcnt,
 // blk_row0 (cross-tile accumulators of rows blk_row0 on), fx_scale, fx_inv,
-// s, outdeg, damp, m.  The base of the update is given per tile (one graph's
+// s, outdeg, damp.  The base of the update is given per tile (one graph's
 // (1 - d) / m_g).
 #pragma once
 
@@ -14,7 +14,7 @@ namespace blk {
 
 using namespace gpr::dev;
 
-// Rows [n_long, n_nz) are summed block by block (gpr_blocked.cu): the CTA that
+// The blocked rows are summed block by block (gpr_blocked.cu): the CTA that
 // takes a tile zeroes one accumulator per row of the tile's block in shared
 // memory, its warps take the tile's runs (source-ordered entries, so a warp's
 // gathers share lines) and add each contribution to its row's accumulator.

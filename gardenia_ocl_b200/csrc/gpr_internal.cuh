@@ -153,10 +153,10 @@ struct BlockedLayout {
 // Rows of the blocked form that stay chunked: the first *row0 rows of the
 // exact-order layout's chunked rows [0, L.n_long), either those with more than
 // long_min in-edges or, when long_min is 0, those holding more than 1/8 of the
-// in-edges of the R rows that start at them; their *n_chunks chunks and the
-// *long_words padded entries of those rows.  Synchronizes st.
+// in-edges of the R rows that start at them; and their *n_chunks chunks.
+// Synchronizes st.
 int blocked_split(const PrLayout &L, const int *d_rowptr, int long_min, int R, int *row0,
-                  int *n_chunks, long long *long_words, cudaStream_t st);
+                  int *n_chunks, cudaStream_t st);
 int build_blocked_layout(int m, long long nnz, const int *d_rowptr, const int *d_col,
                          const PrLayout &L, int row0, int n_chunks, int R, int tile_slots,
                          int run_words, int workers, BlockedLayout *B, cudaStream_t st);

@@ -768,10 +768,9 @@ int create_impl(int m, long long nnz, const int *any_rowptr, const int *any_col,
           gpr::kBlockedRows,
           std::max<long long>(256, gpr::ceil_div((long long)g->L.n_nz, 2LL * nsm)));
     int row0 = 0, n_chunks = 0;
-    long long long_words = 0;
     rc = gpr::blocked_split(g->L, (const int *)rp,
                             blocked_long > 0 ? std::max(blocked_long, chunk_min) : 0, block_rows,
-                            &row0, &n_chunks, &long_words, st);
+                            &row0, &n_chunks, st);
     if (tile_words == 0) tile_words = gpr::kTileWordsDefault;
     if (rc == GPR_OK)
       rc = gpr::build_blocked_layout(m, nnz, (const int *)rp, (const int *)cp, g->L, row0,
