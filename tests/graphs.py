@@ -52,3 +52,39 @@ def degree_ladder(seed=0):
     src.append(rng.integers(0, m, 4 * m))
     dst.append(rng.integers(len(degs), m, 4 * m))
     return in_csr(m, np.concatenate(src), np.concatenate(dst))
+
+
+def zoo(kind, seed):
+    """One small graph of a given shape for property tests: 'er' uniform,
+    'power' power-law sources and targets, 'chain' a directed path plus a
+    few back edges, 'islands' disconnected pieces with isolated vertices,
+    'sink' many vertices without out-edges."""
+    rng = np.random.default_rng(seed)
+    m = int(rng.integers(300, 30000))
+    if kind == "er":
+        return erdos_renyi(m, float(rng.uniform(1, 12)), seed)
+    if kind == "power":
+        w = 1.0 / np.arange(1, m + 1) ** rng.uniform(0.6, 1.1)
+        p = w / w.sum()
+        ne = int(m * rng.uniform(4, 16))
+        return in_csr(m, rng.choice(m, ne, p=p), rng.permutation(m)[rng.choice(m, ne, p=p)])
+    if kind == "chain":
+        src = np.concatenate([np.arange(m - 1), rng.integers(0, m, m // 10)])
+        dst = np.concatenate([np.arange(1, m), rng.integers(0, m, m // 10)])
+        return in_csr(m, src, dst)
+    if kind == "islands":
+        k = int(rng.integers(2, 8))
+        cuts = np.sort(rng.choice(np.arange(1, m), k - 1, replace=False))
+        bounds = np.concatenate([[0], cuts, [m]])
+        src, dst = [], []
+        for a, b in zip(bounds[:-1], bounds[1:]):
+            if b - a > 3:
+                n = (b - a) * 4
+                src.append(rng.integers(a, b - 2, n))   # the last two of each piece isolated
+                dst.append(rng.integers(a, b - 2, n))
+        return in_csr(m, np.concatenate(src), np.concatenate(dst))
+    if kind == "sink":
+        ne = m * 6
+        src = rng.integers(0, m // 3, ne)               # two thirds have no out-edges
+        return in_csr(m, src, rng.integers(0, m, ne))
+    raise ValueError(kind)

@@ -17,7 +17,7 @@ import math
 import numpy as np
 import pytest
 
-from graphs import degree_ladder, erdos_renyi, star
+from graphs import degree_ladder, erdos_renyi, star, zoo
 
 pytestmark = pytest.mark.gpu
 
@@ -243,3 +243,26 @@ def test_blocked_barrier_wait_is_bounded(G, O):
         s, st = g.pagerank(tol=1e-6, max_iter=10, form=G.FORM_BLOCKED)
     ref, ref_it, _ = O.pr_plain_f32(rp, col, od, tol=1e-6, max_iter=10)
     assert np.abs(s - ref).max() <= ABS_TOL
+
+
+@pytest.mark.parametrize("kind", ["er", "power", "chain", "islands", "sink"])
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_graph_zoo_is_the_fixed_point_recurrence(G, O, kind, seed):
+    """Random shapes and random cuts into blocks and tiles (one or two CTAs
+    per SM): two sweeps bit for bit the fixed-point restatement, and a solve
+    to tol 1e-6 within the parity bar of the oracle."""
+    rp, col, od = zoo(kind, seed)
+    m = len(rp) - 1
+    rng = np.random.default_rng(100 * seed + len(kind))
+    layout = dict(block_rows=int(rng.integers(1, 12289)), tile_words=int(rng.integers(512, 1 << 17)),
+                  blocked_long=1 << 30)
+    s0 = np.full(m, np.float32(1.0) / np.float32(m), dtype=np.float32)
+    with G.Graph(rp, col, od, blocked=True, **layout) as g:
+        s, st = g.pagerank(tol=0.0, max_iter=2, form=G.FORM_BLOCKED)
+        ref, _ = fixed_point_sweeps(rp, col, od, s0, 2)
+        assert np.array_equal(s, ref), (kind, seed, layout)
+        s, st = g.pagerank(tol=1e-6, max_iter=100, form=G.FORM_BLOCKED)
+    ref, ref_it, _ = O.pr_plain_f32(rp, col, od, tol=1e-6, max_iter=100)
+    assert abs(st.iterations - ref_it) <= 1
+    s64, _, _ = O.pr_f64(rp, col, od, tol=0.0, max_iter=st.iterations)
+    assert np.all(np.abs(s - ref) <= ABS_TOL + np.abs(ref - s64))

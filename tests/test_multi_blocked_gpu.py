@@ -16,7 +16,7 @@ import math
 import numpy as np
 import pytest
 
-from graphs import erdos_renyi
+from graphs import erdos_renyi, zoo
 from test_multi_gpu import concat, local
 
 pytestmark = pytest.mark.gpu
@@ -175,3 +175,27 @@ def test_blocked_barrier_wait_is_bounded(G, O, batch):
         s, iters, _, _ = mg.pagerank(tol=1e-6, max_iter=20, form=G.FORM_BLOCKED)
         s2, iters2, _, _ = mg.pagerank(tol=1e-6, max_iter=20, form=G.FORM_BLOCKED)
     assert np.array_equal(s, s2) and np.array_equal(iters, iters2)
+
+
+@pytest.mark.parametrize("seed", [1, 2, 3])
+def test_zoo_batch_is_the_fixed_point_recurrence(G, O, seed):
+    """A batch of random shapes (and an empty graph) cut into random blocks:
+    three sweeps of every graph bit for bit the fixed-point restatement."""
+    rng = np.random.default_rng(seed)
+    kinds = ["er", "power", "chain", "islands", "sink"]
+    parts = [zoo(kinds[i % 5], 10 * seed + i) for i in range(int(rng.integers(3, 9)))]
+    parts.insert(int(rng.integers(0, len(parts))),
+                 (np.zeros(1, np.int32), np.zeros(0, np.int32), np.zeros(0, np.int32)))
+    rp, col, od, voff = concat(parts)
+    layout = dict(block_rows=int(rng.integers(1, 12289)), tile_words=int(rng.integers(512, 1 << 17)))
+    with G.MultiGraph(rp, col, od, voff, blocked=True, **layout) as mg:
+        s0 = mg.initial_scores()
+        S = batch_shift(voff, len(col), s0)
+        s, iters, _, _ = mg.pagerank(s0.copy(), tol=0.0, max_iter=3, form=G.FORM_BLOCKED)
+    for g, (lrp, lcol, lod) in enumerate(parts):
+        a, b = voff[g], voff[g + 1]
+        if b == a:
+            continue
+        assert iters[g] == 3
+        ref = fixed_point_sweeps(lrp, lcol, lod, s0[a:b], 3, S)
+        assert np.array_equal(s[a:b], ref), (seed, g, layout)
