@@ -50,6 +50,7 @@
 #include <algorithm>
 #include <functional>
 #include <queue>
+#include <type_traits>
 #include <vector>
 
 #include "gpr_internal.cuh"
@@ -73,14 +74,45 @@ __global__ void k_inverse(int m, const int *__restrict__ perm, int *inv) {
   if (i < m) inv[perm[i]] = i;
 }
 
+// Sort keys of the blocked edges.  Wide: key = block << 32 | source (64
+// bits), value = row in block.  Compact (when the bits fit 31): key = block
+// << sb | source >> 3, the 8-source sector in sb >= 13 bits (32 bits: fewer
+// passes and two thirds of the bytes of the sort), value = (source & 7) << 16
+// | row in block.  Both order a block's edges by segment (source >> 16), then by
+// sector: a warp's gathers share lines either way (within a sector the
+// compact sort keeps the edges in input order; the sums do not depend on it).
+// Excluded edges get the key ~0 (sorted last).
+template <bool C>
+struct BlockKey {
+  using T = typename std::conditional<C, unsigned, unsigned long long>::type;
+  static constexpr T none = ~(T)0;
+  __device__ static T make(unsigned long long blk, unsigned src, int sb) {
+    return C ? (T)((blk << sb) | (src >> 3)) : (T)((blk << 32) | src);
+  }
+  __device__ static unsigned value(unsigned src, unsigned dl) {
+    return C ? ((src & 7u) << 16) | dl : dl;
+  }
+  __device__ static unsigned long long group(T k) { return C ? (k >> 13) : (k >> 16); }
+  __device__ static int block(T k, int sb) { return C ? (int)(k >> sb) : (int)(k >> 32); }
+  __device__ static int segment(T k, int sb) {
+    return C ? (int)((k & ((1u << sb) - 1u)) >> 13) : (int)((k & 0xFFFFFFFFull) >> 16);
+  }
+  // the entry word: (source & 0xFFFF) << 16 | row in block
+  __device__ static unsigned entry(T k, unsigned v) {
+    const unsigned lo = C ? ((unsigned)(k & 0x1FFFu) << 3) | ((v >> 16) & 7u)
+                          : (unsigned)(k & 0xFFFFull);
+    return (lo << 16) | (v & 0xFFFFu);
+  }
+};
+
 // One warp per original row: the keys and values of its in-edges when its
 // new label falls in a blocked range [rb[i], re[i]) (ranges ascending and
-// disjoint, range i's blocks numbered from bb[i]); other edges get the key ~0
-// (sorted last).
+// disjoint, range i's blocks numbered from bb[i]); other edges get the key ~0.
+template <bool C>
 __global__ void k_block_keys(int m, const int *__restrict__ rowptr, const int *__restrict__ col,
                              const int *__restrict__ inv, int n_ranges, const int *__restrict__ rb,
-                             const int *__restrict__ re, const int *__restrict__ bb, int R,
-                             unsigned long long *key, unsigned *val) {
+                             const int *__restrict__ re, const int *__restrict__ bb, int R, int sb,
+                             typename BlockKey<C>::T *key, unsigned *val) {
   const long long w = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (w >= m) return;
@@ -96,50 +128,57 @@ __global__ void k_block_keys(int m, const int *__restrict__ rowptr, const int *_
   const unsigned long long blk = in ? (unsigned long long)(bb[lo] + (r - rb[lo]) / R) : 0ull;
   const unsigned dl = in ? (unsigned)((r - rb[lo]) % R) : 0u;
   for (int e = rowptr[o] + lane; e < rowptr[o + 1]; e += 32) {
-    key[e] = in ? (blk << 32) | (unsigned)inv[col[e]] : ~0ull;
-    val[e] = dl;
+    const unsigned src = (unsigned)inv[col[e]];
+    key[e] = in ? BlockKey<C>::make(blk, src, sb) : BlockKey<C>::none;
+    val[e] = BlockKey<C>::value(src, dl);
   }
 }
 
 // First index whose key is ~0 (the blocked edges precede it): one thread.
-__global__ void k_count_blocked(long long n, const unsigned long long *__restrict__ key,
+template <bool C>
+__global__ void k_count_blocked(long long n, const typename BlockKey<C>::T *__restrict__ key,
                                 long long *out) {
   long long lo = 0, hi = n;
   while (lo < hi) {
     const long long mid = (lo + hi) / 2;
-    if (key[mid] == ~0ull) hi = mid;
+    if (key[mid] == BlockKey<C>::none) hi = mid;
     else lo = mid + 1;
   }
   *out = lo;
 }
 
-__global__ void k_group_flags(long long n, const unsigned long long *__restrict__ key,
+// 1 where a (block, segment) group starts
+template <bool C>
+__global__ void k_group_flags(long long n, const typename BlockKey<C>::T *__restrict__ key,
                               int *flag) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i < n) flag[i] = (i == 0 || (key[i] >> 16) != (key[i - 1] >> 16)) ? 1 : 0;
+  if (i < n)
+    flag[i] = (i == 0 || BlockKey<C>::group(key[i]) != BlockKey<C>::group(key[i - 1])) ? 1 : 0;
 }
 
+template <bool C>
 __global__ void k_group_keys(int ng, const int *__restrict__ gstart,
-                             const unsigned long long *__restrict__ key, int *gblk, int *gseg) {
+                             const typename BlockKey<C>::T *__restrict__ key, int sb, int *gblk,
+                             int *gseg) {
   const int g = blockIdx.x * blockDim.x + threadIdx.x;
   if (g < ng) {
-    const unsigned long long k = key[gstart[g]];
-    gblk[g] = (int)(k >> 32);
-    gseg[g] = (int)((k & 0xFFFFFFFFull) >> 16);
+    const typename BlockKey<C>::T k = key[gstart[g]];
+    gblk[g] = BlockKey<C>::block(k, sb);
+    gseg[g] = BlockKey<C>::segment(k, sb);
   }
 }
 
 // Entry i of the sorted edges goes to word gpos[gid] + (i - gstart[gid]),
 // gid = (inclusive count of group starts up to i) - 1.
-__global__ void k_place(long long n, const unsigned long long *__restrict__ key,
+template <bool C>
+__global__ void k_place(long long n, const typename BlockKey<C>::T *__restrict__ key,
                         const unsigned *__restrict__ val, const int *__restrict__ gid1,
                         const int *__restrict__ gstart, const long long *__restrict__ gpos,
                         unsigned *entry) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int g = gid1[i] - 1;
-  const unsigned src = (unsigned)(key[i] & 0xFFFFFFFFull);
-  entry[gpos[g] + (i - gstart[g])] = ((src & 0xFFFFu) << 16) | val[i];
+  entry[gpos[g] + (i - gstart[g])] = BlockKey<C>::entry(key[i], val[i]);
 }
 
 unsigned grid_of(long long n, int block = 256) {
@@ -273,37 +312,51 @@ int build_blocked_ranges(int m, long long nnz, const int *d_rowptr, const int *d
       (rc = GPR_CUDA_RC(cudaMemcpyAsync(d_rng + 2 * n_ranges, bb.data(), sizeof(int) * n_ranges,
                                         cudaMemcpyHostToDevice, st))) != GPR_OK)
     return fail(rc);
-  k_inverse<<<grid_of(m), 256, 0, st>>>(m, d_perm, inv);
-  k_block_keys<<<grid_of((long long)m * 32), 256, 0, st>>>(m, d_rowptr, d_col, inv, n_ranges,
-                                                           d_rng, d_rng + n_ranges,
-                                                           d_rng + 2 * n_ranges, R, k0, v0);
-  if ((rc = GPR_CUDA_RC(cudaGetLastError())) != GPR_OK) return fail(rc);
-  // Sort on (block, source): bits of the source ids, then of the block ids
-  // (the ~0 keys of the excluded edges have every bit set and sort last).
-  int blk_bits = 1;
+  // Sort on (block, source or sector): the bits of the sources, then of the
+  // blocks (the ~0 keys of the excluded edges have every bit set and sort
+  // last).  Compact keys when block and sector fit 31 bits.
+  int blk_bits = 1, src_bits = 3;
   while ((1LL << blk_bits) <= B->n_blocks) ++blk_bits;
-  const int end_bit = 32 + blk_bits;
-  {
+  while ((1LL << src_bits) < m) ++src_bits;
+  const int sb = std::max(src_bits - 3, 13);  // sector bits: key >> 13 is (block, segment)
+  const bool compact = sb + blk_bits <= 31;
+  const int end_bit = compact ? sb + blk_bits : 32 + blk_bits;
+  unsigned *c0 = reinterpret_cast<unsigned *>(k0), *c1 = reinterpret_cast<unsigned *>(k1);
+  k_inverse<<<grid_of(m), 256, 0, st>>>(m, d_perm, inv);
+  if (compact)
+    k_block_keys<true><<<grid_of((long long)m * 32), 256, 0, st>>>(
+        m, d_rowptr, d_col, inv, n_ranges, d_rng, d_rng + n_ranges, d_rng + 2 * n_ranges, R, sb,
+        c0, v0);
+  else
+    k_block_keys<false><<<grid_of((long long)m * 32), 256, 0, st>>>(
+        m, d_rowptr, d_col, inv, n_ranges, d_rng, d_rng + n_ranges, d_rng + 2 * n_ranges, R, sb,
+        k0, v0);
+  if ((rc = GPR_CUDA_RC(cudaGetLastError())) != GPR_OK) return fail(rc);
+  auto sort = [&](auto *ka, auto *kb_) -> int {
+    using KT = typename std::remove_pointer<decltype(ka)>::type;
     size_t tb = 0;
-    cub::DoubleBuffer<unsigned long long> kb(k0, k1);
+    cub::DoubleBuffer<KT> kb(ka, kb_);
     cub::DoubleBuffer<unsigned> vb(v0, v1);
-    if ((rc = GPR_CUDA_RC(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, (int)nnz, 0,
-                                                          end_bit, st))) != GPR_OK)
-      return fail(rc);
-    if ((rc = dmalloc(&tmp, tb, "blocked: sort scratch")) != GPR_OK) return fail(rc);
-    if ((rc = GPR_CUDA_RC(cub::DeviceRadixSort::SortPairs(tmp, tb, kb, vb, (int)nnz, 0, end_bit,
-                                                          st))) != GPR_OK)
-      return fail(rc);
+    int r = GPR_CUDA_RC(cub::DeviceRadixSort::SortPairs(nullptr, tb, kb, vb, (int)nnz, 0, end_bit, st));
+    if (r == GPR_OK) r = dmalloc(&tmp, tb, "blocked: sort scratch");
+    if (r == GPR_OK)
+      r = GPR_CUDA_RC(cub::DeviceRadixSort::SortPairs(tmp, tb, kb, vb, (int)nnz, 0, end_bit, st));
     dfree(tmp);
     tmp = nullptr;
-    if (kb.Current() != k0) std::swap(k0, k1);
-    if (vb.Current() != v0) std::swap(v0, v1);
-  }
+    if (r == GPR_OK && kb.Current() != ka) {
+      std::swap(k0, k1);
+      std::swap(c0, c1);
+    }
+    if (r == GPR_OK && vb.Current() != v0) std::swap(v0, v1);
+    return r;
+  };
+  if ((rc = compact ? sort(c0, c1) : sort(k0, k1)) != GPR_OK) return fail(rc);
   // Number of blocked edges: the keys before the first ~0.
   long long n_edges = 0;
   {
     long long *d_n = reinterpret_cast<long long *>(inv);  // inv is no longer needed
-    k_count_blocked<<<1, 1, 0, st>>>(nnz, k0, d_n);
+    if (compact) k_count_blocked<true><<<1, 1, 0, st>>>(nnz, c0, d_n);
+    else k_count_blocked<false><<<1, 1, 0, st>>>(nnz, k0, d_n);
     if ((rc = GPR_CUDA_RC(cudaGetLastError())) != GPR_OK ||
         (rc = GPR_CUDA_RC(cudaMemcpyAsync(&n_edges, d_n, sizeof(n_edges), cudaMemcpyDeviceToHost,
                                           st))) != GPR_OK ||
@@ -319,7 +372,8 @@ int build_blocked_ranges(int m, long long nnz, const int *d_rowptr, const int *d
   // Group starts (block, segment) and their keys.
   int *flag = reinterpret_cast<int *>(k1);  // k1 is free now
   int *gid1 = reinterpret_cast<int *>(v1);                       // so is v1
-  k_group_flags<<<grid_of(n_edges), 256, 0, st>>>(n_edges, k0, flag);
+  if (compact) k_group_flags<true><<<grid_of(n_edges), 256, 0, st>>>(n_edges, c0, flag);
+  else k_group_flags<false><<<grid_of(n_edges), 256, 0, st>>>(n_edges, k0, flag);
   int *gstart = nullptr, *nsel = nullptr;
   if ((rc = dalloc(&gstart, (size_t)n_edges, "blocked: groups")) != GPR_OK ||
       (rc = dalloc(&nsel, 1, "blocked: group count")) != GPR_OK) {
@@ -360,7 +414,8 @@ int build_blocked_ranges(int m, long long nnz, const int *d_rowptr, const int *d
     rc = dalloc(&gblk, (size_t)ng, "blocked: group blocks");
     if (rc == GPR_OK) rc = dalloc(&gseg, (size_t)ng, "blocked: group segments");
     if (rc == GPR_OK) {
-      k_group_keys<<<grid_of(ng), 256, 0, st>>>(ng, gstart, k0, gblk, gseg);
+      if (compact) k_group_keys<true><<<grid_of(ng), 256, 0, st>>>(ng, gstart, c0, sb, gblk, gseg);
+      else k_group_keys<false><<<grid_of(ng), 256, 0, st>>>(ng, gstart, k0, sb, gblk, gseg);
       rc = GPR_CUDA_RC(cudaGetLastError());
     }
     if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemcpyAsync(h_gstart.data(), gstart, sizeof(int) * ng,
@@ -506,7 +561,10 @@ int build_blocked_ranges(int m, long long nnz, const int *d_rowptr, const int *d
   if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemsetAsync(B->gacc, 0, sizeof(unsigned long long) * n_rows, st));
   if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaMemsetAsync(B->bcnt, 0, sizeof(int) * B->n_blocks, st));
   if (rc == GPR_OK) {
-    k_place<<<grid_of(n_edges), 256, 0, st>>>(n_edges, k0, v0, gid1, gstart, d_gpos, B->entry);
+    if (compact)
+      k_place<true><<<grid_of(n_edges), 256, 0, st>>>(n_edges, c0, v0, gid1, gstart, d_gpos, B->entry);
+    else
+      k_place<false><<<grid_of(n_edges), 256, 0, st>>>(n_edges, k0, v0, gid1, gstart, d_gpos, B->entry);
     rc = GPR_CUDA_RC(cudaGetLastError());
   }
   if (rc == GPR_OK) rc = GPR_CUDA_RC(cudaStreamSynchronize(st));
