@@ -362,7 +362,8 @@ class MultiGraph:
     graph: graph g owns vertices [voff[g], voff[g+1]) and the in-edges of its
     rows come from that range (global vertex ids).  ``layouts``: None, or one
     dict per graph with any of sell_max / chunk / chunk_min (each graph's own
-    bins).  Every graph is solved as ``Graph.pagerank`` solves it alone, all
+    bins) and blocked / block_rows / tile_words (the blocked form for the
+    whole batch, as ``tune_multigraph`` returns them).  Every graph is solved as ``Graph.pagerank`` solves it alone, all
     in one persistent launch.  ``blocked``: also build the blocked form's
     layout (each graph's rows in blocks; ``block_rows`` / ``tile_words`` as
     for ``Graph``), which ``pagerank`` uses from 50.3M edges up (AUTO) or when
@@ -382,10 +383,12 @@ class MultiGraph:
             lo = (LayoutOptions * self.n_graphs)()
             for i in range(self.n_graphs):
                 d = (layouts[i] if layouts is not None else None) or {}
+                b = blocked or bool(d.get("blocked", False))
                 lo[i] = LayoutOptions(int(d.get("sell_max", 0)), int(d.get("chunk", 0)),
                                       int(d.get("chunk_min", 0)), 0,
-                                      LAYOUT_BLOCKED if blocked else 0, int(block_rows),
-                                      int(tile_words), 0)
+                                      LAYOUT_BLOCKED if b else 0,
+                                      int(block_rows or d.get("block_rows", 0)),
+                                      int(tile_words or d.get("tile_words", 0)), 0)
         pr, k0 = _ptr(rowptr, np.int32)
         pc, k1 = _ptr(col, np.int32)
         pd, k2 = _ptr(outdeg, np.int32)
@@ -755,8 +758,9 @@ def tune_graph(rowptr, col, outdeg, m=None, nnz=None, cache=None, sweeps=5) -> d
 
 
 def tune_multigraph(rowptr, col, outdeg, voff, nnz=None, cache=None, sweeps=5):
-    """Per-graph bins for a batch (gpr_tune_multigraph): returns (layouts, summary),
-    ``layouts`` ready for ``MultiGraph(..., layouts=layouts)``."""
+    """Per-graph bins, or the blocked form, for a batch (gpr_tune_multigraph):
+    returns (layouts, summary), ``layouts`` ready for
+    ``MultiGraph(..., layouts=layouts)``."""
     voff = np.ascontiguousarray(voff, dtype=np.int32)
     n = len(voff) - 1
     nnz = int(len(col)) if nnz is None else int(nnz)
@@ -768,7 +772,9 @@ def tune_multigraph(rowptr, col, outdeg, voff, nnz=None, cache=None, sweeps=5):
     _check(lib().gpr_tune_multigraph(n, C.c_void_p(voff.ctypes.data), nnz, pr, pc, pd,
                                      os.fsencode(cache) if cache else None, int(sweeps), lo,
                                      C.byref(r)))
-    layouts = [{"sell_max": x.sell_max, "chunk": x.chunk, "chunk_min": x.chunk_min} for x in lo]
+    layouts = [{"sell_max": x.sell_max, "chunk": x.chunk, "chunk_min": x.chunk_min,
+                "blocked": bool(x.flags & LAYOUT_BLOCKED), "block_rows": x.block_rows,
+                "tile_words": x.tile_words} for x in lo]
     return layouts, r.as_dict()
 
 

@@ -18,9 +18,10 @@
 // rows are summed in chunks rather than in blocks.  Each candidate is timed as the best of kReps solves of exactly
 // `sweeps` sweeps (tol 0), device time of the sweep loop
 // (gpr_pr_stats.loop_ms), and taken only when at least kMargin faster than the
-// current pick.  The batch tuner groups graphs by signature and tunes one
-// group at a time on the whole batch, the other groups keeping their current
-// picks (exact order only).
+// current pick.  The batch tuner first tries the blocked form for the whole
+// batch (with its rows per block and words per tile); otherwise it groups
+// graphs by signature and tunes the exact-order bins one group at a time on
+// the whole batch, the other groups keeping their current picks.
 //
 // Cache file: one line per entry, later lines override earlier ones:
 //   <signature> <sell_max> <chunk> <chunk_min> <hot_entries> <variant> <ms_per_sweep>
@@ -339,8 +340,39 @@ int gpr_tune_multigraph(int n_graphs, const int *h_voff, long long nnz, const in
   const double t0 = run(pick);
   if (!isfinite(t0)) return GPR_ECUDA;
   double best = t0;
+  // The blocked form covers the whole batch: it is built when any graph asks
+  // for it, with the rows per block and words per tile of the first graph
+  // that does.  So it is a batch-wide choice, tried first and carried by the
+  // group with the largest edge share; when it wins, only its knobs are
+  // searched (the sweep does not read the exact-order bins).
+  bool blocked = false;
+  for (auto &k : groups) blocked = blocked || (pick[k].flags & GPR_LAYOUT_BLOCKED) != 0;
+  const std::string &k0 = groups[0];
+  if (!blocked && !cached[k0]) {
+    std::function<double(const Cfg &)> time = [&](const Cfg &x) {
+      auto p = pick;
+      p[k0] = x;
+      return run(p);
+    };
+    Cfg xb = pick[k0];
+    xb.flags |= GPR_LAYOUT_BLOCKED;
+    const double tb = time(xb);
+    if (tb < best * (1.0 - kMargin)) {
+      best = tb;
+      descend(&xb, &best, std::vector<int>{6144, 8192},
+              [](Cfg *y, int v) { y->block_rows = v; }, time);
+      descend(&xb, &best, std::vector<int>{2097152, 4194304},
+              [](Cfg *y, int v) { y->tile_words = v; }, time);
+      pick[k0] = xb;
+      blocked = true;
+    }
+  }
   for (auto &k : groups) {
     if (cached[k]) continue;
+    if (blocked) {
+      save_cache(cache_path, k, pick[k], best);
+      continue;
+    }
     std::function<double(const Cfg &)> time = [&](const Cfg &x) {
       auto p = pick;
       p[k] = x;

@@ -268,14 +268,17 @@ int gpr_multigraph_pagerank(gpr_multigraph *mg, float *any_scores,
 
 /* ---- autotuner -------------------------------------------------------------
  * No counterpart in the reference (its launch shape is fixed at compile time,
- * include/common.h:30, src/pr/Makefile:17-47).  Picks the layout bins
- * (sell_max = lanes-per-row bound of the SELL width classes, chunk_min /
- * chunk = chunked-row threshold and chunk size), the shared-memory hot prefix
- * and the sweep-kernel variant for a graph's in-degree distribution by timing
- * candidates on the graph (coordinate descent from the defaults, each
- * candidate the best of 2 solves of exactly `sweeps` sweeps), and caches the
- * pick per distribution signature in the text file cache_path (NULL: no
- * cache).  A cached signature returns at once (from_cache = 1). */
+ * include/common.h:30, src/pr/Makefile:17-47).  Picks the form (exact order,
+ * or GPR_LAYOUT_BLOCKED with its block_rows / tile_words / blocked_long), the
+ * layout bins (sell_max = lanes-per-row bound of the SELL width classes,
+ * chunk_min / chunk = chunked-row threshold and chunk size), the
+ * shared-memory hot prefix and the sweep-kernel variant for a graph's
+ * in-degree distribution by timing candidates on the graph (coordinate
+ * descent from the defaults, each candidate the best of 3 solves of exactly
+ * `sweeps` sweeps after a warm-up solve, kept only when 3% faster than the
+ * current pick), and caches the pick per distribution signature in the text
+ * file cache_path (NULL: no cache).  A cached signature returns at once
+ * (from_cache = 1). */
 typedef struct {
   gpr_layout_opts layout;       /* pass to gpr_graph_create_ex */
   int variant;                  /* pass as gpr_pr_opts.variant */
@@ -288,8 +291,10 @@ typedef struct {
 int gpr_tune_graph(int m, long long nnz, const int *any_rowptr,
                    const int *any_col, const int *any_outdeg,
                    const char *cache_path, int sweeps, gpr_tune_result *out);
-/* Batch: graphs grouped by signature, one group tuned at a time on the whole
- * batch; h_lopts_out (n_graphs entries) receives each graph's bins for
+/* Batch: first the blocked form for the whole batch (carried by the group
+ * with the largest edge share, with its block_rows / tile_words); else graphs
+ * grouped by signature, one group's bins tuned at a time on the whole batch.
+ * h_lopts_out (n_graphs entries) receives each graph's options for
  * gpr_multigraph_create; out (may be NULL) describes the largest group. */
 int gpr_tune_multigraph(int n_graphs, const int *h_voff, long long nnz,
                         const int *any_rowptr, const int *any_col,

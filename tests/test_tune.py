@@ -86,3 +86,29 @@ def test_tune_multigraph(G, O, tmp_path):
         assert np.all(np.abs(s[a:b] - ref) <= 1e-6 + np.abs(ref - s64))
     lays2, r2 = G.tune_multigraph(rp, col, od, voff, cache=cache, sweeps=4)
     assert lays2 == lays and r2["candidates"] == 1
+
+
+@pytest.mark.gpu
+def test_tune_multigraph_blocked_pick_reaches_the_batch(G, O, tmp_path):
+    """A blocked pick (here written into the cache, as the tuner writes it
+    when the blocked form wins) comes back in every graph's layout and builds
+    the batch's blocked form, which then solves like the units form."""
+    rp, col, od, voff = O.multigraph(10, 300, 20000, seed=6)
+    cache = str(tmp_path / "tune.txt")
+    sigs = {G.tune_signature(rp[voff[g]:voff[g + 1] + 1] - rp[voff[g]], batch=True)
+            for g in range(10)}
+    with open(cache, "w") as f:
+        for s in sorted(sigs):  # flags 4: GPR_LAYOUT_BLOCKED
+            f.write(f"{s} 64 4096 4096 32768 0 0.5 4 300 1024 0\n")
+    lays, r = G.tune_multigraph(rp, col, od, voff, cache=cache, sweeps=4)
+    assert r["from_cache"] and r["blocked"] and r["candidates"] == 1
+    assert all(d["blocked"] and d["block_rows"] == 300 and d["tile_words"] == 1024
+               for d in lays)
+    with G.MultiGraph(rp, col, od, voff, layouts=lays) as mg:
+        s, iters, _, _ = mg.pagerank(tol=1e-6, max_iter=100, form=G.FORM_BLOCKED)
+        u, it_u, _, _ = mg.pagerank(tol=1e-6, max_iter=100, form=G.FORM_EXACT)
+    assert np.all(np.abs(iters.astype(int) - it_u.astype(int)) <= 1)
+    assert np.all(np.abs(s - u) <= 1e-6)
+    with G.MultiGraph(rp, col, od, voff) as mg:  # no blocked layout: refused
+        with pytest.raises(G.GprError):
+            mg.pagerank(tol=1e-6, max_iter=100, form=G.FORM_BLOCKED)
