@@ -678,7 +678,7 @@ S16_SCALE, S16_TOL, S16_MAX_ITER = 16, 1e-4, 100
 
 
 def s16_leg(G, torch, dev, stream, args):
-    """plain PageRank on RMAT scale 16 (edge factor 16, same
+    """The small workload: plain PageRank on RMAT scale 16 (edge factor 16, same
     RMAT parameters), tol 1e-4, at most 100 sweeps, from 1/m.  On the GPU
     through the graph handle (device-resident graph: exact-order and blocked
     forms, device time of the solve) and end to end through PageRank() with

@@ -1,7 +1,7 @@
 /*
  * extern "C" entry points over the reference's own OpenMP solvers, verifiers
  * and graph loader (compiled from the reference tree into oracle/_ref).
- * TEST / BASELINE INFRASTRUCTURE ONLY: loaded by the tests and by bench.py's
+ * TEST AND CPU-BASELINE INFRASTRUCTURE ONLY: loaded by the tests and by bench.py's
  * CPU-baseline and reference legs, never by the product library.
  *
  * Bound symbols (C++ linkage in the reference):

@@ -39,7 +39,7 @@ def test_bench_line_contract():
     acc = line["accuracy"]
     assert acc["l1_error_vs_fp64_fixed_point"] <= 1e-5
     assert acc["max_error_vs_fp64_fixed_point"] <= acc["l1_error_vs_fp64_fixed_point"]
-    # BASELINE config 1 (RMAT s16, tol 1e-4) beside the reference's OpenMP solver
+    # the small workload (RMAT s16, tol 1e-4) beside the reference's OpenMP solver
     s16 = line["s16"]
     assert abs(s16["gpu_exact"]["sweeps"] - s16["cpu_reference"]["sweeps"]) <= 1
     assert s16["max_abs_diff_gpu_vs_reference"] <= 1e-6
