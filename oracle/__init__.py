@@ -1,8 +1,8 @@
 """ctypes bindings for the oracle (test infrastructure only).
 
-This package is the checker.  Only the tests, ``__graft_entry__.smoke()`` and
-the CPU-baseline / reference legs of ``bench.py`` import it; the product
-package ``gardenia_ocl_b200`` never does.
+It checks results; it is never the thing measured or shipped.  Only the
+tests, ``__graft_entry__.smoke()`` and the CPU-baseline / reference legs of
+``bench.py`` import it; the product package ``gardenia_ocl_b200`` never does.
 
 Two libraries are bound:
 
